@@ -1,0 +1,183 @@
+/*
+ * pscf_gpu.h -- C ABI of the B200 SCFT propagator engine (libpscfgpu.so).
+ *
+ * Drop-in boundary for the hot path of the Fortran PSCF solver.  Each entry
+ * point names the reference routine it replaces.  The reference keeps its
+ * state in module globals and exits with `stop` on errors; here the state
+ * lives in an opaque engine handle and every call returns a status code
+ * (0 = OK, see PSCFG_E*), with a message from pscfg_last_error().
+ *
+ * Conventions (kept from the reference so a Fortran host can pass its
+ * arrays through ISO_C_BINDING without copies):
+ *   - grid fields are x-fastest (Fortran column-major (0:n1-1,0:n2-1,0:n3-1)),
+ *     unused dimensions have extent 1 (src/grid_mod.f90:84-93);
+ *   - a multi-monomer field is [n_monomer][nr] with nr = n1*n2*n3, i.e. the
+ *     Fortran omega_grid(0:,0:,0:,1:N_monomer) (src/grid_mod.f90:43-46);
+ *   - monomer indices are 0-based (1-based in Fortran input);
+ *   - all values are double precision on the host side.
+ *
+ * An engine holds a batch of n_inst independent SCFT instances that share
+ * one grid shape (dim, n1, n2, n3) and precision; each instance has its own
+ * chemistry and unit cell.  Batch calls act on every instance.  Host-side
+ * arrays are laid out instance-major ([n_inst][...]).  Calls on one engine
+ * are not thread safe; an engine owns one CUDA stream.
+ */
+#ifndef PSCF_GPU_H
+#define PSCF_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSCFG_MAXM 4      /* monomer types   */
+#define PSCFG_MAXC 4      /* chain species   */
+#define PSCFG_MAXB 8      /* blocks per chain */
+#define PSCFG_MAXS 4      /* solvent species */
+#define PSCFG_MAXCP 6     /* cell parameters */
+
+/* status codes */
+#define PSCFG_OK 0
+#define PSCFG_EINVAL 1     /* invalid argument */
+#define PSCFG_ECUDA 2      /* CUDA runtime error */
+#define PSCFG_ENOMEM 3     /* device allocation failed */
+#define PSCFG_ESTATE 4     /* call order violated (e.g. stress before density) */
+#define PSCFG_ENOTCONV 5   /* iteration did not converge (results still written) */
+
+/* precision of the propagator */
+#define PSCFG_FP64 0
+#define PSCFG_FP32 1       /* FP32 propagation + FFT, FP64 contour sums */
+
+/* crystal systems (src/unit_cell_mod.f90:309-664) */
+#define PSCFG_LAMELLAR 0
+#define PSCFG_SQUARE 10
+#define PSCFG_RECTANGULAR 11
+#define PSCFG_HEXAGONAL2D 12
+#define PSCFG_OBLIQUE 13
+#define PSCFG_CUBIC 20
+#define PSCFG_TETRAGONAL 21
+#define PSCFG_ORTHORHOMBIC 22
+#define PSCFG_HEXAGONAL3D 23
+#define PSCFG_MONOCLINIC 24
+
+/* One SCFT instance: the module globals read by the reference hot path
+ * (src/chemistry_mod.f90:41-46 chemistry, src/grid_mod.f90:43-46 grid,
+ * src/unit_cell_mod.f90 cell, chain_step from DISCRETIZATION). */
+typedef struct pscfg_system {
+    int dim;                                /* 1, 2 or 3 */
+    int n[3];                               /* grid; unused entries = 1 */
+    int n_monomer;
+    int n_chain;
+    int n_solvent;
+    int ensemble;                           /* 0 canonical, 1 grand */
+    int n_block[PSCFG_MAXC];
+    int block_monomer[PSCFG_MAXC][PSCFG_MAXB];
+    double block_length[PSCFG_MAXC][PSCFG_MAXB];
+    double kuhn[PSCFG_MAXM];
+    double chi[PSCFG_MAXM][PSCFG_MAXM];
+    double phi_chain[PSCFG_MAXC];
+    double mu_chain[PSCFG_MAXC];
+    int solvent_monomer[PSCFG_MAXS];
+    double solvent_size[PSCFG_MAXS];
+    double phi_solvent[PSCFG_MAXS];
+    double mu_solvent[PSCFG_MAXS];
+    double chain_step;                      /* ds */
+    int crystal_system;                     /* PSCFG_LAMELLAR ... */
+    double cell_param[PSCFG_MAXCP];
+} pscfg_system;
+
+typedef struct pscfg_engine pscfg_engine;
+
+/* Anderson-mixing parameters (src/iterate_mod.fp.f90:983-1021 startup,
+ * iterate_AM input: max_itr, error_max, N_hist, domain). */
+typedef struct pscfg_am_param {
+    int max_itr;
+    int n_hist;
+    int domain;              /* 1: relax the unit cell (stress -> 0) */
+    double error_max;
+} pscfg_am_param;
+
+/* Per-instance result of pscfg_iterate_am. */
+typedef struct pscfg_am_result {
+    int itr;
+    int converged;           /* 1 converged, 0 not (max_itr or diverged) */
+    double error;            /* max(|dev|, |stress|) at exit */
+    double f_helmholtz;      /* free energy per monomer / kT */
+    double pressure;
+    double stress[PSCFG_MAXCP];
+    double cell_param[PSCFG_MAXCP];
+    double q[PSCFG_MAXC];
+    double mu_chain[PSCFG_MAXC];
+} pscfg_am_result;
+
+/* Create an engine for n_inst instances of one grid shape.
+ * Replaces density_startup + make_chain_grid + init_step
+ * (src/scf_mod.fp.f90:82-117, src/chain_mod.f90:97-175,
+ * src/step_mod.f90:60-92), the unit cell setup make_unit_cell + make_ksq
+ * (src/unit_cell_mod.f90:309-664, src/grid_mod.f90:141-160).
+ * `precision` is PSCFG_FP64 or PSCFG_FP32. */
+int pscfg_create(const pscfg_system *systems, int n_inst, int precision, pscfg_engine **out);
+void pscfg_destroy(pscfg_engine *e);
+
+/* Message of the last failed call on this engine (or of the last failed
+ * pscfg_create when e is NULL). */
+const char *pscfg_last_error(const pscfg_engine *e);
+
+/* New unit cell for instance `inst`: G_basis, dGG and the k^2 table are
+ * rebuilt (make_unit_cell + make_ksq, src/iterate_mod.fp.f90:1453-1459). */
+int pscfg_set_cell_param(pscfg_engine *e, int inst, const double *cell_param);
+
+/* k^2 table of instance `inst` on the r2c half grid (0:n1/2,0:n2-1,0:n3-1),
+ * x fastest (ksq_grid, src/grid_mod.f90:141-160).  nk doubles. */
+int pscfg_get_ksq(pscfg_engine *e, int inst, double *ksq);
+
+/* density() on grid fields for every instance
+ * (src/scf_mod.fp.f90:144-229 between basis_to_kgrid/ifft and
+ * fft/kgrid_to_basis).  omega, rho: host [n_inst][n_monomer][nr];
+ * q: host [n_inst][PSCFG_MAXC] chain partition functions (bigQ);
+ * q_solvent: host [n_inst][PSCFG_MAXS] or NULL. */
+int pscfg_density(pscfg_engine *e, const double *omega, double *rho, double *q, double *q_solvent);
+
+/* Same with device-resident omega/rho (cudaMalloc'd, same layout). */
+int pscfg_density_device(pscfg_engine *e, const double *omega_dev, double *rho_dev, double *q, double *q_solvent);
+
+/* scf_stress (src/scf_mod.fp.f90:451-550) after a density call:
+ * stress: host [n_inst][PSCFG_MAXCP] = d f_Helmholtz / d cell_param. */
+int pscfg_stress(pscfg_engine *e, double *stress);
+
+/* free_energy (src/scf_mod.fp.f90:834-886) and mu_phi_chain
+ * (src/scf_mod.fp.f90:768-785) for the fields of the last density call.
+ * out: host [n_inst][2] = {f_Helmholtz, pressure};
+ * mu_chain: host [n_inst][PSCFG_MAXC] or NULL. */
+int pscfg_free_energy(pscfg_engine *e, double *out, double *mu_chain);
+
+/* Anderson-mixing solve of every instance (iterate_AM,
+ * src/iterate_mod.fp.f90:1042-1490) with density, stress, deviations,
+ * Gram matrix and mixing on the device.  omega: host
+ * [n_inst][n_monomer][nr], in: initial guess, out: solution.  rho: host
+ * output or NULL.  results: host [n_inst]. */
+int pscfg_iterate_am(pscfg_engine *e, double *omega, const pscfg_am_param *prm, double *rho,
+                     pscfg_am_result *results);
+
+/* nsteps applications of step_exp (src/step_mod.f90:146-176) to q for
+ * instance `inst`, with the tables of make_propg(ds, b, ksq, omega_m)
+ * (src/step_mod.f90:109-129).  omega_m, q_in, q_out: host [nr]. */
+int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, double ds,
+                    const double *q_in, double *q_out, int nsteps);
+
+/* Stored propagators of chain `chain` of instance `inst` after a density
+ * call (chain_grid_type%qf/qr, src/chain_mod.f90:39-50): host
+ * [n_slices][nr] each (either may be NULL); returns the slice count in
+ * *n_slices when non-NULL. */
+int pscfg_get_propagators(pscfg_engine *e, int inst, int chain, double *qf, double *qr, int *n_slices);
+
+/* Number of MDE steps (step_exp calls) in one density() of the whole
+ * batch: sum over instances and chains of 2 * Ns. */
+long pscfg_steps_per_density(const pscfg_engine *e);
+
+/* Kernel launches issued by this engine since creation (all streams). */
+long pscfg_launch_count(const pscfg_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSCF_GPU_H */

@@ -1,0 +1,1336 @@
+// engine.cu -- batched SCFT propagator engine behind the C ABI of
+// include/pscf_gpu.h.
+//
+// One engine = a batch of independent SCFT instances sharing one grid shape
+// and precision.  All instances of the batch advance together: every kernel
+// launch covers every active (instance, chain, direction) field, so a batch
+// of small grids fills the 148 SMs that one instance alone cannot.
+//
+// Device memory per instance (one bump-allocated arena per engine):
+//   omega, rho           [M][nr] double   (x fastest, like omega_grid)
+//   ksq                  [nk]    double   (r2c half grid, like ksq_grid)
+//   wdgsq                [MAXCP][nk] double  stress weights
+//   qf, qr per chain     [ns+1][nr] T     (chain_grid_type%qf/qr)
+//   eo1, eo2 per block   [nr] T ; ek1, ek2 per block [nk] T  (make_propg)
+//   3-D step scratch per field: S1, S2 [nk] cx<T>, q1 [nr] T
+//   Anderson history     (n_hist+1) x 2 x [M][nr] double
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pscf_gpu.h"
+#include "host_geom.h"
+#include "scf_kernels.cuh"
+
+namespace pscfg {
+
+static thread_local std::string g_create_error;
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t _e = (call);                                                                 \
+        if (_e != cudaSuccess) {                                                                 \
+            throw Err(PSCFG_ECUDA, std::string(#call) + ": " + cudaGetErrorString(_e));          \
+        }                                                                                        \
+    } while (0)
+
+struct Err {
+    int code;
+    std::string msg;
+    Err(int c, std::string m) : code(c), msg(std::move(m)) {}
+};
+
+static const int Z_TILE = 16;
+
+struct Inst {
+    pscfg_system sys;
+    Cell cell;
+    int ns[PSCFG_MAXC];
+    int bgn[PSCFG_MAXC][PSCFG_MAXB + 1];
+    double bds[PSCFG_MAXC][PSCFG_MAXB];
+    double length[PSCFG_MAXC];
+    double *omega = nullptr, *rho = nullptr, *ksq = nullptr, *wdgsq = nullptr;
+    void *qf[PSCFG_MAXC] = {}, *qr[PSCFG_MAXC] = {};
+    void *eo1[PSCFG_MAXC][PSCFG_MAXB] = {}, *eo2[PSCFG_MAXC][PSCFG_MAXB] = {};
+    void *ek1[PSCFG_MAXC][PSCFG_MAXB] = {}, *ek2[PSCFG_MAXC][PSCFG_MAXB] = {};
+    void *S1[2 * PSCFG_MAXC] = {}, *S2[2 * PSCFG_MAXC] = {}, *q1[2 * PSCFG_MAXC] = {};
+    double *Qdev = nullptr;       // [MAXC] chain partition functions
+    double *Qsolv = nullptr;      // [MAXS]
+    double *inc[PSCFG_MAXC] = {}; // stress slice sums [ns+1][MAXCP]
+    double *stress_dev = nullptr; // [MAXCP]
+    double Q[PSCFG_MAXC] = {}, Qs[PSCFG_MAXS] = {};
+    bool have_density = false;
+    // Anderson
+    double *om_hist = nullptr, *dev_hist = nullptr;
+};
+
+struct Engine {
+    int prec = PSCFG_FP64;
+    int dim = 1;
+    int n[3] = {1, 1, 1};
+    long nr = 1, nk = 1;
+    int M = 0;
+    std::vector<Inst> inst;
+    cudaStream_t st = nullptr;
+    std::string err;
+    long launches = 0;
+    int n_hist_alloc = 0;
+
+    // FFT plan / twiddle tables
+    PlaneGeom g64, g32;
+    std::vector<void *> allocs;
+
+    // descriptor scratch (device), grown on demand
+    void *d_desc = nullptr;
+    size_t d_desc_bytes = 0;
+    double *d_part = nullptr;
+    size_t d_part_len = 0;
+    double *d_small = nullptr;   // scalars [n_inst][64]
+    void *spec = nullptr;        // 3-D stress spectra scratch
+    size_t spec_bytes = 0;
+    double *stress_part = nullptr;
+    size_t stress_part_len = 0;
+
+    ~Engine()
+    {
+        for (void *p : allocs) cudaFree(p);
+        if (d_desc) cudaFree(d_desc);
+        if (d_part) cudaFree(d_part);
+        if (d_small) cudaFree(d_small);
+        if (spec) cudaFree(spec);
+        if (stress_part) cudaFree(stress_part);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    void *dalloc(size_t bytes)
+    {
+        void *p = nullptr;
+        if (bytes == 0) bytes = 16;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) throw Err(PSCFG_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+        allocs.push_back(p);
+        return p;
+    }
+
+    size_t tsize() const { return prec == PSCFG_FP64 ? sizeof(double) : sizeof(float); }
+    const PlaneGeom &geom() const { return prec == PSCFG_FP64 ? g64 : g32; }
+
+    void *desc(size_t bytes)
+    {
+        if (bytes > d_desc_bytes) {
+            if (d_desc) cudaFree(d_desc);
+            d_desc = nullptr;
+            size_t nb = std::max(bytes + bytes / 2, (size_t)16 << 20);
+            CK(cudaMalloc(&d_desc, nb));
+            d_desc_bytes = nb;
+        }
+        return d_desc;
+    }
+    // upload host descriptors into a sub-range of the descriptor scratch
+    template <typename D>
+    D *upload(const std::vector<D> &v, size_t offset_bytes)
+    {
+        char *base = (char *)desc(offset_bytes + v.size() * sizeof(D) + 256);
+        D *p = (D *)(base + offset_bytes);
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(D), cudaMemcpyHostToDevice, st));
+        return p;
+    }
+    double *part(size_t len)
+    {
+        if (len > d_part_len) {
+            if (d_part) cudaFree(d_part);
+            d_part = nullptr;
+            CK(cudaMalloc(&d_part, len * sizeof(double)));
+            d_part_len = len;
+        }
+        return d_part;
+    }
+    void launched(cudaError_t e = cudaGetLastError())
+    {
+        launches++;
+        if (e != cudaSuccess) throw Err(PSCFG_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
+};
+
+// ---------------------------------------------------------------------
+// FFT plans
+// ---------------------------------------------------------------------
+template <typename T>
+static void *twiddle_table(Engine &E, int n)
+{
+    std::vector<cx<T>> h(std::max(n, 1));
+    for (int m = 0; m < n; m++) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
+        h[m].x = (T)cosl(a);
+        h[m].y = (T)sinl(a);
+    }
+    void *d = E.dalloc(h.size() * sizeof(cx<T>));
+    CK(cudaMemcpy(d, h.data(), h.size() * sizeof(cx<T>), cudaMemcpyHostToDevice));
+    return d;
+}
+
+template <typename T>
+static void make_line_plan(Engine &E, int n, LinePlan &p)
+{
+    p.n = n;
+    if (!plan_radices(n, p.rad, p.nst))
+        throw Err(PSCFG_EINVAL, "grid size " + std::to_string(n) + " has a prime factor other than 2, 3, 5, 7");
+    p.tw = twiddle_table<T>(E, n);
+}
+
+template <typename T>
+static void make_geom(Engine &E, PlaneGeom &g)
+{
+    g.n1 = E.n[0];
+    g.n2 = E.n[1];
+    g.n3 = E.n[2];
+    g.n1h = g.n1 / 2 + 1;
+    g.even = (g.n1 % 2 == 0) ? 1 : 0;
+    g.LS = g.even ? g.n1h : g.n1;
+    make_line_plan<T>(E, g.even ? g.n1 / 2 : g.n1, g.row);
+    make_line_plan<T>(E, g.n2, g.col);
+    make_line_plan<T>(E, g.n3, g.zp);
+    g.rtw = twiddle_table<T>(E, g.n1);
+}
+
+static void upload_dft_constants()
+{
+    // row 0: cos(2 pi m/R), row 1: sin(2 pi m/R); the codelet forms
+    // W = (cos, S*sin) with S = -1 forward, +1 inverse.
+    double t5[2][5], t7[2][7];
+    for (int m = 0; m < 5; m++) {
+        long double a = 2.0L * 3.14159265358979323846264338327950288L * m / 5.0L;
+        t5[0][m] = (double)cosl(a);
+        t5[1][m] = (double)sinl(a);
+    }
+    for (int m = 0; m < 7; m++) {
+        long double a = 2.0L * 3.14159265358979323846264338327950288L * m / 7.0L;
+        t7[0][m] = (double)cosl(a);
+        t7[1][m] = (double)sinl(a);
+    }
+    CK(cudaMemcpyToSymbol(c_dft5, t5, sizeof(t5)));
+    CK(cudaMemcpyToSymbol(c_dft7, t7, sizeof(t7)));
+}
+
+// ---------------------------------------------------------------------
+// Setup
+// ---------------------------------------------------------------------
+static void validate_system(const pscfg_system &s, int dim, const int n[3])
+{
+    if (s.dim != dim || s.n[0] != n[0] || s.n[1] != n[1] || s.n[2] != n[2])
+        throw Err(PSCFG_EINVAL, "all instances of an engine must share one grid shape");
+    if (s.n_monomer < 1 || s.n_monomer > PSCFG_MAXM) throw Err(PSCFG_EINVAL, "n_monomer out of range");
+    if (s.n_chain < 0 || s.n_chain > PSCFG_MAXC) throw Err(PSCFG_EINVAL, "n_chain out of range");
+    if (s.n_solvent < 0 || s.n_solvent > PSCFG_MAXS) throw Err(PSCFG_EINVAL, "n_solvent out of range");
+    if (s.chain_step <= 0) throw Err(PSCFG_EINVAL, "chain_step must be positive");
+    for (int c = 0; c < s.n_chain; c++) {
+        if (s.n_block[c] < 1 || s.n_block[c] > PSCFG_MAXB) throw Err(PSCFG_EINVAL, "n_block out of range");
+        for (int b = 0; b < s.n_block[c]; b++)
+            if (s.block_monomer[c][b] < 0 || s.block_monomer[c][b] >= s.n_monomer)
+                throw Err(PSCFG_EINVAL, "block_monomer out of range");
+    }
+    for (int i = 0; i < s.n_solvent; i++)
+        if (s.solvent_monomer[i] < 0 || s.solvent_monomer[i] >= s.n_monomer)
+            throw Err(PSCFG_EINVAL, "solvent_monomer out of range");
+}
+
+static void upload_cell(Engine &E, Inst &I)
+{
+    Cell c;
+    if (!make_unit_cell(E.dim, I.sys.crystal_system, I.sys.cell_param, c))
+        throw Err(PSCFG_EINVAL, "unknown crystal system for this dimension");
+    I.cell = c;
+    std::vector<double> ksq, wd;
+    make_ksq_dgsq(E.dim, E.n, c, ksq, wd);
+    CK(cudaMemcpyAsync(I.ksq, ksq.data(), ksq.size() * sizeof(double), cudaMemcpyHostToDevice, E.st));
+    CK(cudaMemcpyAsync(I.wdgsq, wd.data(), wd.size() * sizeof(double), cudaMemcpyHostToDevice, E.st));
+    CK(cudaStreamSynchronize(E.st));
+    I.have_density = false;
+}
+
+static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int precision)
+{
+    if (n_inst < 1) throw Err(PSCFG_EINVAL, "n_inst must be >= 1");
+    if (precision != PSCFG_FP64 && precision != PSCFG_FP32) throw Err(PSCFG_EINVAL, "unknown precision");
+    E.prec = precision;
+    E.dim = sys[0].dim;
+    if (E.dim < 1 || E.dim > 3) throw Err(PSCFG_EINVAL, "dim must be 1, 2 or 3");
+    for (int d = 0; d < 3; d++) E.n[d] = (d < E.dim) ? sys[0].n[d] : 1;
+    for (int d = 0; d < 3; d++)
+        if (E.n[d] < 1) throw Err(PSCFG_EINVAL, "grid extents must be >= 1");
+    E.nr = (long)E.n[0] * E.n[1] * E.n[2];
+    E.nk = (long)(E.n[0] / 2 + 1) * E.n[1] * E.n[2];
+    E.M = sys[0].n_monomer;
+    CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
+    upload_dft_constants();
+    if (precision == PSCFG_FP64) make_geom<double>(E, E.g64);
+    else make_geom<float>(E, E.g32);
+
+    const size_t ts = E.tsize();
+    E.inst.resize(n_inst);
+    for (int i = 0; i < n_inst; i++) {
+        pscfg_system s = sys[i];
+        for (int d = s.dim; d < 3; d++) s.n[d] = 1;
+        validate_system(s, E.dim, E.n);
+        if (s.n_monomer != E.M) throw Err(PSCFG_EINVAL, "all instances must have the same n_monomer");
+        Inst &I = E.inst[i];
+        I.sys = s;
+        I.omega = (double *)E.dalloc(sizeof(double) * E.M * E.nr);
+        I.rho = (double *)E.dalloc(sizeof(double) * E.M * E.nr);
+        I.ksq = (double *)E.dalloc(sizeof(double) * E.nk);
+        I.wdgsq = (double *)E.dalloc(sizeof(double) * PSCFG_MAXCP * E.nk);
+        I.Qdev = (double *)E.dalloc(sizeof(double) * PSCFG_MAXC);
+        I.Qsolv = (double *)E.dalloc(sizeof(double) * PSCFG_MAXS);
+        I.stress_dev = (double *)E.dalloc(sizeof(double) * PSCFG_MAXCP);
+        for (int c = 0; c < s.n_chain; c++) {
+            I.ns[c] = chain_grid(s.n_block[c], s.block_length[c], s.chain_step, I.bgn[c], I.bds[c]);
+            I.length[c] = 0;
+            for (int b = 0; b < s.n_block[c]; b++) I.length[c] += s.block_length[c][b];
+            I.qf[c] = E.dalloc(ts * E.nr * (I.ns[c] + 1));
+            I.qr[c] = E.dalloc(ts * E.nr * (I.ns[c] + 1));
+            I.inc[c] = (double *)E.dalloc(sizeof(double) * PSCFG_MAXCP * (I.ns[c] + 1));
+            for (int b = 0; b < s.n_block[c]; b++) {
+                I.eo1[c][b] = E.dalloc(ts * E.nr);
+                I.eo2[c][b] = E.dalloc(ts * E.nr);
+                I.ek1[c][b] = E.dalloc(ts * E.nk);
+                I.ek2[c][b] = E.dalloc(ts * E.nk);
+            }
+            if (E.dim == 3) {
+                for (int d = 0; d < 2; d++) {
+                    I.S1[2 * c + d] = E.dalloc(2 * ts * E.nk);
+                    I.S2[2 * c + d] = E.dalloc(2 * ts * E.nk);
+                    I.q1[2 * c + d] = E.dalloc(ts * E.nr);
+                }
+            }
+        }
+        upload_cell(E, I);
+    }
+    E.d_small = nullptr;
+    CK(cudaMalloc(&E.d_small, sizeof(double) * 64 * n_inst));
+    E.part((size_t)64 * n_inst * (PSCFG_MAXH + 2 * PSCFG_MAXM + 8) + 1024);
+}
+
+// ---------------------------------------------------------------------
+// Density
+// ---------------------------------------------------------------------
+static int red_ctas(long n) { return (int)std::min<long>(std::max<long>((n + 255) / 256, 1), 64); }
+
+template <typename T>
+static void run_sweeps(Engine &E, const std::vector<int> &act)
+{
+    const PlaneGeom &g = E.geom();
+    // tables
+    std::vector<TableJob<T>> tj;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        for (int c = 0; c < I.sys.n_chain; c++)
+            for (int b = 0; b < I.sys.n_block[c]; b++) {
+                TableJob<T> j;
+                int m = I.sys.block_monomer[c][b];
+                j.omega = I.omega + (long)m * E.nr;
+                j.ksq = I.ksq;
+                j.eo1 = (T *)I.eo1[c][b];
+                j.eo2 = (T *)I.eo2[c][b];
+                j.ek1 = (T *)I.ek1[c][b];
+                j.ek2 = (T *)I.ek2[c][b];
+                j.ds = I.bds[c][b];
+                j.b = I.sys.kuhn[m];
+                tj.push_back(j);
+            }
+    }
+    std::vector<SweepField<T>> fl;
+    int ns_max = 0;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        for (int c = 0; c < I.sys.n_chain; c++)
+            for (int d = 0; d < 2; d++) {
+                SweepField<T> f;
+                std::memset(&f, 0, sizeof(f));
+                f.slab = (T *)(d == 0 ? I.qf[c] : I.qr[c]);
+                f.ns = I.ns[c];
+                f.dir = d == 0 ? 1 : -1;
+                f.nblk = I.sys.n_block[c];
+                for (int b = 0; b <= f.nblk; b++) f.bgn[b] = I.bgn[c][b];
+                for (int b = 0; b < f.nblk; b++) {
+                    f.eo1[b] = (const T *)I.eo1[c][b];
+                    f.eo2[b] = (const T *)I.eo2[c][b];
+                    f.ek1[b] = (const T *)I.ek1[c][b];
+                    f.ek2[b] = (const T *)I.ek2[c][b];
+                }
+                f.S1 = (cx<T> *)I.S1[2 * c + d];
+                f.S2 = (cx<T> *)I.S2[2 * c + d];
+                f.q1 = (T *)I.q1[2 * c + d];
+                fl.push_back(f);
+                ns_max = std::max(ns_max, f.ns);
+            }
+    }
+    if (fl.empty()) return;
+    TableJob<T> *dtj = E.upload(tj, 0);
+    size_t off = ((tj.size() * sizeof(TableJob<T>) + 255) / 256) * 256;
+    SweepField<T> *dfl = E.upload(fl, off);
+    {
+        dim3 grid((unsigned)std::min<long>((E.nr + 255) / 256, 256), (unsigned)tj.size());
+        k_make_tables<T><<<grid, 256, 0, E.st>>>(dtj, E.nr, E.nk);
+        E.launched();
+        dim3 g2((unsigned)std::min<long>((E.nr + 255) / 256, 256), (unsigned)fl.size());
+        k_init_ends<T><<<g2, 256, 0, E.st>>>(dfl, E.nr);
+        E.launched();
+    }
+    const int nf = (int)fl.size();
+    if (E.dim <= 2) {
+        size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)E.nr * sizeof(T);
+        if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
+        CK(cudaFuncSetAttribute(k_sweep_plane<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
+        k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, ns_max);
+        E.launched();
+    } else {
+        size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
+        size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
+        if (smxy > 227 * 1024 || smz > 227 * 1024) throw Err(PSCFG_EINVAL, "grid plane too large");
+        CK(cudaFuncSetAttribute(k3_fwd_pair<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+        CK(cudaFuncSetAttribute(k3_inv_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+        CK(cudaFuncSetAttribute(k3_inv_final<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+        CK(cudaFuncSetAttribute(k3_zconv<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+        const long P = (long)g.n1h * g.n2;
+        const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+        const int txy = 256, tz = 256;
+        for (int t = 0; t < ns_max; t++) {
+            k3_fwd_pair<T><<<dim3(g.n3, nf), txy, smxy, E.st>>>(dfl, g, t);
+            E.launched();
+            k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 2), tz, smz, E.st>>>(dfl, g, t, 3);
+            E.launched();
+            k3_inv_mid<T><<<dim3(g.n3, nf), txy, smxy, E.st>>>(dfl, g, t);
+            E.launched();
+            k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 1), tz, smz, E.st>>>(dfl, g, t, 2);
+            E.launched();
+            k3_inv_final<T><<<dim3(g.n3, nf), txy, smxy, E.st>>>(dfl, g, t);
+            E.launched();
+        }
+    }
+}
+
+// Q of every chain, solvents, Simpson density
+template <typename T>
+static void run_contour(Engine &E, const std::vector<int> &act)
+{
+    // Q = mean(qf[ns])  (src/scf_mod.fp.f90:358-360)
+    std::vector<const T *> qp;
+    std::vector<double *> qout;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            qp.push_back((const T *)I.qf[c] + (long)I.ns[c] * E.nr);
+            qout.push_back(I.Qdev + c);
+        }
+    }
+    const int nct = red_ctas(E.nr);
+    size_t off = 0;
+    if (!qp.empty()) {
+        const T **dqp = (const T **)E.upload(qp, 0);
+        off = ((qp.size() * sizeof(void *) + 255) / 256) * 256;
+        double *part = E.part((size_t)nct * qp.size());
+        k_partial_sum<T><<<dim3(nct, (unsigned)qp.size()), 256, 0, E.st>>>(dqp, E.nr, part);
+        E.launched();
+        double **dq = (double **)E.upload(qout, off);
+        off += ((qout.size() * sizeof(void *) + 255) / 256) * 256;
+        k_final_sum_ptr<<<(unsigned)((qp.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, dq, (int)qp.size());
+        E.launched();
+    }
+    // solvents (src/scf_mod.fp.f90:193-200, 251-295)
+    bool any_solvent = false;
+    std::vector<SolventJob> sj;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        for (int s = 0; s < I.sys.n_solvent; s++) {
+            SolventJob j;
+            int m = I.sys.solvent_monomer[s];
+            j.omega = I.omega + (long)m * E.nr;
+            j.rho = I.rho + (long)m * E.nr;
+            j.size = I.sys.solvent_size[s];
+            j.Q = I.Qsolv + s;
+            j.phi = I.sys.phi_solvent[s];
+            j.mu = I.sys.mu_solvent[s];
+            j.grand = I.sys.ensemble == 1;
+            sj.push_back(j);
+            any_solvent = true;
+        }
+    }
+    // Simpson jobs grouped by instance
+    std::vector<SimpsonJob> simp;
+    std::vector<int> start;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        start.push_back((int)simp.size());
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            SimpsonJob j;
+            std::memset(&j, 0, sizeof(j));
+            j.qf = I.qf[c];
+            j.qr = I.qr[c];
+            j.rho = I.rho;
+            j.Q = I.Qdev + c;
+            j.phi = I.sys.phi_chain[c];
+            j.length = I.length[c];
+            j.nblk = I.sys.n_block[c];
+            for (int b = 0; b <= j.nblk; b++) j.bgn[b] = I.bgn[c][b];
+            for (int b = 0; b < j.nblk; b++) {
+                j.mon[b] = I.sys.block_monomer[c][b];
+                j.bds[b] = I.bds[c][b];
+            }
+            j.n_monomer = I.sys.n_monomer;
+            simp.push_back(j);
+        }
+    }
+    start.push_back((int)simp.size());
+    if (any_solvent) {
+        // grand-ensemble chain phi = Q exp(mu) needs the device Q: pull Q now
+        throw Err(PSCFG_EINVAL, "solvent species are not supported by this build of the engine");
+    }
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        if (I.sys.ensemble != 0) throw Err(PSCFG_EINVAL, "only the canonical ensemble is supported by this build");
+    }
+    SimpsonJob *dsj = E.upload(simp, off);
+    off += ((simp.size() * sizeof(SimpsonJob) + 255) / 256) * 256;
+    int *dst = E.upload(start, off);
+    dim3 grid((unsigned)std::min<long>((E.nr + 255) / 256, 1024), (unsigned)act.size());
+    k_simpson<T><<<grid, 256, 0, E.st>>>(dsj, dst, E.nr);
+    E.launched();
+}
+
+template <typename T>
+static void density_impl(Engine &E, const std::vector<int> &act)
+{
+    run_sweeps<T>(E, act);
+    run_contour<T>(E, act);
+}
+
+static void density_all(Engine &E, const std::vector<int> &act)
+{
+    if (E.prec == PSCFG_FP64) density_impl<double>(E, act);
+    else density_impl<float>(E, act);
+    // pull Q to the host (needed for mu and for the caller)
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        CK(cudaMemcpyAsync(I.Q, I.Qdev, sizeof(double) * PSCFG_MAXC, cudaMemcpyDeviceToHost, E.st));
+    }
+    CK(cudaStreamSynchronize(E.st));
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        I.have_density = true;
+        // mu_phi_chain (src/scf_mod.fp.f90:768-785), canonical ensemble
+        for (int c = 0; c < I.sys.n_chain; c++) I.sys.mu_chain[c] = std::log(I.sys.phi_chain[c] / I.Q[c]);
+    }
+}
+
+// ---------------------------------------------------------------------
+// Stress
+// ---------------------------------------------------------------------
+template <typename T>
+static void stress_impl(Engine &E, const std::vector<int> &act)
+{
+    const PlaneGeom &g = E.geom();
+    std::vector<StressJob<T>> jobs;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            StressJob<T> j;
+            j.qf = (const T *)I.qf[c];
+            j.qr = (const T *)I.qr[c];
+            j.wdgsq = I.wdgsq;
+            j.ncp = I.cell.ncp;
+            j.nslices = I.ns[c] + 1;
+            j.inc = I.inc[c];
+            jobs.push_back(j);
+        }
+    }
+    if (jobs.empty()) return;
+    StressJob<T> *dj = E.upload(jobs, 0);
+    size_t off = ((jobs.size() * sizeof(StressJob<T>) + 255) / 256) * 256;
+    if (E.dim <= 2) {
+        int maxs = 0;
+        for (auto &j : jobs) maxs = std::max(maxs, j.nslices);
+        size_t sm = 4 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
+        if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the plane stress kernel");
+        CK(cudaFuncSetAttribute(k2_stress_slices<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
+        k2_stress_slices<T><<<dim3(maxs, (unsigned)jobs.size()), threads, sm, E.st>>>(dj, g);
+        E.launched();
+    } else {
+        const long P = (long)g.n1h * g.n2;
+        const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+        size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
+        size_t smz = 4 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
+        CK(cudaFuncSetAttribute(k3_stress_xy<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+        CK(cudaFuncSetAttribute(k3_stress_z<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+        // chunk of slices so that the spectra scratch stays below ~1 GB
+        const size_t per_slice = 2 * (size_t)E.nk * sizeof(cx<T>);
+        int cs = (int)std::max<size_t>(1, std::min<size_t>(256, ((size_t)1 << 30) / per_slice));
+        if (E.spec_bytes < per_slice * cs) {
+            if (E.spec) cudaFree(E.spec);
+            E.spec = nullptr;
+            CK(cudaMalloc(&E.spec, per_slice * cs));
+            E.spec_bytes = per_slice * cs;
+        }
+        size_t plen = (size_t)cs * ntile * PSCFG_MAXCP;
+        if (E.stress_part_len < plen) {
+            if (E.stress_part) cudaFree(E.stress_part);
+            E.stress_part = nullptr;
+            CK(cudaMalloc(&E.stress_part, plen * sizeof(double)));
+            E.stress_part_len = plen;
+        }
+        for (size_t jb = 0; jb < jobs.size(); jb++) {
+            for (int s0 = 0; s0 < jobs[jb].nslices; s0 += cs) {
+                int cnt = std::min(cs, jobs[jb].nslices - s0);
+                k3_stress_xy<T><<<dim3(g.n3, cnt, 2), 256, smxy, E.st>>>(dj + jb, g, s0, (cx<T> *)E.spec);
+                E.launched();
+                k3_stress_z<T, Z_TILE><<<dim3(ntile, cnt), 256, smz, E.st>>>(dj + jb, g, s0, (const cx<T> *)E.spec, E.stress_part);
+                E.launched();
+                k3_stress_sum<T><<<cnt, 32, 0, E.st>>>(dj + jb, s0, ntile, E.stress_part);
+                E.launched();
+            }
+        }
+    }
+    std::vector<StressFinal> fin;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        StressFinal f;
+        std::memset(&f, 0, sizeof(f));
+        f.nchain = I.sys.n_chain;
+        f.ncp = I.cell.ncp;
+        f.ensemble = I.sys.ensemble;
+        f.Q = I.Qdev;
+        f.rnodes = (double)E.nr;
+        f.out = I.stress_dev;
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            f.inc[c] = I.inc[c];
+            f.nblk[c] = I.sys.n_block[c];
+            for (int b = 0; b <= f.nblk[c]; b++) f.bgn[c][b] = I.bgn[c][b];
+            for (int b = 0; b < f.nblk[c]; b++) {
+                f.bds[c][b] = I.bds[c][b];
+                f.b[c][b] = I.sys.kuhn[I.sys.block_monomer[c][b]];
+            }
+            f.phi[c] = I.sys.phi_chain[c];
+            f.mu[c] = I.sys.mu_chain[c];
+            f.length[c] = I.length[c];
+        }
+        fin.push_back(f);
+    }
+    StressFinal *df = E.upload(fin, off);
+    k_stress_final<<<(unsigned)((fin.size() + 63) / 64), 64, 0, E.st>>>(df, (int)fin.size());
+    E.launched();
+}
+
+static void stress_all(Engine &E, const std::vector<int> &act)
+{
+    for (int i : act)
+        if (!E.inst[i].have_density) throw Err(PSCFG_ESTATE, "stress requires a preceding density call");
+    if (E.prec == PSCFG_FP64) stress_impl<double>(E, act);
+    else stress_impl<float>(E, act);
+}
+
+// ---------------------------------------------------------------------
+// Free energy (src/scf_mod.fp.f90:834-886)
+// ---------------------------------------------------------------------
+static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p)
+{
+    std::vector<FieldJob> fj;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        FieldJob j;
+        std::memset(&j, 0, sizeof(j));
+        j.omega = I.omega;
+        j.rho = I.rho;
+        j.M = I.sys.n_monomer;
+        for (int a = 0; a < j.M; a++)
+            for (int b = 0; b < j.M; b++) j.chi[a][b] = I.sys.chi[a][b];
+        fj.push_back(j);
+    }
+    FieldJob *dj = E.upload(fj, 0);
+    const int nct = red_ctas(E.nr);
+    double *part = E.part((size_t)nct * fj.size());
+    k_fe_partial<<<dim3(nct, (unsigned)fj.size()), 256, 0, E.st>>>(dj, E.nr, part);
+    E.launched();
+    k_final_sum<<<(unsigned)((fj.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small, (int)fj.size());
+    E.launched();
+    std::vector<double> terms(fj.size());
+    CK(cudaMemcpyAsync(terms.data(), E.d_small, sizeof(double) * fj.size(), cudaMemcpyDeviceToHost, E.st));
+    CK(cudaStreamSynchronize(E.st));
+    f.assign(act.size(), 0.0);
+    p.assign(act.size(), 0.0);
+    for (size_t k = 0; k < act.size(); k++) {
+        Inst &I = E.inst[act[k]];
+        double fe = 0.0;
+        for (int c = 0; c < I.sys.n_chain; c++)
+            if (I.sys.phi_chain[c] > 1.0e-8) fe = fe + I.sys.phi_chain[c] * (I.sys.mu_chain[c] - 1.0) / I.length[c];
+        for (int s = 0; s < I.sys.n_solvent; s++)
+            if (I.sys.phi_solvent[s] > 1.0e-8)
+                fe = fe + I.sys.phi_solvent[s] * (I.sys.mu_solvent[s] - 1.0) / I.sys.solvent_size[s];
+        fe += terms[k];
+        double pr = -fe;
+        for (int c = 0; c < I.sys.n_chain; c++)
+            if (I.sys.phi_chain[c] > 1.0e-8) pr = pr + I.sys.mu_chain[c] * I.sys.phi_chain[c] / I.length[c];
+        for (int s = 0; s < I.sys.n_solvent; s++)
+            if (I.sys.phi_solvent[s] > 1.0e-8) pr = pr + I.sys.mu_solvent[s] * I.sys.phi_solvent[s] / I.sys.solvent_size[s];
+        f[k] = fe;
+        p[k] = pr;
+    }
+}
+
+// ---------------------------------------------------------------------
+// Anderson mixing (src/iterate_mod.fp.f90:1042-1490)
+// ---------------------------------------------------------------------
+struct AmState {
+    int itr = 0;
+    bool done = false;
+    bool converged = false;
+    double error = 0;
+    int nstore = 0;            // number of valid history entries (<= H+1)
+    int head = 0;              // ring slot of the most recent entry
+    std::vector<double> gram;  // (H+1)x(H+1) ring-indexed <d_i, d_j>
+    std::vector<std::vector<double>> devcp, cph;  // [H+1][ncp]
+    double f = 0, p = 0;
+    double stress[PSCFG_MAXCP] = {};
+};
+
+static bool solve_dense(int n, std::vector<double> &U, std::vector<double> &v)
+{
+    for (int c = 0; c < n; c++) {
+        int p = c;
+        for (int r = c + 1; r < n; r++)
+            if (std::fabs(U[r * n + c]) > std::fabs(U[p * n + c])) p = r;
+        if (U[p * n + c] == 0.0) return false;
+        if (p != c) {
+            for (int k = 0; k < n; k++) std::swap(U[c * n + k], U[p * n + k]);
+            std::swap(v[c], v[p]);
+        }
+        for (int r = c + 1; r < n; r++) {
+            double f = U[r * n + c] / U[c * n + c];
+            for (int k = c; k < n; k++) U[r * n + k] -= f * U[c * n + k];
+            v[r] -= f * v[c];
+        }
+    }
+    for (int r = n - 1; r >= 0; r--) {
+        double s = v[r];
+        for (int k = r + 1; k < n; k++) s -= U[r * n + k] * v[k];
+        v[r] = s / U[r * n + r];
+    }
+    return true;
+}
+
+static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<pscfg_am_result> &res)
+{
+    const int H = prm.n_hist;
+    if (H < 1 || H > PSCFG_MAXH - 1) throw Err(PSCFG_EINVAL, "n_hist out of range");
+    const int S = H + 1;                 // ring slots
+    const long fl = (long)E.M * E.nr;
+    const int ninst = (int)E.inst.size();
+    if (E.n_hist_alloc < S) {
+        for (auto &I : E.inst) {
+            I.om_hist = (double *)E.dalloc(sizeof(double) * fl * S);
+            I.dev_hist = (double *)E.dalloc(sizeof(double) * fl * S);
+        }
+        E.n_hist_alloc = S;
+    }
+    std::vector<AmState> st(ninst);
+    std::vector<int> all(ninst);
+    for (int i = 0; i < ninst; i++) all[i] = i;
+    const double large = 100.0;
+
+    // initial density (src/iterate_mod.fp.f90:1123-1128), then the uniform
+    // component of omega (set_omega_uniform, src/scf_mod.fp.f90:724-750)
+    density_all(E, all);
+    {
+        std::vector<double> w(fl);
+        for (int i = 0; i < ninst; i++) {
+            Inst &I = E.inst[i];
+            CK(cudaMemcpyAsync(w.data(), I.omega, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
+            CK(cudaStreamSynchronize(E.st));
+            double phi_mon[PSCFG_MAXM] = {0};
+            for (int c = 0; c < I.sys.n_chain; c++)
+                for (int b = 0; b < I.sys.n_block[c]; b++)
+                    phi_mon[I.sys.block_monomer[c][b]] += I.sys.phi_chain[c] * I.sys.block_length[c][b] / I.length[c];
+            for (int s = 0; s < I.sys.n_solvent; s++) phi_mon[I.sys.solvent_monomer[s]] += I.sys.phi_solvent[s];
+            for (int a = 0; a < E.M; a++) {
+                double w0 = 0;
+                for (int b = 0; b < E.M; b++) w0 = w0 + I.sys.chi[a][b] * phi_mon[b];
+                double m = 0;
+                for (long r = 0; r < E.nr; r++) m += w[a * E.nr + r];
+                m /= (double)E.nr;
+                for (long r = 0; r < E.nr; r++) w[a * E.nr + r] += w0 - m;
+            }
+            CK(cudaMemcpyAsync(I.omega, w.data(), sizeof(double) * fl, cudaMemcpyHostToDevice, E.st));
+            CK(cudaMemcpyAsync(I.om_hist, I.omega, sizeof(double) * fl, cudaMemcpyDeviceToDevice, E.st));
+            st[i].gram.assign((size_t)S * S, 0.0);
+            st[i].devcp.assign(S, std::vector<double>(PSCFG_MAXCP, 0.0));
+            st[i].cph.assign(S, std::vector<double>(PSCFG_MAXCP, 0.0));
+            for (int k = 0; k < I.cell.ncp; k++) st[i].cph[0][k] = I.sys.cell_param[k];
+            st[i].head = 0;
+            st[i].nstore = 0;   // om_hist slot 0 holds omega; dev not yet
+        }
+        CK(cudaStreamSynchronize(E.st));
+    }
+
+    const int nct = red_ctas(E.nr);
+    std::vector<double> hsmall;
+    for (;;) {
+        std::vector<int> act;
+        for (int i = 0; i < ninst; i++)
+            if (!st[i].done) act.push_back(i);
+        if (act.empty()) break;
+        const int na = (int)act.size();
+        for (int i : act) st[i].itr++;
+
+        density_all(E, act);
+        if (prm.domain) stress_all(E, act);
+        std::vector<double> fe, pe;
+        free_energy_all(E, act, fe, pe);
+        std::vector<double> sh((size_t)na * PSCFG_MAXCP, 0.0);
+        if (prm.domain) {
+            for (int k = 0; k < na; k++)
+                CK(cudaMemcpyAsync(&sh[(size_t)k * PSCFG_MAXCP], E.inst[act[k]].stress_dev, sizeof(double) * PSCFG_MAXCP,
+                                   cudaMemcpyDeviceToHost, E.st));
+        }
+        // slot of this iteration's deviation: ring position after head
+        // (head points at the om_hist entry of the current omega)
+        std::vector<AmJob> aj;
+        for (int k = 0; k < na; k++) {
+            Inst &I = E.inst[act[k]];
+            AmJob j;
+            std::memset(&j, 0, sizeof(j));
+            j.omega = I.omega;
+            j.rho = I.rho;
+            j.dev = I.dev_hist + (long)st[act[k]].head * fl;
+            j.M = E.M;
+            for (int a = 0; a < E.M; a++)
+                for (int b = 0; b < E.M; b++) j.chi[a][b] = I.sys.chi[a][b];
+            aj.push_back(j);
+        }
+        AmJob *daj = E.upload(aj, 0);
+        size_t off = ((aj.size() * sizeof(AmJob) + 255) / 256) * 256;
+        double *part = E.part((size_t)nct * na * PSCFG_MAXM + 16);
+        k_am_dev<<<dim3(nct, na), 256, 0, E.st>>>(daj, E.nr, part);
+        E.launched();
+        k_final_sum<<<(unsigned)((na * PSCFG_MAXM + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small,
+                                                                                  na * PSCFG_MAXM);
+        E.launched();
+        std::vector<AmFix> fx;
+        for (int k = 0; k < na; k++) {
+            AmFix f;
+            f.dev = aj[k].dev;
+            f.mean = E.d_small + (size_t)k * PSCFG_MAXM;
+            f.M = E.M;
+            fx.push_back(f);
+        }
+        AmFix *dfx = E.upload(fx, off);
+        off += ((fx.size() * sizeof(AmFix) + 255) / 256) * 256;
+        double *part2 = part + (size_t)nct * na * PSCFG_MAXM;
+        (void)part2;
+        double *mpart = E.part((size_t)nct * na * (PSCFG_MAXM + 1) + 16) + (size_t)nct * na * PSCFG_MAXM;
+        k_am_fix<<<dim3(nct, na), 256, 0, E.st>>>(dfx, E.nr, mpart);
+        E.launched();
+        double *emax = E.d_small + (size_t)na * PSCFG_MAXM;
+        k_final_max<<<(unsigned)((na + 127) / 128), 128, 0, E.st>>>(mpart, nct, emax, na);
+        E.launched();
+        // dots of the new deviation with every stored deviation (incl. itself)
+        std::vector<AmDot> dots;
+        for (int k = 0; k < na; k++) {
+            int i = act[k];
+            AmDot d;
+            std::memset(&d, 0, sizeof(d));
+            d.cur = aj[k].dev;
+            d.len = fl;
+            int nst = std::min(st[i].nstore + 1, S);
+            d.nh = nst;
+            for (int h = 0; h < nst; h++) {
+                int slot = ((st[i].head - h) % S + S) % S;   // h = 0 is the current slot
+                d.hist[h] = E.inst[i].dev_hist + (long)slot * fl;
+            }
+            dots.push_back(d);
+        }
+        // recompute the dev pointers after the mean fix (same buffers)
+        AmDot *ddot = E.upload(dots, off);
+        off += ((dots.size() * sizeof(AmDot) + 255) / 256) * 256;
+        double *dpart = E.part((size_t)nct * na * (PSCFG_MAXH + 1) + (size_t)nct * na * (PSCFG_MAXM + 1) + 16) +
+                        (size_t)nct * na * (PSCFG_MAXM + 1);
+        k_am_dots<<<dim3(nct, na), 256, 0, E.st>>>(ddot, dpart);
+        E.launched();
+        double *dres = E.d_small + (size_t)na * (PSCFG_MAXM + 1);
+        if ((size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1) > (size_t)64 * ninst) throw Err(PSCFG_EINVAL, "scratch");
+        k_final_sum<<<(unsigned)((na * (PSCFG_MAXH + 1) + 127) / 128), 128, 0, E.st>>>(dpart, nct, 1.0, dres,
+                                                                                       na * (PSCFG_MAXH + 1));
+        E.launched();
+        hsmall.resize((size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1));
+        CK(cudaMemcpyAsync(hsmall.data(), E.d_small, sizeof(double) * hsmall.size(), cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+
+        std::vector<AmMix> mixes;
+        std::vector<int> mix_inst;
+        for (int k = 0; k < na; k++) {
+            const int i = act[k];
+            AmState &s = st[i];
+            Inst &I = E.inst[i];
+            const int ncp = prm.domain ? I.cell.ncp : 0;
+            s.f = fe[k];
+            s.p = pe[k];
+            for (int b = 0; b < PSCFG_MAXCP; b++) s.stress[b] = sh[(size_t)k * PSCFG_MAXCP + b];
+            // update gram ring with <d_cur, d_h>/nr
+            const double *g = &hsmall[(size_t)na * (PSCFG_MAXM + 1) + (size_t)k * (PSCFG_MAXH + 1)];
+            int nst = std::min(s.nstore + 1, S);
+            for (int h = 0; h < nst; h++) {
+                int slot = ((s.head - h) % S + S) % S;
+                s.gram[(size_t)s.head * S + slot] = g[h] / (double)E.nr;
+                s.gram[(size_t)slot * S + s.head] = g[h] / (double)E.nr;
+            }
+            for (int b = 0; b < ncp; b++) s.devcp[s.head][b] = -s.stress[b];
+            double e1 = hsmall[(size_t)na * PSCFG_MAXM + k];
+            double e2 = 0;
+            for (int b = 0; b < ncp; b++) e2 = std::max(e2, std::fabs(s.stress[b]));
+            s.error = std::max(e1, e2);
+            s.nstore = nst;
+            if (s.error < prm.error_max) { s.converged = true; s.done = true; continue; }
+            if (s.itr > prm.max_itr || !(s.error <= 100.0 * large)) { s.done = true; continue; }
+
+            // lambda and number of previous entries (src/iterate_mod.fp.f90:1147-1153)
+            int itr_prev;
+            double lam;
+            if (s.itr < H + 1) { itr_prev = s.itr - 1; lam = 1.0 - std::pow(0.9, s.itr); }
+            else { itr_prev = H; lam = 1.0; }
+            AmMix m;
+            std::memset(&m, 0, sizeof(m));
+            m.omega = I.omega;
+            m.om_cur = I.om_hist + (long)s.head * fl;
+            m.d_cur = I.dev_hist + (long)s.head * fl;
+            m.len = fl;
+            m.lam = lam;
+            const int cur = s.head;
+            std::vector<double> cp_new(ncp);
+            if (itr_prev == 0) {
+                m.n = 0;
+                for (int b = 0; b < ncp; b++) cp_new[b] = I.sys.cell_param[b] + lam * s.devcp[cur][b];
+            } else {
+                const int n = itr_prev;
+                std::vector<double> U((size_t)n * n), V(n);
+                auto G = [&](int a, int b) { return s.gram[(size_t)a * S + b]; };
+                std::vector<int> sl(n);
+                for (int mm = 0; mm < n; mm++) sl[mm] = ((cur - 1 - mm) % S + S) % S;
+                for (int mm = 0; mm < n; mm++) {
+                    for (int nn = mm; nn < n; nn++) {
+                        double u = G(cur, cur) - G(cur, sl[nn]) - G(sl[mm], cur) + G(sl[mm], sl[nn]);
+                        for (int b = 0; b < ncp; b++)
+                            u += (s.devcp[cur][b] - s.devcp[sl[mm]][b]) * (s.devcp[cur][b] - s.devcp[sl[nn]][b]);
+                        U[(size_t)mm * n + nn] = u;
+                        U[(size_t)nn * n + mm] = u;
+                    }
+                    double v = G(cur, cur) - G(sl[mm], cur);
+                    for (int b = 0; b < ncp; b++) v += (s.devcp[cur][b] - s.devcp[sl[mm]][b]) * s.devcp[cur][b];
+                    V[mm] = v;
+                }
+                if (!solve_dense(n, U, V)) { s.done = true; s.error = INFINITY; continue; }
+                m.n = n;
+                for (int nn = 0; nn < n; nn++) {
+                    m.C[nn] = V[nn];
+                    m.om[nn] = I.om_hist + (long)sl[nn] * fl;
+                    m.d[nn] = I.dev_hist + (long)sl[nn] * fl;
+                }
+                for (int b = 0; b < ncp; b++) {
+                    double ww = I.sys.cell_param[b], dd = s.devcp[cur][b];
+                    for (int nn = 0; nn < n; nn++) {
+                        ww += V[nn] * (s.cph[sl[nn]][b] - s.cph[cur][b]);
+                        dd += V[nn] * (s.devcp[sl[nn]][b] - s.devcp[cur][b]);
+                    }
+                    cp_new[b] = ww + lam * dd;
+                }
+            }
+            mixes.push_back(m);
+            mix_inst.push_back(i);
+            for (int b = 0; b < ncp; b++) I.sys.cell_param[b] = cp_new[b];
+        }
+        if (!mixes.empty()) {
+            AmMix *dm = E.upload(mixes, 0);
+            k_am_mix<<<dim3(nct, (unsigned)mixes.size()), 256, 0, E.st>>>(dm);
+            E.launched();
+            for (int i : mix_inst) {
+                AmState &s = st[i];
+                Inst &I = E.inst[i];
+                s.head = (s.head + 1) % S;
+                CK(cudaMemcpyAsync(I.om_hist + (long)s.head * fl, I.omega, sizeof(double) * fl, cudaMemcpyDeviceToDevice,
+                                   E.st));
+                for (int b = 0; b < I.cell.ncp; b++) s.cph[s.head][b] = I.sys.cell_param[b];
+                if (prm.domain) upload_cell(E, I);
+            }
+            CK(cudaStreamSynchronize(E.st));
+        }
+    }
+    if (!prm.domain) stress_all(E, all);
+    std::vector<double> shost((size_t)ninst * PSCFG_MAXCP);
+    if (!prm.domain) {
+        for (int i = 0; i < ninst; i++)
+            CK(cudaMemcpyAsync(&shost[(size_t)i * PSCFG_MAXCP], E.inst[i].stress_dev, sizeof(double) * PSCFG_MAXCP,
+                               cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+    }
+    res.resize(ninst);
+    for (int i = 0; i < ninst; i++) {
+        pscfg_am_result &r = res[i];
+        std::memset(&r, 0, sizeof(r));
+        AmState &s = st[i];
+        Inst &I = E.inst[i];
+        r.itr = s.itr;
+        r.converged = s.converged ? 1 : 0;
+        r.error = s.error;
+        r.f_helmholtz = s.f;
+        r.pressure = s.p;
+        for (int b = 0; b < I.cell.ncp; b++) {
+            r.stress[b] = prm.domain ? s.stress[b] : shost[(size_t)i * PSCFG_MAXCP + b];
+            r.cell_param[b] = I.sys.cell_param[b];
+        }
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            r.q[c] = I.Q[c];
+            r.mu_chain[c] = I.sys.mu_chain[c];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// Single-field propagation (parity checks of step_exp)
+// ---------------------------------------------------------------------
+template <typename T>
+static void propagate_impl(Engine &E, int inst, const double *omega_m, double b, double ds, const double *qin,
+                           double *qout, int nsteps)
+{
+    Inst &I = E.inst[inst];
+    const size_t ts = sizeof(T);
+    // scratch: omega, slab [nsteps+1][nr], tables, 3-D scratch
+    double *w = nullptr;
+    void *slab = nullptr, *eo1 = nullptr, *eo2 = nullptr, *ek1 = nullptr, *ek2 = nullptr;
+    void *S1 = nullptr, *S2 = nullptr, *q1 = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(w); cudaFree(slab); cudaFree(eo1); cudaFree(eo2); cudaFree(ek1); cudaFree(ek2);
+        cudaFree(S1); cudaFree(S2); cudaFree(q1);
+    };
+    try {
+        CK(cudaMalloc(&w, sizeof(double) * E.nr));
+        CK(cudaMalloc(&slab, ts * E.nr * (nsteps + 1)));
+        CK(cudaMalloc(&eo1, ts * E.nr));
+        CK(cudaMalloc(&eo2, ts * E.nr));
+        CK(cudaMalloc(&ek1, ts * E.nk));
+        CK(cudaMalloc(&ek2, ts * E.nk));
+        CK(cudaMalloc(&S1, 2 * ts * E.nk));
+        CK(cudaMalloc(&S2, 2 * ts * E.nk));
+        CK(cudaMalloc(&q1, ts * E.nr));
+        CK(cudaMemcpyAsync(w, omega_m, sizeof(double) * E.nr, cudaMemcpyHostToDevice, E.st));
+        std::vector<T> h(E.nr);
+        for (long r = 0; r < E.nr; r++) h[r] = (T)qin[r];
+        CK(cudaMemcpyAsync(slab, h.data(), ts * E.nr, cudaMemcpyHostToDevice, E.st));
+        std::vector<TableJob<T>> tj(1);
+        tj[0].omega = w;
+        tj[0].ksq = I.ksq;
+        tj[0].eo1 = (T *)eo1;
+        tj[0].eo2 = (T *)eo2;
+        tj[0].ek1 = (T *)ek1;
+        tj[0].ek2 = (T *)ek2;
+        tj[0].ds = ds;
+        tj[0].b = b;
+        TableJob<T> *dtj = E.upload(tj, 0);
+        SweepField<T> f;
+        std::memset(&f, 0, sizeof(f));
+        f.slab = (T *)slab;
+        f.ns = nsteps;
+        f.dir = 1;
+        f.nblk = 1;
+        f.bgn[0] = 0;
+        f.bgn[1] = nsteps;
+        f.eo1[0] = (T *)eo1;
+        f.eo2[0] = (T *)eo2;
+        f.ek1[0] = (T *)ek1;
+        f.ek2[0] = (T *)ek2;
+        f.S1 = (cx<T> *)S1;
+        f.S2 = (cx<T> *)S2;
+        f.q1 = (T *)q1;
+        std::vector<SweepField<T>> fl(1, f);
+        SweepField<T> *dfl = E.upload(fl, 1024);
+        k_make_tables<T><<<dim3((unsigned)std::min<long>((E.nr + 255) / 256, 256), 1), 256, 0, E.st>>>(dtj, E.nr, E.nk);
+        E.launched();
+        const PlaneGeom &g = E.geom();
+        if (E.dim <= 2) {
+            size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)E.nr * sizeof(T);
+            if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
+            CK(cudaFuncSetAttribute(k_sweep_plane<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
+            k_sweep_plane<T><<<1, threads, sm, E.st>>>(dfl, g, 0, nsteps);
+            E.launched();
+        } else {
+            size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
+            size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
+            CK(cudaFuncSetAttribute(k3_fwd_pair<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(cudaFuncSetAttribute(k3_inv_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(cudaFuncSetAttribute(k3_inv_final<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(cudaFuncSetAttribute(k3_zconv<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+            const long P = (long)g.n1h * g.n2;
+            const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+            for (int t = 0; t < nsteps; t++) {
+                k3_fwd_pair<T><<<dim3(g.n3, 1), 256, smxy, E.st>>>(dfl, g, t);
+                E.launched();
+                k3_zconv<T, Z_TILE><<<dim3(ntile, 1, 2), 256, smz, E.st>>>(dfl, g, t, 3);
+                E.launched();
+                k3_inv_mid<T><<<dim3(g.n3, 1), 256, smxy, E.st>>>(dfl, g, t);
+                E.launched();
+                k3_zconv<T, Z_TILE><<<dim3(ntile, 1, 1), 256, smz, E.st>>>(dfl, g, t, 2);
+                E.launched();
+                k3_inv_final<T><<<dim3(g.n3, 1), 256, smxy, E.st>>>(dfl, g, t);
+                E.launched();
+            }
+        }
+        CK(cudaMemcpyAsync(h.data(), (T *)slab + (long)nsteps * E.nr, ts * E.nr, cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+        for (long r = 0; r < E.nr; r++) qout[r] = (double)h[r];
+    } catch (...) {
+        cudaStreamSynchronize(E.st);
+        cleanup();
+        throw;
+    }
+    cleanup();
+}
+
+}  // namespace pscfg
+
+// =====================================================================
+// C ABI
+// =====================================================================
+using namespace pscfg;
+
+struct pscfg_engine {
+    Engine E;
+};
+
+#define ABI_BEGIN try {
+#define ABI_END(e)                                    \
+    }                                                 \
+    catch (const Err &x)                              \
+    {                                                 \
+        if (e) (e)->E.err = x.msg;                    \
+        return x.code;                                \
+    }                                                 \
+    catch (const std::exception &x)                   \
+    {                                                 \
+        if (e) (e)->E.err = x.what();                 \
+        return PSCFG_EINVAL;                          \
+    }                                                 \
+    return PSCFG_OK;
+
+extern "C" {
+
+int pscfg_create(const pscfg_system *systems, int n_inst, int precision, pscfg_engine **out)
+{
+    if (!systems || !out) {
+        g_create_error = "null argument";
+        return PSCFG_EINVAL;
+    }
+    *out = nullptr;
+    pscfg_engine *e = new (std::nothrow) pscfg_engine();
+    if (!e) {
+        g_create_error = "host allocation failed";
+        return PSCFG_ENOMEM;
+    }
+    try {
+        create_engine(e->E, systems, n_inst, precision);
+    } catch (const Err &x) {
+        g_create_error = x.msg;
+        delete e;
+        return x.code;
+    }
+    *out = e;
+    return PSCFG_OK;
+}
+
+void pscfg_destroy(pscfg_engine *e) { delete e; }
+
+const char *pscfg_last_error(const pscfg_engine *e)
+{
+    if (!e) return g_create_error.c_str();
+    return e->E.err.c_str();
+}
+
+int pscfg_set_cell_param(pscfg_engine *e, int inst, const double *cell_param)
+{
+    if (!e || !cell_param) return PSCFG_EINVAL;
+    ABI_BEGIN
+    if (inst < 0 || inst >= (int)e->E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
+    Inst &I = e->E.inst[inst];
+    for (int k = 0; k < PSCFG_MAXCP; k++) I.sys.cell_param[k] = cell_param[k];
+    upload_cell(e->E, I);
+    ABI_END(e)
+}
+
+int pscfg_get_ksq(pscfg_engine *e, int inst, double *ksq)
+{
+    if (!e || !ksq) return PSCFG_EINVAL;
+    ABI_BEGIN
+    if (inst < 0 || inst >= (int)e->E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
+    CK(cudaMemcpyAsync(ksq, e->E.inst[inst].ksq, sizeof(double) * e->E.nk, cudaMemcpyDeviceToHost, e->E.st));
+    CK(cudaStreamSynchronize(e->E.st));
+    ABI_END(e)
+}
+
+static int density_common(pscfg_engine *e, const double *omega, double *rho, double *q, double *qs, bool device)
+{
+    ABI_BEGIN
+    Engine &E = e->E;
+    const long fl = (long)E.M * E.nr;
+    const int ni = (int)E.inst.size();
+    for (int i = 0; i < ni; i++)
+        CK(cudaMemcpyAsync(E.inst[i].omega, omega + (long)i * fl, sizeof(double) * fl,
+                           device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, E.st));
+    std::vector<int> all(ni);
+    for (int i = 0; i < ni; i++) all[i] = i;
+    density_all(E, all);
+    if (rho) {
+        for (int i = 0; i < ni; i++)
+            CK(cudaMemcpyAsync(rho + (long)i * fl, E.inst[i].rho, sizeof(double) * fl,
+                               device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, E.st));
+    }
+    CK(cudaStreamSynchronize(E.st));
+    for (int i = 0; i < ni; i++) {
+        if (q)
+            for (int c = 0; c < PSCFG_MAXC; c++) q[(long)i * PSCFG_MAXC + c] = (c < E.inst[i].sys.n_chain) ? E.inst[i].Q[c] : 0.0;
+        if (qs)
+            for (int s = 0; s < PSCFG_MAXS; s++) qs[(long)i * PSCFG_MAXS + s] = E.inst[i].Qs[s];
+    }
+    ABI_END(e)
+}
+
+int pscfg_density(pscfg_engine *e, const double *omega, double *rho, double *q, double *q_solvent)
+{
+    if (!e || !omega) return PSCFG_EINVAL;
+    return density_common(e, omega, rho, q, q_solvent, false);
+}
+
+int pscfg_density_device(pscfg_engine *e, const double *omega_dev, double *rho_dev, double *q, double *q_solvent)
+{
+    if (!e || !omega_dev) return PSCFG_EINVAL;
+    return density_common(e, omega_dev, rho_dev, q, q_solvent, true);
+}
+
+int pscfg_stress(pscfg_engine *e, double *stress)
+{
+    if (!e || !stress) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    const int ni = (int)E.inst.size();
+    std::vector<int> all(ni);
+    for (int i = 0; i < ni; i++) all[i] = i;
+    stress_all(E, all);
+    for (int i = 0; i < ni; i++)
+        CK(cudaMemcpyAsync(stress + (long)i * PSCFG_MAXCP, E.inst[i].stress_dev, sizeof(double) * PSCFG_MAXCP,
+                           cudaMemcpyDeviceToHost, E.st));
+    CK(cudaStreamSynchronize(E.st));
+    for (int i = 0; i < ni; i++)
+        for (int b = E.inst[i].cell.ncp; b < PSCFG_MAXCP; b++) stress[(long)i * PSCFG_MAXCP + b] = 0.0;
+    ABI_END(e)
+}
+
+int pscfg_free_energy(pscfg_engine *e, double *out, double *mu_chain)
+{
+    if (!e || !out) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    const int ni = (int)E.inst.size();
+    std::vector<int> all(ni);
+    for (int i = 0; i < ni; i++) {
+        all[i] = i;
+        if (!E.inst[i].have_density) throw Err(PSCFG_ESTATE, "free_energy requires a preceding density call");
+    }
+    std::vector<double> f, p;
+    free_energy_all(E, all, f, p);
+    for (int i = 0; i < ni; i++) {
+        out[2 * i] = f[i];
+        out[2 * i + 1] = p[i];
+        if (mu_chain)
+            for (int c = 0; c < PSCFG_MAXC; c++)
+                mu_chain[(long)i * PSCFG_MAXC + c] = (c < E.inst[i].sys.n_chain) ? E.inst[i].sys.mu_chain[c] : 0.0;
+    }
+    ABI_END(e)
+}
+
+int pscfg_iterate_am(pscfg_engine *e, double *omega, const pscfg_am_param *prm, double *rho, pscfg_am_result *results)
+{
+    if (!e || !omega || !prm || !results) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    const long fl = (long)E.M * E.nr;
+    const int ni = (int)E.inst.size();
+    for (int i = 0; i < ni; i++)
+        CK(cudaMemcpyAsync(E.inst[i].omega, omega + (long)i * fl, sizeof(double) * fl, cudaMemcpyHostToDevice, E.st));
+    std::vector<pscfg_am_result> res;
+    iterate_am_impl(E, *prm, res);
+    int any_fail = 0;
+    for (int i = 0; i < ni; i++) {
+        results[i] = res[i];
+        if (!res[i].converged) any_fail = 1;
+        CK(cudaMemcpyAsync(omega + (long)i * fl, E.inst[i].omega, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
+        if (rho) CK(cudaMemcpyAsync(rho + (long)i * fl, E.inst[i].rho, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
+    }
+    CK(cudaStreamSynchronize(E.st));
+    if (any_fail) {
+        E.err = "at least one instance did not converge";
+        return PSCFG_ENOTCONV;
+    }
+    ABI_END(e)
+}
+
+int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, double ds, const double *q_in,
+                    double *q_out, int nsteps)
+{
+    if (!e || !omega_m || !q_in || !q_out || nsteps < 1) return PSCFG_EINVAL;
+    ABI_BEGIN
+    if (inst < 0 || inst >= (int)e->E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
+    if (e->E.prec == PSCFG_FP64) propagate_impl<double>(e->E, inst, omega_m, b, ds, q_in, q_out, nsteps);
+    else propagate_impl<float>(e->E, inst, omega_m, b, ds, q_in, q_out, nsteps);
+    ABI_END(e)
+}
+
+int pscfg_get_propagators(pscfg_engine *e, int inst, int chain, double *qf, double *qr, int *n_slices)
+{
+    if (!e) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    if (inst < 0 || inst >= (int)E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
+    Inst &I = E.inst[inst];
+    if (chain < 0 || chain >= I.sys.n_chain) throw Err(PSCFG_EINVAL, "chain index out of range");
+    const long ns = I.ns[chain] + 1;
+    if (n_slices) *n_slices = (int)ns;
+    for (int d = 0; d < 2; d++) {
+        double *dst = d == 0 ? qf : qr;
+        if (!dst) continue;
+        const void *src = d == 0 ? I.qf[chain] : I.qr[chain];
+        if (E.prec == PSCFG_FP64) {
+            CK(cudaMemcpyAsync(dst, src, sizeof(double) * E.nr * ns, cudaMemcpyDeviceToHost, E.st));
+            CK(cudaStreamSynchronize(E.st));
+        } else {
+            std::vector<float> h(E.nr * ns);
+            CK(cudaMemcpyAsync(h.data(), src, sizeof(float) * E.nr * ns, cudaMemcpyDeviceToHost, E.st));
+            CK(cudaStreamSynchronize(E.st));
+            for (long k = 0; k < E.nr * ns; k++) dst[k] = h[k];
+        }
+    }
+    ABI_END(e)
+}
+
+long pscfg_steps_per_density(const pscfg_engine *e)
+{
+    if (!e) return 0;
+    long s = 0;
+    for (const Inst &I : e->E.inst)
+        for (int c = 0; c < I.sys.n_chain; c++) s += 2L * I.ns[c];
+    return s;
+}
+
+long pscfg_launch_count(const pscfg_engine *e) { return e ? e->E.launches : 0; }
+
+}  // extern "C"

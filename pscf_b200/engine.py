@@ -1,0 +1,272 @@
+"""ctypes binding of the C ABI in include/pscf_gpu.h (libpscfgpu.so).
+
+Method names follow the reference routines the ABI replaces:
+``density`` (src/scf_mod.fp.f90:144-229), ``scf_stress`` (:451-550),
+``free_energy`` (:834-886), ``iterate_am`` (src/iterate_mod.fp.f90:1042-1490),
+``propagate`` (step_exp, src/step_mod.f90:146-176).
+
+The library is the only compute path: if it cannot be loaded this module
+raises, there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Sequence
+
+import numpy as np
+
+from .system import (MAX_BLOCK, MAX_CELL_PARAM, MAX_CHAIN, MAX_MONOMER,
+                     MAX_SOLVENT, System)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libpscfgpu.so")
+
+FP64 = 0
+FP32 = 1
+
+OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENOTCONV = 0, 1, 2, 3, 4, 5
+
+
+class PscfgSystem(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int),
+        ("n", C.c_int * 3),
+        ("n_monomer", C.c_int),
+        ("n_chain", C.c_int),
+        ("n_solvent", C.c_int),
+        ("ensemble", C.c_int),
+        ("n_block", C.c_int * MAX_CHAIN),
+        ("block_monomer", (C.c_int * MAX_BLOCK) * MAX_CHAIN),
+        ("block_length", (C.c_double * MAX_BLOCK) * MAX_CHAIN),
+        ("kuhn", C.c_double * MAX_MONOMER),
+        ("chi", (C.c_double * MAX_MONOMER) * MAX_MONOMER),
+        ("phi_chain", C.c_double * MAX_CHAIN),
+        ("mu_chain", C.c_double * MAX_CHAIN),
+        ("solvent_monomer", C.c_int * MAX_SOLVENT),
+        ("solvent_size", C.c_double * MAX_SOLVENT),
+        ("phi_solvent", C.c_double * MAX_SOLVENT),
+        ("mu_solvent", C.c_double * MAX_SOLVENT),
+        ("chain_step", C.c_double),
+        ("crystal_system", C.c_int),
+        ("cell_param", C.c_double * MAX_CELL_PARAM),
+    ]
+
+
+class PscfgAmParam(C.Structure):
+    _fields_ = [
+        ("max_itr", C.c_int),
+        ("n_hist", C.c_int),
+        ("domain", C.c_int),
+        ("error_max", C.c_double),
+    ]
+
+
+class PscfgAmResult(C.Structure):
+    _fields_ = [
+        ("itr", C.c_int),
+        ("converged", C.c_int),
+        ("error", C.c_double),
+        ("f_helmholtz", C.c_double),
+        ("pressure", C.c_double),
+        ("stress", C.c_double * MAX_CELL_PARAM),
+        ("cell_param", C.c_double * MAX_CELL_PARAM),
+        ("q", C.c_double * MAX_CHAIN),
+        ("mu_chain", C.c_double * MAX_CHAIN),
+    ]
+
+
+# Every symbol the header declares, with its ctypes signature.
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+SIGNATURES = {
+    "pscfg_create": (C.c_int, [C.POINTER(PscfgSystem), C.c_int, C.c_int, C.POINTER(_vp)]),
+    "pscfg_destroy": (None, [_vp]),
+    "pscfg_last_error": (C.c_char_p, [_vp]),
+    "pscfg_set_cell_param": (C.c_int, [_vp, C.c_int, _dp]),
+    "pscfg_get_ksq": (C.c_int, [_vp, C.c_int, _dp]),
+    "pscfg_density": (C.c_int, [_vp, _dp, _dp, _dp, _dp]),
+    "pscfg_density_device": (C.c_int, [_vp, _vp, _vp, _dp, _dp]),
+    "pscfg_stress": (C.c_int, [_vp, _dp]),
+    "pscfg_free_energy": (C.c_int, [_vp, _dp, _dp]),
+    "pscfg_iterate_am": (C.c_int, [_vp, _dp, C.POINTER(PscfgAmParam), _dp, C.POINTER(PscfgAmResult)]),
+    "pscfg_propagate": (C.c_int, [_vp, C.c_int, _dp, C.c_double, C.c_double, _dp, _dp, C.c_int]),
+    "pscfg_get_propagators": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]),
+    "pscfg_steps_per_density": (C.c_long, [_vp]),
+    "pscfg_launch_count": (C.c_long, [_vp]),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libpscfgpu.so and bind every declared entry point."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise RuntimeError(
+                f"engine library {path} is missing: build it with `python -m pscf_b200.build`")
+        lib = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def to_c(system: System) -> PscfgSystem:
+    s = PscfgSystem()
+    s.dim = system.dim
+    for i, v in enumerate(system.n):
+        s.n[i] = v
+    s.n_monomer = system.n_monomer
+    s.n_chain = len(system.chains)
+    s.n_solvent = len(system.solvents)
+    s.ensemble = system.ensemble
+    for i, c in enumerate(system.chains):
+        s.n_block[i] = len(c.block_length)
+        for b, (m, L) in enumerate(zip(c.block_monomer, c.block_length)):
+            s.block_monomer[i][b] = m
+            s.block_length[i][b] = L
+        s.phi_chain[i] = c.phi
+        s.mu_chain[i] = c.mu
+    for i, sv in enumerate(system.solvents):
+        s.solvent_monomer[i] = sv.monomer
+        s.solvent_size[i] = sv.size
+        s.phi_solvent[i] = sv.phi
+        s.mu_solvent[i] = sv.mu
+    for a in range(system.n_monomer):
+        s.kuhn[a] = system.kuhn[a]
+        for b in range(system.n_monomer):
+            s.chi[a][b] = system.chi[a, b]
+    s.chain_step = system.ds
+    s.crystal_system = system.crystal_code
+    for k, v in enumerate(system.cell_param):
+        s.cell_param[k] = v
+    return s
+
+
+class EngineError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pscfg error {code}: {msg}")
+        self.code = code
+
+
+class Engine:
+    """A batch of SCFT instances of one grid shape on the GPU."""
+
+    def __init__(self, systems: Sequence[System], precision: int = FP64):
+        self.lib = load_library()
+        if isinstance(systems, System):
+            systems = [systems]
+        self.systems: List[System] = list(systems)
+        arr = (PscfgSystem * len(self.systems))(*[to_c(s) for s in self.systems])
+        h = _vp()
+        rc = self.lib.pscfg_create(arr, len(self.systems), precision, C.byref(h))
+        if rc != OK:
+            raise EngineError(rc, self.lib.pscfg_last_error(None).decode())
+        self._h = h
+        self.precision = precision
+        s0 = self.systems[0]
+        self.nr, self.nk, self.M = s0.nr, s0.nk, s0.n_monomer
+        self.n_inst = len(self.systems)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.pscfg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, allow=()):
+        if rc != OK and rc not in allow:
+            raise EngineError(rc, self.lib.pscfg_last_error(self._h).decode())
+        return rc
+
+    # -- geometry --------------------------------------------------------
+    def set_cell_param(self, inst: int, cell_param: Sequence[float]):
+        cp = np.zeros(MAX_CELL_PARAM)
+        cp[: len(cell_param)] = cell_param
+        self._check(self.lib.pscfg_set_cell_param(self._h, inst, _ptr(cp)))
+        self.systems[inst].cell_param = list(cell_param)
+
+    def ksq(self, inst: int = 0) -> np.ndarray:
+        out = np.zeros(self.nk)
+        self._check(self.lib.pscfg_get_ksq(self._h, inst, _ptr(out)))
+        return out
+
+    # -- hot path --------------------------------------------------------
+    def density(self, omega: np.ndarray):
+        """omega [n_inst][M][nr] -> (rho [n_inst][M][nr], q [n_inst][MAXC])."""
+        w = np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
+        rho = np.zeros_like(w)
+        q = np.zeros((self.n_inst, MAX_CHAIN))
+        self._check(self.lib.pscfg_density(self._h, _ptr(w), _ptr(rho), _ptr(q), None))
+        return rho, q
+
+    def density_device(self, omega_dev_ptr: int, rho_dev_ptr: int):
+        q = np.zeros((self.n_inst, MAX_CHAIN))
+        self._check(self.lib.pscfg_density_device(self._h, _vp(omega_dev_ptr), _vp(rho_dev_ptr), _ptr(q), None))
+        return q
+
+    def scf_stress(self) -> np.ndarray:
+        out = np.zeros((self.n_inst, MAX_CELL_PARAM))
+        self._check(self.lib.pscfg_stress(self._h, _ptr(out)))
+        return out
+
+    def free_energy(self):
+        out = np.zeros((self.n_inst, 2))
+        mu = np.zeros((self.n_inst, MAX_CHAIN))
+        self._check(self.lib.pscfg_free_energy(self._h, _ptr(out), _ptr(mu)))
+        return out[:, 0].copy(), out[:, 1].copy(), mu
+
+    def propagate(self, inst: int, omega_m, b: float, ds: float, q_in, nsteps: int = 1) -> np.ndarray:
+        w = np.ascontiguousarray(omega_m, dtype=np.float64).ravel()
+        q = np.ascontiguousarray(q_in, dtype=np.float64).ravel()
+        out = np.zeros(self.nr)
+        self._check(self.lib.pscfg_propagate(self._h, inst, _ptr(w), b, ds, _ptr(q), _ptr(out), nsteps))
+        return out
+
+    def propagators(self, inst: int = 0, chain: int = 0):
+        ns = C.c_int(0)
+        self._check(self.lib.pscfg_get_propagators(self._h, inst, chain, None, None, C.byref(ns)))
+        qf = np.zeros((ns.value, self.nr))
+        qr = np.zeros((ns.value, self.nr))
+        self._check(self.lib.pscfg_get_propagators(self._h, inst, chain, _ptr(qf), _ptr(qr), None))
+        return qf, qr
+
+    def iterate_am(self, omega: np.ndarray, error_max=1e-10, max_itr=1000, n_hist=20, domain=False):
+        """Anderson-mixing solve of every instance; returns (omega, rho, results)."""
+        w = np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr).copy()
+        rho = np.zeros_like(w)
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max)
+        res = (PscfgAmResult * self.n_inst)()
+        self._check(self.lib.pscfg_iterate_am(self._h, _ptr(w), C.byref(prm), _ptr(rho), res), allow=(ENOTCONV,))
+        out = []
+        for i, r in enumerate(res):
+            ncp = len(self.systems[i].cell_param)
+            nch = len(self.systems[i].chains)
+            out.append(dict(itr=r.itr, converged=bool(r.converged), error=r.error,
+                            f_helmholtz=r.f_helmholtz, pressure=r.pressure,
+                            stress=list(r.stress)[:ncp], cell_param=list(r.cell_param)[:ncp],
+                            q=list(r.q)[:nch], mu_chain=list(r.mu_chain)[:nch]))
+            if domain:
+                self.systems[i].cell_param = list(r.cell_param)[:ncp]
+        return w, rho, out
+
+    @property
+    def steps_per_density(self) -> int:
+        return int(self.lib.pscfg_steps_per_density(self._h))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.pscfg_launch_count(self._h))

@@ -1,0 +1,108 @@
+"""GPU engine vs the FP64 CPU oracle: single steps, density, stress, F."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from pscf_b200.engine import Engine, FP32, FP64
+from tests.cases import diblock, omega_guess, rel_err, smooth_field, triblock
+
+pytestmark = pytest.mark.gpu
+
+STEP_CASES = [
+    (1, [32], "lamellar", [1.7]),
+    (1, [30], "lamellar", [1.3]),
+    (1, [27], "lamellar", [1.4]),
+    (2, [24, 24], "hexagonal", [1.9]),
+    (2, [20, 14], "rectangular", [1.6, 2.1]),
+    (2, [15, 12], "rectangular", [1.6, 2.1]),
+    (3, [16, 16, 16], "cubic", [3.9]),
+    (3, [20, 12, 14], "orthorhombic", [2.0, 2.5, 3.0]),
+    (3, [9, 10, 8], "orthorhombic", [2.0, 2.5, 3.0]),
+]
+
+
+@pytest.mark.parametrize("dim,ngrid,crystal,cell", STEP_CASES)
+def test_step_parity_fp64(dim, ngrid, crystal, cell):
+    s = diblock(dim, ngrid, crystal, cell)
+    e = Engine([s], FP64)
+    o = O.Oracle(s)
+    ksq = o.ksq()
+    np.testing.assert_allclose(e.ksq(0), ksq, rtol=1e-14, atol=1e-12)
+    w = 7.5 + smooth_field(s, 11, 3.0)
+    q0 = 1.0 + 0.3 * smooth_field(s, 12, 1.0)
+    for nsteps in (1, 7):
+        ref = O.step(s, ksq, 1.0, 0.01, w, q0, nsteps)
+        got = e.propagate(0, w, 1.0, 0.01, q0, nsteps)
+        assert rel_err(got, ref) < 1e-12, (nsteps, rel_err(got, ref))
+
+
+DENSITY_CASES = [
+    (1, [32], "lamellar", [1.7], 0.5),
+    (2, [24, 24], "hexagonal", [1.9], 0.3),
+    (3, [16, 16, 16], "cubic", [3.9], 0.25),
+    (3, [12, 10, 14], "orthorhombic", [2.0, 2.5, 3.0], 0.4),
+]
+
+
+@pytest.mark.parametrize("dim,ngrid,crystal,cell,fA", DENSITY_CASES)
+def test_density_stress_free_energy_fp64(dim, ngrid, crystal, cell, fA):
+    s = diblock(dim, ngrid, crystal, cell, fA=fA, chiN=15.0)
+    w = omega_guess(s, 5, 2.0)
+    o = O.Oracle(s)
+    rho_ref, q_ref = o.density(w)
+    st_ref = o.stress()
+    f_ref, p_ref = o.free_energy(w, rho_ref)
+    e = Engine([s], FP64)
+    rho, q = e.density(w[None])
+    assert rel_err(q[0, :1], q_ref) < 1e-12
+    assert rel_err(rho[0], rho_ref) < 1e-12
+    qf_ref, qr_ref = o.propagators(0)
+    qf, qr = e.propagators(0, 0)
+    assert rel_err(qf, qf_ref) < 1e-12 and rel_err(qr, qr_ref) < 1e-12
+    st = e.scf_stress()[0, : len(st_ref)]
+    assert np.max(np.abs(st - st_ref)) < 1e-10 * max(1.0, np.max(np.abs(st_ref)))
+    f, p, mu = e.free_energy()
+    assert abs(f[0] - f_ref) < 1e-11 and abs(p[0] - p_ref) < 1e-11
+
+
+def test_triblock_density_fp64():
+    s = triblock(3, [8, 12, 20], "orthorhombic", [1.5, 3.0, 5.25], ds=0.02)
+    w = omega_guess(s, 9, 2.0)
+    o = O.Oracle(s)
+    rho_ref, q_ref = o.density(w)
+    e = Engine([s], FP64)
+    rho, q = e.density(w[None])
+    assert rel_err(rho[0], rho_ref) < 1e-12
+    assert rel_err(q[0, :1], q_ref) < 1e-12
+    st = e.scf_stress()[0, :3]
+    np.testing.assert_allclose(st, o.stress(), rtol=1e-10, atol=1e-12)
+
+
+def test_batched_uneven_instances_fp64():
+    """Instances with different f_A (uneven step counts), chi and cells."""
+    systems = [diblock(3, [12, 12, 12], "cubic", [3.6 + 0.1 * i], fA=0.25 + 0.05 * i, chiN=14.0 + i)
+               for i in range(4)]
+    ws = np.stack([omega_guess(s, 40 + i, 1.5) for i, s in enumerate(systems)])
+    e = Engine(systems, FP64)
+    rho, q = e.density(ws)
+    st = e.scf_stress()
+    f, p, mu = e.free_energy()
+    for i, s in enumerate(systems):
+        o = O.Oracle(s)
+        rr, qq = o.density(ws[i])
+        assert rel_err(rho[i], rr) < 1e-12
+        assert rel_err(q[i, :1], qq) < 1e-12
+        assert abs(st[i, 0] - o.stress()[0]) < 1e-10 * max(1.0, abs(o.stress()[0]))
+        fr, pr = o.free_energy(ws[i], rr)
+        assert abs(f[i] - fr) < 1e-11
+
+
+def test_density_fp32_close():
+    s = diblock(3, [16, 16, 16], "cubic", [3.9], fA=0.3)
+    w = omega_guess(s, 3, 2.0)
+    o = O.Oracle(s)
+    rho_ref, q_ref = o.density(w)
+    e = Engine([s], FP32)
+    rho, q = e.density(w[None])
+    assert rel_err(rho[0], rho_ref) < 2e-5
+    assert rel_err(q[0, :1], q_ref) < 2e-5
