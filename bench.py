@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: MDE contour steps/s and converged SCFT solves/s on one node.
+
+Workload (per GPU): a batch of B instances of the BCC sphere phase,
+space group I m -3 m on a 32^3 grid: AB diblock f_A = 0.25, chi N = 20,
+b_A = b_B = 1, ds = 0.01 (26 + 76 contour steps), cubic cell a = 3.9,
+Anderson mixing with 20 history vectors, cell relaxed by the stress, to a
+residual of 1e-10.  Initial fields: delta = -1.0 (g - <g>) with g the
+max-normalised sum of Gaussians (width 0.3 a) on the BCC sites and images,
+omega_A = chiN phi_B + delta, omega_B = chiN phi_A - delta, plus seeded
+N(0, 0.01) noise (seed 20261203 + 1 + instance).
+
+One bench step = one Anderson iteration of the whole batch: density
+(forward and backward MDE sweeps, Simpson contour integrals), stress,
+deviations, Gram matrix and mixing, all on the device.  `value` counts the
+MDE steps (one step_exp of one chain in one direction) processed per second
+over the timed steps.  The batch's propagator slabs (about 53 MB per
+instance) exceed the 126 MB L2, so no L2 flush is inserted.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B]
+  python bench.py --impl reference   (CPU reference arm: the FP64 oracle)
+
+Under torchrun every rank solves its own batch on its own GPU (instances
+are independent: weak scaling, no data-path collective); the elapsed time
+is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 32
+CELL = 3.9
+F_A = 0.25
+CHI_N = 20.0
+DS = 0.01
+N_HIST = 20
+ERROR_MAX = 1e-10
+SEED = 20261203 + 1
+WORKLOAD = ("BCC I m -3 m 32^3 AB diblock fA=0.25 chiN=20 ds=0.01 a=3.9, Anderson n_hist=20 "
+            "with cell relaxation to 1e-10")
+
+
+def make_system():
+    from pscf_b200.system import Chain, System
+    return System(dim=3, ngrid=[N_GRID] * 3, crystal_system="cubic", cell_param=[CELL],
+                  kuhn=[1.0, 1.0], chi=[[0.0, CHI_N], [CHI_N, 0.0]],
+                  chains=[Chain([0, 1], [F_A, 1.0 - F_A])], ds=DS)
+
+
+def initial_omega(system, inst):
+    n = system.n[0]
+    x = np.arange(n) / n
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    g = np.zeros_like(X)
+    sig = 0.3
+    for c in [(0.0, 0.0, 0.0), (0.5, 0.5, 0.5)]:
+        for sx in (-1, 0, 1):
+            for sy in (-1, 0, 1):
+                for sz in (-1, 0, 1):
+                    dx, dy, dz = X - c[0] - sx, Y - c[1] - sy, Z - c[2] - sz
+                    g += np.exp(-(dx * dx + dy * dy + dz * dz) / (2 * sig * sig))
+    g = g / g.max()
+    delta = -1.0 * (g - g.mean())
+    rng = np.random.default_rng(SEED + inst)
+    w0 = system.omega_uniform()
+    w = np.zeros((2, system.nr))
+    w[0] = w0[0] + delta.ravel() + rng.normal(0.0, 0.01, system.nr)
+    w[1] = w0[1] - delta.ravel() + rng.normal(0.0, 0.01, system.nr)
+    return w
+
+
+def bytes_per_step(system, wq=8, ww=8):
+    """Algorithmic HBM bytes of one MDE step: read q(s), write q(s +- ds),
+    read the block's omega: N_r (2 w_q + w_omega)."""
+    return system.nr * (2 * wq + ww)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic_per_step():
+    """DRAM bytes per MDE step of the sweep kernels from the committed ncu
+    summary (profiles/mde_step_bcc32_fp64.md, line 'traffic_bytes_per_step:')."""
+    path = os.path.join(ROOT, "profiles", "mde_step_bcc32_fp64.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_bytes_per_step:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (the oracle): cpu_baseline of our arm, and the reference arm
+# ---------------------------------------------------------------------------
+def cpu_mde_rate(nthreads, nsteps_per_thread, rounds=1):
+    """MDE steps/s of the FP64 oracle's step_exp on the 32^3 C2 grid, one
+    field per thread (ctypes releases the GIL).  Returns (rate, seconds)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    s = make_system()
+    o = O.Oracle(s)
+    ksq = o.ksq()
+    w = initial_omega(s, 0)
+    q0 = np.ones(s.nr)
+    O.step(s, ksq, 1.0, 0.01, w[0], q0, 1)   # load / warm
+    total = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(nthreads) as ex:
+        for _ in range(rounds):
+            futs = [ex.submit(O.step, s, ksq, 1.0, 0.01, w[0], q0, nsteps_per_thread) for _ in range(nthreads)]
+            for f in futs:
+                f.result()
+            total += nthreads * nsteps_per_thread
+    dt = time.perf_counter() - t0
+    return total / dt, dt
+
+
+def run_reference(args, rank):
+    """Reference arm: the reference is Fortran/FFTW and cannot be built in
+    this image (no Fortran compiler, no FFTW); the FP64 C restatement of
+    its propagator (oracle/) stands in, on all host threads."""
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    per = 2
+    for _ in range(args.warmup):
+        cpu_mde_rate(nthreads, per)
+    rates, secs = [], 0.0
+    total_steps = 0
+    for _ in range(args.steps):
+        r, dt = cpu_mde_rate(nthreads, per)
+        rates.append(r)
+        secs += dt
+        total_steps += nthreads * per
+    value = total_steps / secs
+    s = make_system()
+    line = {
+        "impl": "reference", "metric": "MDE steps/s", "value": value, "unit": "MDE steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [N_GRID] * 3, "contour_steps_per_chain": s.contour_steps()},
+        "cpu_baseline": {"value": value, "unit": "MDE steps/s", "cores": nthreads, "kind": "port",
+                         "sample": f"each step: {nthreads} threads x {per} step_exp calls of the FP64 C oracle on the "
+                                   f"32^3 grid (the reference Fortran/FFTW cannot be built here)"},
+        "e2e": {"value": value, "unit": "MDE steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from pscf_b200.engine import Engine, FP64
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    B = args.batch
+    systems = [make_system() for _ in range(B)]
+    omega0 = np.stack([initial_omega(systems[i], rank * B + i) for i in range(B)])
+    e = Engine(systems, FP64)
+    for i in range(B):
+        e.set_symmetry(i, "I m -3 m")
+    stream = torch.cuda.ExternalStream(e.stream, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed Anderson iterations -------------------------------------
+    e.am_begin(omega0, error_max=ERROR_MAX, max_itr=10000, n_hist=N_HIST, domain=True)
+    for _ in range(args.warmup):
+        e.am_iterate(1)
+    barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    l0 = e.launch_count
+    e.set_profiling(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e.am_iterate(1)
+    ev1.record(stream)
+    barrier()
+    clocks = sampler.stop()
+    prof = e.profile()
+    e.set_profiling(False)
+    launches = e.launch_count - l0
+    ms = ev0.elapsed_time(ev1)
+    steps_done = prof["steps"]
+    t = torch.tensor([ms / 1e3, float(steps_done)], dtype=torch.float64, device=dev)
+    if world > 1:
+        tmax = t[0:1].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        tsum = t[1:2].clone()
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        elapsed, total_steps = float(tmax.item()), float(tsum.item())
+    else:
+        elapsed, total_steps = ms / 1e3, float(steps_done)
+    value = total_steps / elapsed
+
+    # ---- converged solves/s: fresh full solve of the batch ---------------
+    barrier()
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    e.am_begin(omega0, error_max=ERROR_MAX, max_itr=2000, n_hist=N_HIST, domain=True)
+    while e.am_iterate(8) > 0:
+        pass
+    ev3.record(stream)
+    barrier()
+    solve_s = ev2.elapsed_time(ev3) / 1e3
+    _, _, res = e.am_results(want_fields=False)
+    conv = sum(1 for r in res if r["converged"])
+    itrs = [r["itr"] for r in res]
+    fvals = [r["f_helmholtz"] for r in res]
+    cells = [r["cell_param"][0] for r in res]
+    ts = torch.tensor([solve_s, float(conv)], dtype=torch.float64, device=dev)
+    if world > 1:
+        smax = ts[0:1].clone()
+        dist.all_reduce(smax, op=dist.ReduceOp.MAX)
+        csum = ts[1:2].clone()
+        dist.all_reduce(csum, op=dist.ReduceOp.SUM)
+        solve_s_all, conv_all = float(smax.item()), float(csum.item())
+    else:
+        solve_s_all, conv_all = solve_s, float(conv)
+
+    # ---- end to end through the C ABI with host buffers ------------------
+    w_pin = torch.from_numpy(omega0.copy()).pin_memory()
+    rho_pin = torch.empty_like(w_pin).pin_memory()
+    q = np.zeros((B, 4))
+    import ctypes as C
+    lib = e.lib
+    dp = C.POINTER(C.c_double)
+    wp = C.cast(w_pin.data_ptr(), dp)
+    rp = C.cast(rho_pin.data_ptr(), dp)
+    stress = np.zeros((B, 6))
+    for _ in range(2):
+        e._check(lib.pscfg_density(e._h, wp, rp, q.ctypes.data_as(dp), None))
+    barrier()
+    n_e2e = max(2, min(args.steps, 5))
+    ev4, ev5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev4.record(stream)
+    for _ in range(n_e2e):
+        e._check(lib.pscfg_density(e._h, wp, rp, q.ctypes.data_as(dp), None))
+        e._check(lib.pscfg_stress(e._h, stress.ctypes.data_as(dp)))
+    ev5.record(stream)
+    barrier()
+    e2e_s = ev4.elapsed_time(ev5) / 1e3
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * n_e2e * e.steps_per_density / float(te.item())
+
+    if rank != 0:
+        return
+    s0 = systems[0]
+    bstep = bytes_per_step(s0)
+    peak, peak_kind = measured_peaks()
+    sweep_s = prof["sweep_ms"] / 1e3
+    achieved = steps_done * bstep / sweep_s / 1e9 if sweep_s > 0 else None
+    traffic = ncu_traffic_per_step()
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        rate, dt = cpu_mde_rate(nthreads, 4)
+        cpu = {"value": rate, "unit": "MDE steps/s", "cores": nthreads, "kind": "port",
+               "sample": f"{nthreads} threads x 4 step_exp calls of the FP64 C oracle on the 32^3 grid "
+                         f"({dt:.1f} s)"}
+    line = {
+        "metric": "MDE steps/s", "value": value, "unit": "MDE steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "batch_per_gpu": B, "grid": [N_GRID] * 3,
+                   "contour_steps_per_chain": s0.contour_steps(), "parallelism": f"instances x{world}",
+                   "l2": "inputs larger than L2 (propagator slabs %.1f GB per GPU)" % (B * 2 * 103 * s0.nr * 8 / 1e9)},
+        "solves_per_s": conv_all / solve_s_all, "solve_seconds": solve_s_all, "solves_converged": int(conv_all),
+        "solve_iterations": {"min": int(min(itrs)), "max": int(max(itrs)), "mean": float(np.mean(itrs))},
+        "f_helmholtz": {"min": float(min(fvals)), "max": float(max(fvals))},
+        "cell_param": {"min": float(min(cells)), "max": float(max(cells))},
+        "e2e": {"value": e2e_value, "unit": "MDE steps/s", "api": "pscfg_density + pscfg_stress (host buffers)",
+                "h2d_bytes_per_step": int(omega0.nbytes), "d2h_bytes_per_step": int(omega0.nbytes + q.nbytes + stress.nbytes)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                     "traffic": traffic, "kernel": "MDE step (sweep kernels)",
+                     "bytes_per_step": bstep, "sweep_ms": prof["sweep_ms"], "steps": steps_done},
+        "phase_ms": {k: prof[k] for k in ("sweep_ms", "contour_ms", "stress_ms")},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -158,6 +158,36 @@ int pscfg_free_energy(pscfg_engine *e, double *out, double *mu_chain);
 int pscfg_iterate_am(pscfg_engine *e, double *omega, const pscfg_am_param *prm, double *rho,
                      pscfg_am_result *results);
 
+/* Stepwise form of pscfg_iterate_am for callers that interleave their own
+ * work or time single iterations: pscfg_am_begin loads omega (host, or
+ * NULL to keep the engine's fields) and runs the initial density;
+ * pscfg_am_iterate runs up to `iters` iterations of every unfinished
+ * instance and returns how many are still iterating; pscfg_am_results
+ * writes the per-instance results and, when non-NULL, omega/rho (host). */
+int pscfg_am_begin(pscfg_engine *e, const double *omega, const pscfg_am_param *prm);
+int pscfg_am_iterate(pscfg_engine *e, int iters, int *remaining);
+int pscfg_am_results(pscfg_engine *e, double *omega, double *rho, pscfg_am_result *results);
+
+/* Impose a space group on instance `inst`: omega is projected onto the
+ * group-invariant fields (the span of the reference's symmetry-adapted
+ * star basis, src/basis_mod.f90 / src/grid_basis_mod.f90:47-200) at the
+ * start of an Anderson run and after every mixing step.  ops: [nops][12]
+ * ints, 9 entries of the integer grid-index matrix M (row major) then 3 of
+ * the translation t in grid units: i -> M i + t (mod n).  nops = 0 removes
+ * the constraint. */
+int pscfg_set_symmetry(pscfg_engine *e, int inst, int nops, const int *ops);
+
+/* The CUDA stream (cudaStream_t) every kernel of this engine runs on. */
+void *pscfg_stream(const pscfg_engine *e);
+
+/* Phase timing with CUDA events on the engine stream (the reference's
+ * cpu_time stopwatches scf_time/basis_time, src/pscf.fp.f90:492-494, per
+ * phase).  pscfg_set_profiling(e, 1) resets and enables the accumulators;
+ * pscfg_get_profile writes out[6] = {sweep ms, contour-integral ms,
+ * stress ms, mixing ms, MDE steps in the timed sweeps, sweep launches}. */
+int pscfg_set_profiling(pscfg_engine *e, int on);
+int pscfg_get_profile(const pscfg_engine *e, double *out);
+
 /* nsteps applications of step_exp (src/step_mod.f90:146-176) to q for
  * instance `inst`, with the tables of make_propg(ds, b, ksq, omega_m)
  * (src/step_mod.f90:109-129).  omega_m, q_in, q_out: host [nr]. */

@@ -112,6 +112,8 @@ def lib():
         L.orc_fft_c2c.argtypes = [ip, dp, C.c_int]
         L.orc_am_deviation.argtypes = [C.POINTER(OrcSystem), C.c_long, dp, dp, dp]
         L.orc_am_deviation.restype = C.c_double
+        L.orc_set_symmetry.argtypes = [vp, C.c_int, ip, ip]
+        L.orc_symmetrize.argtypes = [vp, dp]
         L.orc_density_batch.argtypes = [C.POINTER(OrcSystem), C.c_int, dp, vp, C.c_int]
         _lib = L
     return _lib
@@ -227,6 +229,17 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+    def set_symmetry(self, M, t):
+        """Impose a space group: M int [nops,3,3], t int [nops,3] (grid units)."""
+        M = np.ascontiguousarray(M, np.int32)
+        t = np.ascontiguousarray(t, np.int32)
+        lib().orc_set_symmetry(self._c, len(M), M.reshape(-1), t.reshape(-1))
+
+    def symmetrize(self, field):
+        f = np.ascontiguousarray(field, np.float64).ravel().copy()
+        lib().orc_symmetrize(self._c, f)
+        return f
 
     def set_cell(self, cell_param):
         self.cell_param = list(cell_param)

@@ -511,6 +511,10 @@ typedef struct {
     int *gbz;
     double qout[ORC_MAXC];
     double qsolv[ORC_MAXS];
+    double *kweight;    /* [nk] star-basis weights r(G) (1 without a group) */
+    int nops;           /* space-group elements (0: no symmetry imposed) */
+    int *symM;          /* [nops][3][3] integer action on grid indices   */
+    int *symt;          /* [nops][3] translation in grid units           */
 } orc_ctx;
 
 orc_ctx *orc_create(const orc_system *sys)
@@ -533,7 +537,86 @@ void orc_destroy(orc_ctx *c)
     stepper_free(&c->st);
     for (int i = 0; i < c->sys.n_chain; i++) chain_work_free(&c->ch[i]);
     free(c->ksq); free(c->gbz);
+    free(c->symM); free(c->symt); free(c->kweight);
     free(c);
+}
+
+/* Space-group projection on the grid.  The reference keeps fields in a
+ * symmetry-adapted star basis (src/basis_mod.f90, src/grid_basis_mod.f90);
+ * on the grid the same subspace is reached by averaging f over the orbit
+ * i -> M i + t (mod n) of every grid point. */
+void orc_set_symmetry(orc_ctx *c, int nops, const int *M, const int *t)
+{
+    free(c->symM); free(c->symt);
+    c->symM = NULL; c->symt = NULL;
+    c->nops = nops;
+    if (nops <= 0) { c->nops = 0; free(c->kweight); c->kweight = NULL; return; }
+    c->symM = malloc(sizeof(int) * 9 * nops);
+    c->symt = malloc(sizeof(int) * 3 * nops);
+    memcpy(c->symM, M, sizeof(int) * 9 * nops);
+    memcpy(c->symt, t, sizeof(int) * 3 * nops);
+    /* Star weights.  A star is the orbit of a wave G under the point group,
+     * G -> G.m (src/group_mod.f90:77-78), on the FFT grid.  The reference
+     * normalises the star coefficients by sqrt(real(star_N)), a
+     * single-precision square root (src/basis_mod.f90:920), so every star
+     * sum over basis coefficients (free energy, stress) weights the star by
+     * r = fl32(sqrt(N))^2 / N instead of 1. */
+    const int *n = c->sys.n;
+    const int n1h = n[0] / 2 + 1;
+    if (!c->kweight) c->kweight = malloc(sizeof(double) * c->nk);
+    long *seen = malloc(sizeof(long) * nops);
+    for (int i3 = 0; i3 < n[2]; i3++)
+        for (int i2 = 0; i2 < n[1]; i2++)
+            for (int i1 = 0; i1 < n1h; i1++) {
+                int G[3] = {i1, i2, i3};
+                int cnt = 0;
+                for (int k = 0; k < nops; k++) {
+                    const int *m = M + 9 * k;
+                    long key = 0;
+                    for (int j = 0; j < 3; j++) {
+                        long v = 0;
+                        for (int i = 0; i < 3; i++) v += (long)G[i] * m[3 * i + j];
+                        v %= n[j];
+                        if (v < 0) v += n[j];
+                        key = key * n[j] + v;
+                    }
+                    int dup = 0;
+                    for (int q = 0; q < cnt; q++) if (seen[q] == key) { dup = 1; break; }
+                    if (!dup) seen[cnt++] = key;
+                }
+                float sf = sqrtf((float)cnt);
+                c->kweight[i1 + (long)n1h * (i2 + (long)n[1] * i3)] = ((double)sf * (double)sf) / (double)cnt;
+            }
+    free(seen);
+}
+
+void orc_symmetrize(orc_ctx *c, double *f)
+{
+    if (c->nops <= 0) return;
+    const int *n = c->sys.n;
+    const long nr = c->nr;
+    double *acc = malloc(sizeof(double) * nr);
+    for (int i3 = 0; i3 < n[2]; i3++)
+        for (int i2 = 0; i2 < n[1]; i2++)
+            for (int i1 = 0; i1 < n[0]; i1++) {
+                double s = 0;
+                int idx[3] = {i1, i2, i3};
+                for (int k = 0; k < c->nops; k++) {
+                    const int *M = c->symM + 9 * k, *t = c->symt + 3 * k;
+                    int j[3];
+                    for (int a = 0; a < 3; a++) {
+                        long v = t[a];
+                        for (int b = 0; b < 3; b++) v += (long)M[3 * a + b] * idx[b];
+                        v %= n[a];
+                        if (v < 0) v += n[a];
+                        j[a] = (int)v;
+                    }
+                    s += f[j[0] + (long)n[0] * (j[1] + (long)n[1] * j[2])];
+                }
+                acc[i1 + (long)n[0] * (i2 + (long)n[1] * i3)] = s / c->nops;
+            }
+    memcpy(f, acc, sizeof(double) * nr);
+    free(acc);
 }
 
 /* New cell: G_basis and dGG (the caller runs make_unit_cell) and rebuild k^2
@@ -628,6 +711,7 @@ int orc_stress(orc_ctx *c, double *stress)
     for (long k = 0; k < nk; k++) {
         int i1 = (int)(k % n1h);
         wk[k] = (i1 == 0 || (n1 % 2 == 0 && i1 == n1 / 2)) ? 1.0 : 2.0;
+        if (c->kweight) wk[k] *= c->kweight[k];
         const int *G = c->gbz + 3 * k;
         for (int b = 0; b < ncp; b++) {
             double v = 0;
@@ -687,15 +771,38 @@ int orc_free_energy(orc_ctx *c, const double *omega, const double *rho, double *
     for (int i = 0; i < s->n_solvent; i++)
         if (s->phi_solvent[i] > 1.0e-8) f = f + s->phi_solvent[i] * (s->mu_solvent[i] - 1.0) / s->solvent_size[i];
     double acc = 0;
-    for (long r = 0; r < nr; r++) {
-        double t = 0;
-        for (int a = 0; a < s->n_monomer; a++) {
-            for (int b = a + 1; b < s->n_monomer; b++) t += rho[(long)a * nr + r] * s->chi[a][b] * rho[(long)b * nr + r];
-            t -= omega[(long)a * nr + r] * rho[(long)a * nr + r];
+    if (!c->kweight) {
+        for (long r = 0; r < nr; r++) {
+            double t = 0;
+            for (int a = 0; a < s->n_monomer; a++) {
+                for (int b = a + 1; b < s->n_monomer; b++) t += rho[(long)a * nr + r] * s->chi[a][b] * rho[(long)b * nr + r];
+                t -= omega[(long)a * nr + r] * rho[(long)a * nr + r];
+            }
+            acc += t;
         }
-        acc += t;
+        f += acc / (double)nr;
+    } else {
+        /* star sums of src/scf_mod.fp.f90:861-869 with the star weights */
+        const long nk = c->nk;
+        const int M = s->n_monomer, n1 = s->n[0], n1h = n1 / 2 + 1;
+        cplx *R = malloc(sizeof(cplx) * nk * M), *W = malloc(sizeof(cplx) * nk * M);
+        for (int a = 0; a < M; a++) {
+            fft3d_r2c(&c->st.f, rho + (long)a * nr, R + (long)a * nk);
+            fft3d_r2c(&c->st.f, omega + (long)a * nr, W + (long)a * nk);
+        }
+        for (long k = 0; k < nk; k++) {
+            int i1 = (int)(k % n1h);
+            double w = (i1 == 0 || (n1 % 2 == 0 && i1 == n1 / 2)) ? 1.0 : 2.0;
+            double t = 0;
+            for (int a = 0; a < M; a++) {
+                for (int b = a + 1; b < M; b++) t += s->chi[a][b] * creal(R[a * nk + k] * conj(R[b * nk + k]));
+                t -= creal(W[a * nk + k] * conj(R[a * nk + k]));
+            }
+            acc += w * c->kweight[k] * t;
+        }
+        f += acc / ((double)nr * (double)nr);
+        free(R); free(W);
     }
-    f += acc / (double)nr;
     double p = -f;
     for (int i = 0; i < s->n_chain; i++) {
         double L = 0;
@@ -948,6 +1055,7 @@ int orc_iterate_am(orc_ctx *c, double *omega, double *cell_param, const orc_am_p
     memset(devcp, 0, sizeof(devcp)); memset(cph, 0, sizeof(cph));
     double qo[ORC_MAXC], qs[ORC_MAXS];
 
+    for (int a = 0; a < M; a++) orc_symmetrize(c, omega + (long)a * nr);
     orc_density(c, omega, rho, qo, qs);
     mu_phi(c);
     if (s->ensemble == 0) {
@@ -1033,6 +1141,7 @@ int orc_iterate_am(orc_ctx *c, double *omega, double *cell_param, const orc_am_p
                 cell_param[k] = ww + lam * dd;
             }
         }
+        for (int a = 0; a < M; a++) orc_symmetrize(c, omega + (long)a * nr);
         if (itr < H + 1) {
             memcpy(omh + (long)itr * fl, omega, sizeof(double) * fl);
             for (int k = 0; k < ncp; k++) cph[itr][k] = cell_param[k];

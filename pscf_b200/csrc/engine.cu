@@ -67,6 +67,10 @@ struct Inst {
     bool have_density = false;
     // Anderson
     double *om_hist = nullptr, *dev_hist = nullptr;
+    // space group imposed on omega (0 ops: none)
+    int nops = 0;
+    int *d_ops = nullptr;
+    double *kweight = nullptr;    // [nk] star weights (nullptr: exact Parseval weights)
 };
 
 struct Engine {
@@ -80,6 +84,12 @@ struct Engine {
     std::string err;
     long launches = 0;
     int n_hist_alloc = 0;
+    // optional CUDA-event timing of the phases (ms, accumulated)
+    bool profiling = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double t_sweep = 0, t_contour = 0, t_stress = 0, t_mix = 0;
+    long n_steps_timed = 0;     // MDE steps in the timed sweeps
+    long sweep_launches = 0;
 
     // FFT plan / twiddle tables
     PlaneGeom g64, g32;
@@ -88,10 +98,13 @@ struct Engine {
     // descriptor scratch (device), grown on demand
     void *d_desc = nullptr;
     size_t d_desc_bytes = 0;
+    size_t geom_off = (size_t)8 << 20;   // descriptor offset reserved for geometry jobs
     double *d_part = nullptr;
     size_t d_part_len = 0;
     double *d_small = nullptr;   // scalars [n_inst][64]
     void *spec = nullptr;        // 3-D stress spectra scratch
+    void *fe_spec = nullptr;     // spectra for the star-weighted free energy
+    size_t fe_spec_bytes = 0;
     size_t spec_bytes = 0;
     double *stress_part = nullptr;
     size_t stress_part_len = 0;
@@ -103,7 +116,10 @@ struct Engine {
         if (d_part) cudaFree(d_part);
         if (d_small) cudaFree(d_small);
         if (spec) cudaFree(spec);
+        if (fe_spec) cudaFree(fe_spec);
         if (stress_part) cudaFree(stress_part);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -239,19 +255,60 @@ static void validate_system(const pscfg_system &s, int dim, const int n[3])
             throw Err(PSCFG_EINVAL, "solvent_monomer out of range");
 }
 
+// New unit cell for a set of instances: G_basis/dGG on the host
+// (make_unit_cell), k^2 and stress weights on the device (k_make_geom).
+static void update_cells(Engine &E, const std::vector<int> &which)
+{
+    if (which.empty()) return;
+    std::vector<GeomJob> jobs;
+    for (int i : which) {
+        Inst &I = E.inst[i];
+        Cell c;
+        if (!make_unit_cell(E.dim, I.sys.crystal_system, I.sys.cell_param, c))
+            throw Err(PSCFG_EINVAL, "unknown crystal system for this dimension");
+        I.cell = c;
+        GeomJob j;
+        std::memset(&j, 0, sizeof(j));
+        std::memcpy(j.G, c.G, sizeof(j.G));
+        std::memcpy(j.dGG, c.dGG, sizeof(j.dGG));
+        j.ncp = c.ncp;
+        j.ksq = I.ksq;
+        j.wdgsq = I.wdgsq;
+        j.kweight = I.kweight;
+        jobs.push_back(j);
+        I.have_density = false;
+    }
+    GeomJob *dj = E.upload(jobs, E.geom_off);
+    dim3 grid((unsigned)std::min<long>((E.nk + 255) / 256, 512), (unsigned)jobs.size());
+    k_make_geom<<<grid, 256, 0, E.st>>>(dj, E.dim, E.n[0], E.n[1], E.n[2]);
+    E.launched();
+}
+
 static void upload_cell(Engine &E, Inst &I)
 {
-    Cell c;
-    if (!make_unit_cell(E.dim, I.sys.crystal_system, I.sys.cell_param, c))
-        throw Err(PSCFG_EINVAL, "unknown crystal system for this dimension");
-    I.cell = c;
-    std::vector<double> ksq, wd;
-    make_ksq_dgsq(E.dim, E.n, c, ksq, wd);
-    CK(cudaMemcpyAsync(I.ksq, ksq.data(), ksq.size() * sizeof(double), cudaMemcpyHostToDevice, E.st));
-    CK(cudaMemcpyAsync(I.wdgsq, wd.data(), wd.size() * sizeof(double), cudaMemcpyHostToDevice, E.st));
+    update_cells(E, std::vector<int>{(int)(&I - &E.inst[0])});
     CK(cudaStreamSynchronize(E.st));
-    I.have_density = false;
 }
+
+// Phase timer: events recorded on the engine stream around a phase.
+struct PhaseTimer {
+    Engine &E;
+    double *acc;
+    PhaseTimer(Engine &e, double *a) : E(e), acc(a)
+    {
+        if (E.profiling) CK(cudaEventRecord(E.ev0, E.st));
+    }
+    ~PhaseTimer() noexcept(false)
+    {
+        if (E.profiling) {
+            CK(cudaEventRecord(E.ev1, E.st));
+            CK(cudaEventSynchronize(E.ev1));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, E.ev0, E.ev1));
+            *acc += ms;
+        }
+    }
+};
 
 static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int precision)
 {
@@ -268,8 +325,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     E.M = sys[0].n_monomer;
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
-    if (precision == PSCFG_FP64) make_geom<double>(E, E.g64);
-    else make_geom<float>(E, E.g32);
+    make_geom<double>(E, E.g64);
+    if (precision == PSCFG_FP32) make_geom<float>(E, E.g32);
 
     const size_t ts = E.tsize();
     E.inst.resize(n_inst);
@@ -308,7 +365,12 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
                 }
             }
         }
-        upload_cell(E, I);
+    }
+    {
+        std::vector<int> all(n_inst);
+        for (int i = 0; i < n_inst; i++) all[i] = i;
+        update_cells(E, all);
+        CK(cudaStreamSynchronize(E.st));
     }
     E.d_small = nullptr;
     CK(cudaMalloc(&E.d_small, sizeof(double) * 64 * n_inst));
@@ -506,7 +568,17 @@ static void run_contour(Engine &E, const std::vector<int> &act)
 template <typename T>
 static void density_impl(Engine &E, const std::vector<int> &act)
 {
-    run_sweeps<T>(E, act);
+    {
+        long l0 = E.launches;
+        PhaseTimer pt(E, &E.t_sweep);
+        run_sweeps<T>(E, act);
+        if (E.profiling) {
+            for (int i : act)
+                for (int c = 0; c < E.inst[i].sys.n_chain; c++) E.n_steps_timed += 2L * E.inst[i].ns[c];
+            E.sweep_launches += E.launches - l0;
+        }
+    }
+    PhaseTimer pt(E, &E.t_contour);
     run_contour<T>(E, act);
 }
 
@@ -630,6 +702,7 @@ static void stress_all(Engine &E, const std::vector<int> &act)
 {
     for (int i : act)
         if (!E.inst[i].have_density) throw Err(PSCFG_ESTATE, "stress requires a preceding density call");
+    PhaseTimer pt(E, &E.t_stress);
     if (E.prec == PSCFG_FP64) stress_impl<double>(E, act);
     else stress_impl<float>(E, act);
 }
@@ -637,30 +710,121 @@ static void stress_all(Engine &E, const std::vector<int> &act)
 // ---------------------------------------------------------------------
 // Free energy (src/scf_mod.fp.f90:834-886)
 // ---------------------------------------------------------------------
+// Field term sum_k w r [..] / nr^2 for instances with star weights, from
+// the spectra of rho and omega (FP64 forward FFTs).
+static void fe_spectral(Engine &E, const std::vector<int> &which, std::vector<double> &terms)
+{
+    const PlaneGeom &g = E.g64;
+    const int M = E.M;
+    const size_t per = (size_t)2 * M * E.nk * sizeof(cx<double>);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(which.size(), ((size_t)512 << 20) / per));
+    if (E.fe_spec_bytes < per * chunk) {
+        if (E.fe_spec) cudaFree(E.fe_spec);
+        E.fe_spec = nullptr;
+        CK(cudaMalloc(&E.fe_spec, per * chunk));
+        E.fe_spec_bytes = per * chunk;
+    }
+    terms.assign(which.size(), 0.0);
+    const int nct = red_ctas(E.nk);
+    for (size_t c0 = 0; c0 < which.size(); c0 += chunk) {
+        const int cn = (int)std::min<size_t>(chunk, which.size() - c0);
+        std::vector<const double *> src;
+        std::vector<cx<double> *> dst;
+        std::vector<FeSpecJob> jobs;
+        cx<double> *base = (cx<double> *)E.fe_spec;
+        for (int k = 0; k < cn; k++) {
+            Inst &I = E.inst[which[c0 + k]];
+            FeSpecJob j;
+            std::memset(&j, 0, sizeof(j));
+            for (int a = 0; a < M; a++) {
+                cx<double> *R = base + ((size_t)k * 2 * M + a) * E.nk;
+                cx<double> *W = base + ((size_t)k * 2 * M + M + a) * E.nk;
+                src.push_back(I.rho + (long)a * E.nr);
+                dst.push_back(R);
+                src.push_back(I.omega + (long)a * E.nr);
+                dst.push_back(W);
+                j.R[a] = R;
+                j.W[a] = W;
+            }
+            j.kweight = I.kweight;
+            j.M = M;
+            for (int a = 0; a < M; a++)
+                for (int b = 0; b < M; b++) j.chi[a][b] = I.sys.chi[a][b];
+            jobs.push_back(j);
+        }
+        const double **dsrc = (const double **)E.upload(src, 0);
+        size_t off = ((src.size() * sizeof(void *) + 255) / 256) * 256;
+        cx<double> **ddst = (cx<double> **)E.upload(dst, off);
+        off += ((dst.size() * sizeof(void *) + 255) / 256) * 256;
+        FeSpecJob *dj = E.upload(jobs, off);
+        const int nf = (int)src.size();
+        size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<double>);
+        if (E.dim <= 2) {
+            CK(cudaFuncSetAttribute(k2_fft_fields, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
+            k2_fft_fields<<<nf, threads, smxy, E.st>>>(dsrc, ddst, g);
+            E.launched();
+        } else {
+            const long P = (long)g.n1h * g.n2;
+            const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+            size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<double>);
+            CK(cudaFuncSetAttribute(k3_fft_fields_xy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(cudaFuncSetAttribute(k3_fft_fields_z<Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+            k3_fft_fields_xy<<<dim3(g.n3, nf), 256, smxy, E.st>>>(dsrc, ddst, g);
+            E.launched();
+            k3_fft_fields_z<Z_TILE><<<dim3(ntile, nf), 256, smz, E.st>>>(ddst, g);
+            E.launched();
+        }
+        double *part = E.part((size_t)nct * cn);
+        k_fe_spectral<<<dim3(nct, cn), 256, 0, E.st>>>(dj, E.nk, E.n[0], part);
+        E.launched();
+        const double rn2 = (double)E.nr * (double)E.nr;
+        k_final_sum<<<(unsigned)((cn + 127) / 128), 128, 0, E.st>>>(part, nct, rn2, E.d_small, cn);
+        E.launched();
+        CK(cudaMemcpyAsync(terms.data() + c0, E.d_small, sizeof(double) * cn, cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+    }
+}
+
 static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p)
 {
-    std::vector<FieldJob> fj;
-    for (int i : act) {
-        Inst &I = E.inst[i];
-        FieldJob j;
-        std::memset(&j, 0, sizeof(j));
-        j.omega = I.omega;
-        j.rho = I.rho;
-        j.M = I.sys.n_monomer;
-        for (int a = 0; a < j.M; a++)
-            for (int b = 0; b < j.M; b++) j.chi[a][b] = I.sys.chi[a][b];
-        fj.push_back(j);
+    std::vector<int> plain, weighted;
+    std::vector<size_t> pos_plain, pos_w;
+    for (size_t k = 0; k < act.size(); k++) {
+        if (E.inst[act[k]].kweight) { weighted.push_back(act[k]); pos_w.push_back(k); }
+        else { plain.push_back(act[k]); pos_plain.push_back(k); }
     }
-    FieldJob *dj = E.upload(fj, 0);
-    const int nct = red_ctas(E.nr);
-    double *part = E.part((size_t)nct * fj.size());
-    k_fe_partial<<<dim3(nct, (unsigned)fj.size()), 256, 0, E.st>>>(dj, E.nr, part);
-    E.launched();
-    k_final_sum<<<(unsigned)((fj.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small, (int)fj.size());
-    E.launched();
-    std::vector<double> terms(fj.size());
-    CK(cudaMemcpyAsync(terms.data(), E.d_small, sizeof(double) * fj.size(), cudaMemcpyDeviceToHost, E.st));
-    CK(cudaStreamSynchronize(E.st));
+    std::vector<double> terms(act.size(), 0.0);
+    if (!plain.empty()) {
+        std::vector<FieldJob> fj;
+        for (int i : plain) {
+            Inst &I = E.inst[i];
+            FieldJob j;
+            std::memset(&j, 0, sizeof(j));
+            j.omega = I.omega;
+            j.rho = I.rho;
+            j.M = I.sys.n_monomer;
+            for (int a = 0; a < j.M; a++)
+                for (int b = 0; b < j.M; b++) j.chi[a][b] = I.sys.chi[a][b];
+            fj.push_back(j);
+        }
+        FieldJob *dj = E.upload(fj, 0);
+        const int nct = red_ctas(E.nr);
+        double *part = E.part((size_t)nct * fj.size());
+        k_fe_partial<<<dim3(nct, (unsigned)fj.size()), 256, 0, E.st>>>(dj, E.nr, part);
+        E.launched();
+        k_final_sum<<<(unsigned)((fj.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small, (int)fj.size());
+        E.launched();
+        std::vector<double> t(fj.size());
+        CK(cudaMemcpyAsync(t.data(), E.d_small, sizeof(double) * fj.size(), cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+        for (size_t k = 0; k < plain.size(); k++) terms[pos_plain[k]] = t[k];
+    }
+    if (!weighted.empty()) {
+        std::vector<double> t;
+        fe_spectral(E, weighted, t);
+        for (size_t k = 0; k < weighted.size(); k++) terms[pos_w[k]] = t[k];
+    }
     f.assign(act.size(), 0.0);
     p.assign(act.size(), 0.0);
     for (size_t k = 0; k < act.size(); k++) {
@@ -723,11 +887,45 @@ static bool solve_dense(int n, std::vector<double> &U, std::vector<double> &v)
     return true;
 }
 
-static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<pscfg_am_result> &res)
+struct AmRun {
+    bool active = false;
+    pscfg_am_param prm;
+    std::vector<AmState> st;
+};
+
+// Space-group projection of omega for the given instances, into dst slots
+// (dst[i] may alias nothing of omega); then copied back into omega.
+static void symmetrize_omega(Engine &E, const std::vector<int> &which, const std::vector<double *> &dst)
+{
+    std::vector<SymJob> jobs;
+    std::vector<std::pair<double *, double *>> back;
+    for (size_t k = 0; k < which.size(); k++) {
+        Inst &I = E.inst[which[k]];
+        if (I.nops <= 0) continue;
+        SymJob j;
+        j.src = I.omega;
+        j.dst = dst[k];
+        j.ops = I.d_ops;
+        j.nops = I.nops;
+        j.M = E.M;
+        jobs.push_back(j);
+        back.push_back({I.omega, dst[k]});
+    }
+    if (jobs.empty()) return;
+    SymJob *dj = E.upload(jobs, E.geom_off + ((size_t)1 << 20));
+    dim3 grid((unsigned)std::min<long>((E.nr + 255) / 256, 512), (unsigned)jobs.size());
+    k_symmetrize<<<grid, 256, 0, E.st>>>(dj, E.n[0], E.n[1], E.n[2]);
+    E.launched();
+    const long fl = (long)E.M * E.nr;
+    for (auto &b : back) CK(cudaMemcpyAsync(b.first, b.second, sizeof(double) * fl, cudaMemcpyDeviceToDevice, E.st));
+}
+
+static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
 {
     const int H = prm.n_hist;
     if (H < 1 || H > PSCFG_MAXH - 1) throw Err(PSCFG_EINVAL, "n_hist out of range");
-    const int S = H + 1;                 // ring slots
+    if (prm.max_itr < 0) throw Err(PSCFG_EINVAL, "max_itr must be >= 0");
+    const int S = H + 1;
     const long fl = (long)E.M * E.nr;
     const int ninst = (int)E.inst.size();
     if (E.n_hist_alloc < S) {
@@ -737,51 +935,69 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
         }
         E.n_hist_alloc = S;
     }
-    std::vector<AmState> st(ninst);
+    R.prm = prm;
+    R.st.assign(ninst, AmState());
     std::vector<int> all(ninst);
-    for (int i = 0; i < ninst; i++) all[i] = i;
-    const double large = 100.0;
-
-    // initial density (src/iterate_mod.fp.f90:1123-1128), then the uniform
-    // component of omega (set_omega_uniform, src/scf_mod.fp.f90:724-750)
-    density_all(E, all);
-    {
-        std::vector<double> w(fl);
-        for (int i = 0; i < ninst; i++) {
-            Inst &I = E.inst[i];
-            CK(cudaMemcpyAsync(w.data(), I.omega, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
-            CK(cudaStreamSynchronize(E.st));
-            double phi_mon[PSCFG_MAXM] = {0};
-            for (int c = 0; c < I.sys.n_chain; c++)
-                for (int b = 0; b < I.sys.n_block[c]; b++)
-                    phi_mon[I.sys.block_monomer[c][b]] += I.sys.phi_chain[c] * I.sys.block_length[c][b] / I.length[c];
-            for (int s = 0; s < I.sys.n_solvent; s++) phi_mon[I.sys.solvent_monomer[s]] += I.sys.phi_solvent[s];
-            for (int a = 0; a < E.M; a++) {
-                double w0 = 0;
-                for (int b = 0; b < E.M; b++) w0 = w0 + I.sys.chi[a][b] * phi_mon[b];
-                double m = 0;
-                for (long r = 0; r < E.nr; r++) m += w[a * E.nr + r];
-                m /= (double)E.nr;
-                for (long r = 0; r < E.nr; r++) w[a * E.nr + r] += w0 - m;
-            }
-            CK(cudaMemcpyAsync(I.omega, w.data(), sizeof(double) * fl, cudaMemcpyHostToDevice, E.st));
-            CK(cudaMemcpyAsync(I.om_hist, I.omega, sizeof(double) * fl, cudaMemcpyDeviceToDevice, E.st));
-            st[i].gram.assign((size_t)S * S, 0.0);
-            st[i].devcp.assign(S, std::vector<double>(PSCFG_MAXCP, 0.0));
-            st[i].cph.assign(S, std::vector<double>(PSCFG_MAXCP, 0.0));
-            for (int k = 0; k < I.cell.ncp; k++) st[i].cph[0][k] = I.sys.cell_param[k];
-            st[i].head = 0;
-            st[i].nstore = 0;   // om_hist slot 0 holds omega; dev not yet
-        }
-        CK(cudaStreamSynchronize(E.st));
+    std::vector<double *> scratch(ninst);
+    for (int i = 0; i < ninst; i++) {
+        all[i] = i;
+        scratch[i] = E.inst[i].om_hist;
     }
+    // symmetric initial guess, then the first density (src/iterate_mod.fp.f90:1123)
+    symmetrize_omega(E, all, scratch);
+    density_all(E, all);
+    // uniform component of omega (set_omega_uniform, src/scf_mod.fp.f90:724-750)
+    std::vector<double> w(fl);
+    for (int i = 0; i < ninst; i++) {
+        Inst &I = E.inst[i];
+        CK(cudaMemcpyAsync(w.data(), I.omega, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+        double phi_mon[PSCFG_MAXM] = {0};
+        for (int c = 0; c < I.sys.n_chain; c++)
+            for (int b = 0; b < I.sys.n_block[c]; b++)
+                phi_mon[I.sys.block_monomer[c][b]] += I.sys.phi_chain[c] * I.sys.block_length[c][b] / I.length[c];
+        for (int sv = 0; sv < I.sys.n_solvent; sv++) phi_mon[I.sys.solvent_monomer[sv]] += I.sys.phi_solvent[sv];
+        for (int a = 0; a < E.M; a++) {
+            double w0 = 0;
+            for (int b = 0; b < E.M; b++) w0 = w0 + I.sys.chi[a][b] * phi_mon[b];
+            double m = 0;
+            for (long r = 0; r < E.nr; r++) m += w[a * E.nr + r];
+            m /= (double)E.nr;
+            for (long r = 0; r < E.nr; r++) w[a * E.nr + r] += w0 - m;
+        }
+        CK(cudaMemcpyAsync(I.omega, w.data(), sizeof(double) * fl, cudaMemcpyHostToDevice, E.st));
+        CK(cudaMemcpyAsync(I.om_hist, I.omega, sizeof(double) * fl, cudaMemcpyDeviceToDevice, E.st));
+        AmState &st = R.st[i];
+        st.gram.assign((size_t)S * S, 0.0);
+        st.devcp.assign(S, std::vector<double>(PSCFG_MAXCP, 0.0));
+        st.cph.assign(S, std::vector<double>(PSCFG_MAXCP, 0.0));
+        for (int k = 0; k < I.cell.ncp; k++) st.cph[0][k] = I.sys.cell_param[k];
+        st.head = 0;
+        st.nstore = 0;
+    }
+    CK(cudaStreamSynchronize(E.st));
+    R.active = true;
+}
 
+// Up to `iters` Anderson iterations of every unfinished instance; returns
+// the number of instances still iterating.
+static int am_iterate(Engine &E, AmRun &R, int iters)
+{
+    if (!R.active) throw Err(PSCFG_ESTATE, "no Anderson run in progress");
+    const pscfg_am_param &prm = R.prm;
+    const int H = prm.n_hist, S = H + 1;
+    const long fl = (long)E.M * E.nr;
+    const int ninst = (int)E.inst.size();
+    const double large = 100.0;
     const int nct = red_ctas(E.nr);
+    std::vector<AmState> &st = R.st;
     std::vector<double> hsmall;
-    for (;;) {
+    int remaining = 0;
+    for (int it = 0; it < iters; it++) {
         std::vector<int> act;
         for (int i = 0; i < ninst; i++)
             if (!st[i].done) act.push_back(i);
+        remaining = (int)act.size();
         if (act.empty()) break;
         const int na = (int)act.size();
         for (int i : act) st[i].itr++;
@@ -796,8 +1012,7 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
                 CK(cudaMemcpyAsync(&sh[(size_t)k * PSCFG_MAXCP], E.inst[act[k]].stress_dev, sizeof(double) * PSCFG_MAXCP,
                                    cudaMemcpyDeviceToHost, E.st));
         }
-        // slot of this iteration's deviation: ring position after head
-        // (head points at the om_hist entry of the current omega)
+        // deviations into the ring slot of the current omega
         std::vector<AmJob> aj;
         for (int k = 0; k < na; k++) {
             Inst &I = E.inst[act[k]];
@@ -813,7 +1028,9 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
         }
         AmJob *daj = E.upload(aj, 0);
         size_t off = ((aj.size() * sizeof(AmJob) + 255) / 256) * 256;
-        double *part = E.part((size_t)nct * na * PSCFG_MAXM + 16);
+        double *part = E.part((size_t)nct * na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1) + 64);
+        double *mpart = part + (size_t)nct * na * PSCFG_MAXM;
+        double *dpart = mpart + (size_t)nct * na;
         k_am_dev<<<dim3(nct, na), 256, 0, E.st>>>(daj, E.nr, part);
         E.launched();
         k_final_sum<<<(unsigned)((na * PSCFG_MAXM + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small,
@@ -829,15 +1046,11 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
         }
         AmFix *dfx = E.upload(fx, off);
         off += ((fx.size() * sizeof(AmFix) + 255) / 256) * 256;
-        double *part2 = part + (size_t)nct * na * PSCFG_MAXM;
-        (void)part2;
-        double *mpart = E.part((size_t)nct * na * (PSCFG_MAXM + 1) + 16) + (size_t)nct * na * PSCFG_MAXM;
         k_am_fix<<<dim3(nct, na), 256, 0, E.st>>>(dfx, E.nr, mpart);
         E.launched();
         double *emax = E.d_small + (size_t)na * PSCFG_MAXM;
         k_final_max<<<(unsigned)((na + 127) / 128), 128, 0, E.st>>>(mpart, nct, emax, na);
         E.launched();
-        // dots of the new deviation with every stored deviation (incl. itself)
         std::vector<AmDot> dots;
         for (int k = 0; k < na; k++) {
             int i = act[k];
@@ -848,20 +1061,16 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
             int nst = std::min(st[i].nstore + 1, S);
             d.nh = nst;
             for (int h = 0; h < nst; h++) {
-                int slot = ((st[i].head - h) % S + S) % S;   // h = 0 is the current slot
+                int slot = ((st[i].head - h) % S + S) % S;
                 d.hist[h] = E.inst[i].dev_hist + (long)slot * fl;
             }
             dots.push_back(d);
         }
-        // recompute the dev pointers after the mean fix (same buffers)
         AmDot *ddot = E.upload(dots, off);
         off += ((dots.size() * sizeof(AmDot) + 255) / 256) * 256;
-        double *dpart = E.part((size_t)nct * na * (PSCFG_MAXH + 1) + (size_t)nct * na * (PSCFG_MAXM + 1) + 16) +
-                        (size_t)nct * na * (PSCFG_MAXM + 1);
         k_am_dots<<<dim3(nct, na), 256, 0, E.st>>>(ddot, dpart);
         E.launched();
         double *dres = E.d_small + (size_t)na * (PSCFG_MAXM + 1);
-        if ((size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1) > (size_t)64 * ninst) throw Err(PSCFG_EINVAL, "scratch");
         k_final_sum<<<(unsigned)((na * (PSCFG_MAXH + 1) + 127) / 128), 128, 0, E.st>>>(dpart, nct, 1.0, dres,
                                                                                        na * (PSCFG_MAXH + 1));
         E.launched();
@@ -879,7 +1088,6 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
             s.f = fe[k];
             s.p = pe[k];
             for (int b = 0; b < PSCFG_MAXCP; b++) s.stress[b] = sh[(size_t)k * PSCFG_MAXCP + b];
-            // update gram ring with <d_cur, d_h>/nr
             const double *g = &hsmall[(size_t)na * (PSCFG_MAXM + 1) + (size_t)k * (PSCFG_MAXH + 1)];
             int nst = std::min(s.nstore + 1, S);
             for (int h = 0; h < nst; h++) {
@@ -896,7 +1104,7 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
             if (s.error < prm.error_max) { s.converged = true; s.done = true; continue; }
             if (s.itr > prm.max_itr || !(s.error <= 100.0 * large)) { s.done = true; continue; }
 
-            // lambda and number of previous entries (src/iterate_mod.fp.f90:1147-1153)
+            // lambda and history depth (src/iterate_mod.fp.f90:1147-1153)
             int itr_prev;
             double lam;
             if (s.itr < H + 1) { itr_prev = s.itr - 1; lam = 1.0 - std::pow(0.9, s.itr); }
@@ -914,6 +1122,7 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
                 m.n = 0;
                 for (int b = 0; b < ncp; b++) cp_new[b] = I.sys.cell_param[b] + lam * s.devcp[cur][b];
             } else {
+                // U_mn, V_m (src/iterate_mod.fp.f90:1349-1381) from the Gram ring
                 const int n = itr_prev;
                 std::vector<double> U((size_t)n * n), V(n);
                 auto G = [&](int a, int b) { return s.gram[(size_t)a * S + b]; };
@@ -955,21 +1164,38 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
             AmMix *dm = E.upload(mixes, 0);
             k_am_mix<<<dim3(nct, (unsigned)mixes.size()), 256, 0, E.st>>>(dm);
             E.launched();
+            std::vector<double *> slots;
             for (int i : mix_inst) {
                 AmState &s = st[i];
-                Inst &I = E.inst[i];
                 s.head = (s.head + 1) % S;
-                CK(cudaMemcpyAsync(I.om_hist + (long)s.head * fl, I.omega, sizeof(double) * fl, cudaMemcpyDeviceToDevice,
-                                   E.st));
-                for (int b = 0; b < I.cell.ncp; b++) s.cph[s.head][b] = I.sys.cell_param[b];
-                if (prm.domain) upload_cell(E, I);
+                slots.push_back(E.inst[i].om_hist + (long)s.head * fl);
+                for (int b = 0; b < E.inst[i].cell.ncp; b++) s.cph[s.head][b] = E.inst[i].sys.cell_param[b];
             }
-            CK(cudaStreamSynchronize(E.st));
+            // symmetric omega (the reference's star basis), recorded in the history
+            symmetrize_omega(E, mix_inst, slots);
+            for (size_t k = 0; k < mix_inst.size(); k++) {
+                Inst &I = E.inst[mix_inst[k]];
+                if (I.nops <= 0)
+                    CK(cudaMemcpyAsync(slots[k], I.omega, sizeof(double) * fl, cudaMemcpyDeviceToDevice, E.st));
+            }
+            if (prm.domain) update_cells(E, mix_inst);
         }
+        remaining = 0;
+        for (int i = 0; i < ninst; i++)
+            if (!st[i].done) remaining++;
     }
-    if (!prm.domain) stress_all(E, all);
-    std::vector<double> shost((size_t)ninst * PSCFG_MAXCP);
-    if (!prm.domain) {
+    return remaining;
+}
+
+static void am_results(Engine &E, AmRun &R, std::vector<pscfg_am_result> &res)
+{
+    if (!R.active) throw Err(PSCFG_ESTATE, "no Anderson run in progress");
+    const int ninst = (int)E.inst.size();
+    std::vector<int> all(ninst);
+    for (int i = 0; i < ninst; i++) all[i] = i;
+    std::vector<double> shost((size_t)ninst * PSCFG_MAXCP, 0.0);
+    if (!R.prm.domain) {
+        stress_all(E, all);
         for (int i = 0; i < ninst; i++)
             CK(cudaMemcpyAsync(&shost[(size_t)i * PSCFG_MAXCP], E.inst[i].stress_dev, sizeof(double) * PSCFG_MAXCP,
                                cudaMemcpyDeviceToHost, E.st));
@@ -979,7 +1205,7 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
     for (int i = 0; i < ninst; i++) {
         pscfg_am_result &r = res[i];
         std::memset(&r, 0, sizeof(r));
-        AmState &s = st[i];
+        AmState &s = R.st[i];
         Inst &I = E.inst[i];
         r.itr = s.itr;
         r.converged = s.converged ? 1 : 0;
@@ -987,7 +1213,7 @@ static void iterate_am_impl(Engine &E, const pscfg_am_param &prm, std::vector<ps
         r.f_helmholtz = s.f;
         r.pressure = s.p;
         for (int b = 0; b < I.cell.ncp; b++) {
-            r.stress[b] = prm.domain ? s.stress[b] : shost[(size_t)i * PSCFG_MAXCP + b];
+            r.stress[b] = R.prm.domain ? s.stress[b] : shost[(size_t)i * PSCFG_MAXCP + b];
             r.cell_param[b] = I.sys.cell_param[b];
         }
         for (int c = 0; c < I.sys.n_chain; c++) {
@@ -1107,6 +1333,7 @@ using namespace pscfg;
 
 struct pscfg_engine {
     Engine E;
+    AmRun am;
 };
 
 #define ABI_BEGIN try {
@@ -1258,30 +1485,160 @@ int pscfg_free_energy(pscfg_engine *e, double *out, double *mu_chain)
     ABI_END(e)
 }
 
+static void load_omega(Engine &E, const double *omega)
+{
+    const long fl = (long)E.M * E.nr;
+    for (size_t i = 0; i < E.inst.size(); i++)
+        CK(cudaMemcpyAsync(E.inst[i].omega, omega + (long)i * fl, sizeof(double) * fl, cudaMemcpyHostToDevice, E.st));
+}
+
+static void store_fields(Engine &E, double *omega, double *rho)
+{
+    const long fl = (long)E.M * E.nr;
+    for (size_t i = 0; i < E.inst.size(); i++) {
+        if (omega) CK(cudaMemcpyAsync(omega + (long)i * fl, E.inst[i].omega, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
+        if (rho) CK(cudaMemcpyAsync(rho + (long)i * fl, E.inst[i].rho, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
+    }
+    CK(cudaStreamSynchronize(E.st));
+}
+
 int pscfg_iterate_am(pscfg_engine *e, double *omega, const pscfg_am_param *prm, double *rho, pscfg_am_result *results)
 {
     if (!e || !omega || !prm || !results) return PSCFG_EINVAL;
     ABI_BEGIN
     Engine &E = e->E;
-    const long fl = (long)E.M * E.nr;
-    const int ni = (int)E.inst.size();
-    for (int i = 0; i < ni; i++)
-        CK(cudaMemcpyAsync(E.inst[i].omega, omega + (long)i * fl, sizeof(double) * fl, cudaMemcpyHostToDevice, E.st));
+    load_omega(E, omega);
+    am_begin(E, e->am, *prm);
+    while (am_iterate(E, e->am, 1 << 30) > 0) {
+    }
     std::vector<pscfg_am_result> res;
-    iterate_am_impl(E, *prm, res);
+    am_results(E, e->am, res);
+    e->am.active = false;
     int any_fail = 0;
-    for (int i = 0; i < ni; i++) {
+    for (size_t i = 0; i < res.size(); i++) {
         results[i] = res[i];
         if (!res[i].converged) any_fail = 1;
-        CK(cudaMemcpyAsync(omega + (long)i * fl, E.inst[i].omega, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
-        if (rho) CK(cudaMemcpyAsync(rho + (long)i * fl, E.inst[i].rho, sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
     }
-    CK(cudaStreamSynchronize(E.st));
+    store_fields(E, omega, rho);
     if (any_fail) {
         E.err = "at least one instance did not converge";
         return PSCFG_ENOTCONV;
     }
     ABI_END(e)
+}
+
+int pscfg_am_begin(pscfg_engine *e, const double *omega, const pscfg_am_param *prm)
+{
+    if (!e || !prm) return PSCFG_EINVAL;
+    ABI_BEGIN
+    if (omega) load_omega(e->E, omega);
+    am_begin(e->E, e->am, *prm);
+    ABI_END(e)
+}
+
+int pscfg_am_iterate(pscfg_engine *e, int iters, int *remaining)
+{
+    if (!e || iters < 0) return PSCFG_EINVAL;
+    ABI_BEGIN
+    int r = am_iterate(e->E, e->am, iters);
+    if (remaining) *remaining = r;
+    ABI_END(e)
+}
+
+int pscfg_am_results(pscfg_engine *e, double *omega, double *rho, pscfg_am_result *results)
+{
+    if (!e || !results) return PSCFG_EINVAL;
+    ABI_BEGIN
+    std::vector<pscfg_am_result> res;
+    am_results(e->E, e->am, res);
+    for (size_t i = 0; i < res.size(); i++) results[i] = res[i];
+    store_fields(e->E, omega, rho);
+    ABI_END(e)
+}
+
+int pscfg_set_symmetry(pscfg_engine *e, int inst, int nops, const int *ops)
+{
+    if (!e || nops < 0 || (nops > 0 && !ops)) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    if (inst < 0 || inst >= (int)E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
+    Inst &I = E.inst[inst];
+    if (nops > 1024) throw Err(PSCFG_EINVAL, "too many group elements");
+    if (nops > 0) {
+        I.d_ops = (int *)E.dalloc(sizeof(int) * 12 * nops);
+        CK(cudaMemcpyAsync(I.d_ops, ops, sizeof(int) * 12 * nops, cudaMemcpyHostToDevice, E.st));
+        // Star weights: a star is the orbit of a wave G under the point
+        // group (G -> G.m, src/group_mod.f90:77-78) on the FFT grid; the
+        // reference normalises its star coefficients with a single-precision
+        // sqrt(real(star_N)) (src/basis_mod.f90:920), so its star sums weight
+        // a star of N waves by fl32(sqrt(N))^2 / N.
+        std::vector<double> kw(E.nk);
+        std::vector<long> seen(nops);
+        const int n1h = E.n[0] / 2 + 1;
+        for (int i3 = 0; i3 < E.n[2]; i3++)
+            for (int i2 = 0; i2 < E.n[1]; i2++)
+                for (int i1 = 0; i1 < n1h; i1++) {
+                    const int G[3] = {i1, i2, i3};
+                    int cnt = 0;
+                    for (int k = 0; k < nops; k++) {
+                        const int *m = ops + 12 * k;
+                        long key = 0;
+                        for (int j = 0; j < 3; j++) {
+                            long v = 0;
+                            for (int i = 0; i < 3; i++) v += (long)G[i] * m[3 * i + j];
+                            v %= E.n[j];
+                            if (v < 0) v += E.n[j];
+                            key = key * E.n[j] + v;
+                        }
+                        bool dup = false;
+                        for (int q = 0; q < cnt; q++)
+                            if (seen[q] == key) { dup = true; break; }
+                        if (!dup) seen[cnt++] = key;
+                    }
+                    const float sf = std::sqrt((float)cnt);
+                    kw[i1 + (long)n1h * (i2 + (long)E.n[1] * i3)] = ((double)sf * (double)sf) / (double)cnt;
+                }
+        if (!I.kweight) I.kweight = (double *)E.dalloc(sizeof(double) * E.nk);
+        CK(cudaMemcpyAsync(I.kweight, kw.data(), sizeof(double) * E.nk, cudaMemcpyHostToDevice, E.st));
+        CK(cudaStreamSynchronize(E.st));
+    } else {
+        I.kweight = nullptr;
+    }
+    I.nops = nops;
+    update_cells(E, std::vector<int>{inst});
+    CK(cudaStreamSynchronize(E.st));
+    ABI_END(e)
+}
+
+void *pscfg_stream(const pscfg_engine *e) { return e ? (void *)e->E.st : nullptr; }
+
+int pscfg_set_profiling(pscfg_engine *e, int on)
+{
+    if (!e) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    if (on && !E.ev0) {
+        CK(cudaEventCreate(&E.ev0));
+        CK(cudaEventCreate(&E.ev1));
+    }
+    E.profiling = on != 0;
+    E.t_sweep = E.t_contour = E.t_stress = E.t_mix = 0;
+    E.n_steps_timed = 0;
+    E.sweep_launches = 0;
+    ABI_END(e)
+}
+
+int pscfg_get_profile(const pscfg_engine *e, double *out)
+{
+    if (!e || !out) return PSCFG_EINVAL;
+    const Engine &E = e->E;
+    out[0] = E.t_sweep;
+    out[1] = E.t_contour;
+    out[2] = E.t_stress;
+    out[3] = E.t_mix;
+    out[4] = (double)E.n_steps_timed;
+    out[5] = (double)E.sweep_launches;
+    return PSCFG_OK;
 }
 
 int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, double ds, const double *q_in,

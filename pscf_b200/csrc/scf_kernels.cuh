@@ -381,3 +381,203 @@ __global__ void k_am_mix(const AmMix *jobs)
 }
 
 }  // namespace pscfg
+
+namespace pscfg {
+
+// ---------------------------------------------------------------------
+// k^2 and stress weights on the device (make_ksq + G_to_bz,
+// src/grid_mod.f90:141-160, 225-283; make_dGsq src/basis_mod.f90:1993-2014).
+// One thread per half-grid point; the 3^dim images are tried in the
+// reference order (+1, 0, -1 per used dimension) with the 1e-8 tie rule.
+// ---------------------------------------------------------------------
+struct GeomJob {
+    double G[3][3];
+    double dGG[PSCFG_MAXCP][3][3];
+    int ncp;
+    double *ksq;     // [nk]
+    double *wdgsq;   // [PSCFG_MAXCP][nk]
+    const double *kweight;   // [nk] star weights or nullptr (all 1)
+};
+
+__device__ __forceinline__ double gnorm_dev(int dim, const int Gt[3], const double G[3][3])
+{
+    double v0 = 0, v1 = 0, v2 = 0;
+    for (int i = 0; i < dim; i++) {
+        v0 += Gt[i] * G[i][0];
+        v1 += Gt[i] * G[i][1];
+        v2 += Gt[i] * G[i][2];
+    }
+    double s = v0 * v0;
+    if (dim > 1) s += v1 * v1;
+    if (dim > 2) s += v2 * v2;
+    return s;
+}
+
+__global__ void k_make_geom(const GeomJob *jobs, int dim, int n1, int n2, int n3)
+{
+    const GeomJob &J = jobs[blockIdx.y];
+    const int n1h = n1 / 2 + 1;
+    const long nk = (long)n1h * n2 * n3;
+    const int n[3] = {n1, n2, n3};
+    for (long idx = (long)blockIdx.x * blockDim.x + threadIdx.x; idx < nk; idx += (long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(idx % n1h);
+        const int i2 = (int)((idx / n1h) % n2);
+        const int i3 = (int)(idx / ((long)n1h * n2));
+        const int Gin[3] = {i1, i2, i3};
+        int Gmin[3] = {0, 0, 0}, Gt[3] = {0, 0, 0};
+        double gmin = 1.0e10;
+        const int h0 = 1, h1 = dim > 1 ? 1 : 0, h2 = dim > 2 ? 1 : 0;
+        for (int a = h0; a >= -h0; a--) {
+            Gt[0] = Gin[0] + a * n[0];
+            for (int b = h1; b >= -h1; b--) {
+                Gt[1] = dim > 1 ? Gin[1] + b * n[1] : 0;
+                for (int c = h2; c >= -h2; c--) {
+                    Gt[2] = dim > 2 ? Gin[2] + c * n[2] : 0;
+                    double g = gnorm_dev(dim, Gt, J.G);
+                    if (g < gmin - 1.0e-8) {
+                        Gmin[0] = Gt[0];
+                        Gmin[1] = Gt[1];
+                        Gmin[2] = Gt[2];
+                        gmin = g;
+                    }
+                }
+            }
+        }
+        J.ksq[idx] = gnorm_dev(dim, Gmin, J.G);
+        double w = (i1 == 0 || (n1 % 2 == 0 && i1 == n1 / 2)) ? 1.0 : 2.0;
+        if (J.kweight) w *= J.kweight[idx];
+        for (int b = 0; b < PSCFG_MAXCP; b++) {
+            double v = 0;
+            if (b < J.ncp)
+                for (int j = 0; j < dim; j++)
+                    for (int l = 0; l < dim; l++) v += (double)Gmin[j] * (double)Gmin[l] * J.dGG[b][j][l];
+            J.wdgsq[(long)b * nk + idx] = w * v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------
+// Space-group projection: dst[a](i) = mean over ops of src[a](M i + t mod n).
+// ops: [nops][12] = 9 entries of M (row major) + 3 of t.
+// ---------------------------------------------------------------------
+struct SymJob {
+    const double *src;
+    double *dst;
+    const int *ops;
+    int nops;
+    int M;
+};
+
+__global__ void k_symmetrize(const SymJob *jobs, int n1, int n2, int n3)
+{
+    const SymJob &J = jobs[blockIdx.y];
+    const long nr = (long)n1 * n2 * n3;
+    const int n[3] = {n1, n2, n3};
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += (long)gridDim.x * blockDim.x) {
+        const int i[3] = {(int)(r % n1), (int)((r / n1) % n2), (int)(r / ((long)n1 * n2))};
+        double acc[PSCFG_MAXM] = {0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < J.nops; k++) {
+            const int *o = J.ops + 12 * k;
+            int j[3];
+            for (int a = 0; a < 3; a++) {
+                int v = o[9 + a] + o[3 * a] * i[0] + o[3 * a + 1] * i[1] + o[3 * a + 2] * i[2];
+                v %= n[a];
+                if (v < 0) v += n[a];
+                j[a] = v;
+            }
+            const long rr = j[0] + (long)n1 * (j[1] + (long)n2 * j[2]);
+            for (int a = 0; a < J.M; a++) acc[a] += J.src[(long)a * nr + rr];
+        }
+        for (int a = 0; a < J.M; a++) J.dst[(long)a * nr + r] = acc[a] / (double)J.nops;
+    }
+}
+
+}  // namespace pscfg
+
+namespace pscfg {
+
+// ---------------------------------------------------------------------
+// Forward r2c of FP64 grid fields into compact half spectra [nk]
+// (layout [z][y][kx]).  Used by the star-weighted free energy.
+// ---------------------------------------------------------------------
+__global__ void k2_fft_fields(const double *const *src, cx<double> *const *dst, PlaneGeom g)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<double> *A = (cx<double> *)smem_raw;
+    cx<double> *B = A + g.n2 * g.LS;
+    const double *f = src[blockIdx.x];
+    pack_rows<double>(A, g, [&](int r) { return f[r]; });
+    cx<double> *F = plane_forward<double>(A, B, g);
+    store_plane<double>(dst[blockIdx.x], F, g);
+}
+
+__global__ void k3_fft_fields_xy(const double *const *src, cx<double> *const *dst, PlaneGeom g)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<double> *A = (cx<double> *)smem_raw;
+    cx<double> *B = A + g.n2 * g.LS;
+    const int z = blockIdx.x;
+    const long np = (long)g.n1 * g.n2, nkp = (long)g.n1h * g.n2;
+    const double *f = src[blockIdx.y] + z * np;
+    pack_rows<double>(A, g, [&](int r) { return f[r]; });
+    cx<double> *F = plane_forward<double>(A, B, g);
+    store_plane<double>(dst[blockIdx.y] + z * nkp, F, g);
+}
+
+template <int TC>
+__global__ void k3_fft_fields_z(cx<double> *const *dst, PlaneGeom g)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<double> *A = (cx<double> *)smem_raw;
+    cx<double> *B = A + g.n3 * TC;
+    cx<double> *S = dst[blockIdx.y];
+    const long P = (long)g.n1h * g.n2;
+    const long c0 = (long)blockIdx.x * TC;
+    const int nc = (int)min((long)TC, P - c0);
+    for (int i = threadIdx.x; i < g.n3 * TC; i += blockDim.x) {
+        int z = i / TC, c = i - z * TC;
+        A[i] = (c < nc) ? S[z * P + c0 + c] : mk<double>(0.0, 0.0);
+    }
+    cx<double> *F = fft_lines<-1, double>(A, B, g.zp, TC, TC, 1, true);
+    for (int i = threadIdx.x; i < g.n3 * TC; i += blockDim.x) {
+        int z = i / TC, c = i - z * TC;
+        if (c < nc) S[z * P + c0 + c] = F[i];
+    }
+}
+
+// Star-weighted field term of the free energy (src/scf_mod.fp.f90:861-869
+// with the star weights of the reference basis): per instance
+//   sum_k w(kx) r(k) [ sum_{a<b} chi_ab Re(R_a R_b*) - sum_a Re(W_a R_a*) ]
+struct FeSpecJob {
+    const cx<double> *R[PSCFG_MAXM], *W[PSCFG_MAXM];
+    const double *kweight;
+    double chi[PSCFG_MAXM][PSCFG_MAXM];
+    int M;
+};
+
+__global__ void k_fe_spectral(const FeSpecJob *jobs, long nk, int n1, double *part)
+{
+    __shared__ double red[32];
+    const FeSpecJob &J = jobs[blockIdx.y];
+    const int n1h = n1 / 2 + 1;
+    double acc = 0.0;
+    for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += (long)gridDim.x * blockDim.x) {
+        const int i1 = (int)(k % n1h);
+        const double w = (i1 == 0 || ((n1 & 1) == 0 && i1 == n1 / 2)) ? 1.0 : 2.0;
+        double t = 0.0;
+        for (int a = 0; a < J.M; a++) {
+            const cx<double> ra = J.R[a][k];
+            for (int b = a + 1; b < J.M; b++) {
+                const cx<double> rb = J.R[b][k];
+                t += J.chi[a][b] * (ra.x * rb.x + ra.y * rb.y);
+            }
+            const cx<double> wa = J.W[a][k];
+            t -= wa.x * ra.x + wa.y * ra.y;
+        }
+        acc += w * (J.kweight ? J.kweight[k] : 1.0) * t;
+    }
+    acc = block_sum(acc, red);
+    if (threadIdx.x == 0) part[(long)blockIdx.y * gridDim.x + blockIdx.x] = acc;
+}
+
+}  // namespace pscfg

@@ -92,6 +92,13 @@ SIGNATURES = {
     "pscfg_iterate_am": (C.c_int, [_vp, _dp, C.POINTER(PscfgAmParam), _dp, C.POINTER(PscfgAmResult)]),
     "pscfg_propagate": (C.c_int, [_vp, C.c_int, _dp, C.c_double, C.c_double, _dp, _dp, C.c_int]),
     "pscfg_get_propagators": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]),
+    "pscfg_am_begin": (C.c_int, [_vp, _dp, C.POINTER(PscfgAmParam)]),
+    "pscfg_am_iterate": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
+    "pscfg_am_results": (C.c_int, [_vp, _dp, _dp, C.POINTER(PscfgAmResult)]),
+    "pscfg_set_symmetry": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "pscfg_stream": (C.c_void_p, [_vp]),
+    "pscfg_set_profiling": (C.c_int, [_vp, C.c_int]),
+    "pscfg_get_profile": (C.c_int, [_vp, _dp]),
     "pscfg_steps_per_density": (C.c_long, [_vp]),
     "pscfg_launch_count": (C.c_long, [_vp]),
 }
@@ -251,6 +258,22 @@ class Engine:
         prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max)
         res = (PscfgAmResult * self.n_inst)()
         self._check(self.lib.pscfg_iterate_am(self._h, _ptr(w), C.byref(prm), _ptr(rho), res), allow=(ENOTCONV,))
+        return w, rho, self._results(res, domain)
+
+    def set_symmetry(self, inst: int, group_name: str):
+        """Impose a space group (pscf_b200.groups) on instance `inst`."""
+        from .groups import grid_ops
+        s = self.systems[inst]
+        M, t = grid_ops(group_name, list(s.ngrid))
+        ops = np.zeros((len(M), 12), dtype=np.int32)
+        ops[:, :9] = M.reshape(len(M), 9)
+        ops[:, 9:] = t
+        self._check(self.lib.pscfg_set_symmetry(self._h, inst, len(M), ops.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def clear_symmetry(self, inst: int):
+        self._check(self.lib.pscfg_set_symmetry(self._h, inst, 0, None))
+
+    def _results(self, res, domain):
         out = []
         for i, r in enumerate(res):
             ncp = len(self.systems[i].cell_param)
@@ -261,7 +284,39 @@ class Engine:
                             q=list(r.q)[:nch], mu_chain=list(r.mu_chain)[:nch]))
             if domain:
                 self.systems[i].cell_param = list(r.cell_param)[:ncp]
-        return w, rho, out
+        return out
+
+    def am_begin(self, omega, error_max=1e-10, max_itr=1000, n_hist=20, domain=False):
+        w = None if omega is None else np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
+        self._am_domain = domain
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max)
+        self._check(self.lib.pscfg_am_begin(self._h, None if w is None else _ptr(w), C.byref(prm)))
+
+    def am_iterate(self, iters: int = 1) -> int:
+        rem = C.c_int(0)
+        self._check(self.lib.pscfg_am_iterate(self._h, iters, C.byref(rem)))
+        return rem.value
+
+    def am_results(self, want_fields=True):
+        res = (PscfgAmResult * self.n_inst)()
+        w = np.zeros((self.n_inst, self.M, self.nr)) if want_fields else None
+        rho = np.zeros((self.n_inst, self.M, self.nr)) if want_fields else None
+        self._check(self.lib.pscfg_am_results(self._h, None if w is None else _ptr(w),
+                                              None if rho is None else _ptr(rho), res))
+        return w, rho, self._results(res, getattr(self, "_am_domain", False))
+
+    def set_profiling(self, on: bool = True):
+        self._check(self.lib.pscfg_set_profiling(self._h, 1 if on else 0))
+
+    def profile(self) -> dict:
+        out = np.zeros(6)
+        self._check(self.lib.pscfg_get_profile(self._h, _ptr(out)))
+        return dict(sweep_ms=out[0], contour_ms=out[1], stress_ms=out[2], mix_ms=out[3],
+                    steps=int(out[4]), sweep_launches=int(out[5]))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.pscfg_stream(self._h) or 0)
 
     @property
     def steps_per_density(self) -> int:
