@@ -5,10 +5,14 @@ Workload (per GPU): a batch of B instances of the BCC sphere phase,
 space group I m -3 m on a 32^3 grid: AB diblock f_A = 0.25, chi N = 20,
 b_A = b_B = 1, ds = 0.01 (26 + 76 contour steps), cubic cell a = 3.9,
 Anderson mixing with 20 history vectors, cell relaxed by the stress, to a
-residual of 1e-10.  Initial fields: delta = -1.0 (g - <g>) with g the
-max-normalised sum of Gaussians (width 0.3 a) on the BCC sites and images,
-omega_A = chiN phi_B + delta, omega_B = chiN phi_A - delta, plus seeded
-N(0, 0.01) noise (seed 20261203 + 1 + instance).
+residual of 1e-10.  Initial fields from Gaussian sphere densities at the
+BCC sites: g is the max-normalised sum of Gaussians (width 0.3 a) over the
+sites and their images, the A density swing has amplitude 1.0, so
+omega_A - omega_B = -2 chiN (g - <g>) around the uniform values:
+omega_A = chiN phi_B + delta, omega_B = chiN phi_A - delta with
+delta = -chiN (g - <g>), plus seeded N(0, 0.01) noise (seed
+20261203 + 1 + instance).  (A swing of 1.0 in omega itself leads Anderson
+mixing to the disordered state at chiN = 20.)
 
 One bench step = one Anderson iteration of the whole batch: density
 (forward and backward MDE sweeps, Simpson contour integrals), stress,
@@ -72,7 +76,7 @@ def initial_omega(system, inst):
                     dx, dy, dz = X - c[0] - sx, Y - c[1] - sy, Z - c[2] - sz
                     g += np.exp(-(dx * dx + dy * dy + dz * dz) / (2 * sig * sig))
     g = g / g.max()
-    delta = -1.0 * (g - g.mean())
+    delta = -CHI_N * 1.0 * (g - g.mean())
     rng = np.random.default_rng(SEED + inst)
     w0 = system.omega_uniform()
     w = np.zeros((2, system.nr))
