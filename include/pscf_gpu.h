@@ -194,6 +194,39 @@ int pscfg_get_profile(const pscfg_engine *e, double *out);
 int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, double ds,
                     const double *q_in, double *q_out, int nsteps);
 
+/* Limits of pscfg_propagate_noalloc. */
+#define PSCFG_NOALLOC_MAX_NR 65536     /* grid points (n1*n2*n3) */
+#define PSCFG_NOALLOC_MAX_LINE 1024    /* points along any one axis */
+
+/* step_exp applied nsteps times (src/step_mod.f90:146-176), like
+ * pscfg_propagate, for callers that cannot let a library allocate device
+ * memory: hosts whose whole device budget is handed to their own memory
+ * pool (a Fortran host running many solver instances side by side, or a
+ * framework whose caching allocator owns the device) and therefore need
+ * every call to stay inside memory they already account for.  This entry
+ * point has no counterpart in the reference.
+ *
+ * It takes no engine handle and calls no cudaMalloc/cudaFree: its scratch
+ * (propagator tables, spectra, working slices, twiddles) is one file-scope
+ * device array of about 5.6 MB, sized for grids of at most
+ * PSCFG_NOALLOC_MAX_NR points and PSCFG_NOALLOC_MAX_LINE points per axis,
+ * which every GPU that loads the library holds until the process exits.
+ * Larger grids are rejected with PSCFG_EINVAL and a message from
+ * pscfg_last_error(NULL).  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: calls whose GPU work overlaps (other host threads, or streams with
+ * no ordering between them) race on it.  Each call overwrites every scratch
+ * entry it reads, so nothing carries over from the previous call.
+ *
+ * All arrays are device pointers, FP64, x-fastest: ksq_dev [nk] (the k^2
+ * table, e.g. from pscfg_get_ksq), omega_dev [nr] (the block's monomer
+ * field), q_in_dev / q_out_dev [nr] (may alias).  Work is queued on
+ * `stream` (a cudaStream_t, NULL for the default stream); the call returns
+ * without synchronising. */
+int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_dev, const double *omega_dev, double b,
+                            double ds, const double *q_in_dev, double *q_out_dev, int nsteps, void *stream);
+
 /* Stored propagators of chain `chain` of instance `inst` after a density
  * call (chain_grid_type%qf/qr, src/chain_mod.f90:39-50): host
  * [n_slices][nr] each (either may be NULL); returns the slice count in

@@ -31,6 +31,9 @@ namespace pscfg {
 
 static thread_local std::string g_create_error;
 
+// Error text of calls made without an engine handle, for pscfg_last_error(NULL).
+void set_global_error(const std::string &msg) { g_create_error = msg; }
+
 #define CK(call)                                                                                 \
     do {                                                                                         \
         cudaError_t _e = (call);                                                                 \

@@ -320,7 +320,7 @@ __global__ void k_partial_sum(const T *const *ptrs, long n, double *part)
 }
 
 // Fixed-order final reduction of npart partials per job: out[j] = sum/div.
-__global__ void k_final_sum(const double *part, int npart, double div, double *out, int njobs)
+static __global__ void k_final_sum(const double *part, int npart, double div, double *out, int njobs)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;
@@ -330,7 +330,7 @@ __global__ void k_final_sum(const double *part, int npart, double div, double *o
 }
 
 // Same, writing job j's result to *outs[j].
-__global__ void k_final_sum_ptr(const double *part, int npart, double div, double *const *outs, int njobs)
+static __global__ void k_final_sum_ptr(const double *part, int npart, double div, double *const *outs, int njobs)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;

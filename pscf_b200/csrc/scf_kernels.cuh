@@ -22,7 +22,7 @@ struct StressJob {
 
 // dim <= 2: one CTA per (job, slice); 4 plane buffers in shared memory.
 template <typename T>
-__global__ void k2_stress_slices(const StressJob<T> *jobs, PlaneGeom g)
+static __global__ void k2_stress_slices(const StressJob<T> *jobs, PlaneGeom g)
 {
     const StressJob<T> &J = jobs[blockIdx.y];
     const int s = blockIdx.x;
@@ -54,7 +54,7 @@ __global__ void k2_stress_slices(const StressJob<T> *jobs, PlaneGeom g)
 // dim 3, pass 1: xy-forward of slices [s0, s0+cs) of qf and qr into
 // spec[(slice-s0)*2 + fr][z][y][kx].  grid = (n3, cs, 2).
 template <typename T>
-__global__ void k3_stress_xy(const StressJob<T> *job, PlaneGeom g, int s0, cx<T> *spec)
+static __global__ void k3_stress_xy(const StressJob<T> *job, PlaneGeom g, int s0, cx<T> *spec)
 {
     const StressJob<T> &J = *job;
     const int s = s0 + blockIdx.y;
@@ -75,7 +75,7 @@ __global__ void k3_stress_xy(const StressJob<T> *job, PlaneGeom g, int s0, cx<T>
 // weighted dot products.  grid = (ntiles, cs).  Writes
 // part[((slice-s0)*ntiles + tile)*PSCFG_MAXCP + b].
 template <typename T, int TC>
-__global__ void k3_stress_z(const StressJob<T> *job, PlaneGeom g, int s0, const cx<T> *spec, double *part)
+static __global__ void k3_stress_z(const StressJob<T> *job, PlaneGeom g, int s0, const cx<T> *spec, double *part)
 {
     const StressJob<T> &J = *job;
     const int s = s0 + blockIdx.y;
@@ -111,7 +111,7 @@ __global__ void k3_stress_z(const StressJob<T> *job, PlaneGeom g, int s0, const 
 
 // dim 3, pass 3: fixed-order sum of tile partials -> inc.  grid = cs.
 template <typename T>
-__global__ void k3_stress_sum(const StressJob<T> *job, int s0, int ntiles, const double *part)
+static __global__ void k3_stress_sum(const StressJob<T> *job, int s0, int ntiles, const double *part)
 {
     const StressJob<T> &J = *job;
     const int s = s0 + blockIdx.x;
@@ -139,7 +139,7 @@ struct StressFinal {
     double *out;                        // [PSCFG_MAXCP]
 };
 
-__global__ void k_stress_final(const StressFinal *jobs, int n)
+static __global__ void k_stress_final(const StressFinal *jobs, int n)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -186,7 +186,7 @@ struct SolventJob {
     int grand;
 };
 
-__global__ void k_solvent_boltz_partial(const SolventJob *jobs, long nr, double *part)
+static __global__ void k_solvent_boltz_partial(const SolventJob *jobs, long nr, double *part)
 {
     __shared__ double red[32];
     const SolventJob &J = jobs[blockIdx.y];
@@ -197,7 +197,7 @@ __global__ void k_solvent_boltz_partial(const SolventJob *jobs, long nr, double 
     if (threadIdx.x == 0) part[(long)blockIdx.y * gridDim.x + blockIdx.x] = s;
 }
 
-__global__ void k_solvent_rho(const SolventJob *jobs, int njobs, long nr)
+static __global__ void k_solvent_rho(const SolventJob *jobs, int njobs, long nr)
 {
     for (int j = 0; j < njobs; j++) {
         const SolventJob &J = jobs[j];
@@ -208,7 +208,7 @@ __global__ void k_solvent_rho(const SolventJob *jobs, int njobs, long nr)
     }
 }
 
-__global__ void k_zero(double *p, long n)
+static __global__ void k_zero(double *p, long n)
 {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] = 0.0;
 }
@@ -224,7 +224,7 @@ struct FieldJob {
     int M;
 };
 
-__global__ void k_fe_partial(const FieldJob *jobs, long nr, double *part)
+static __global__ void k_fe_partial(const FieldJob *jobs, long nr, double *part)
 {
     __shared__ double red[32];
     const FieldJob &J = jobs[blockIdx.y];
@@ -254,7 +254,7 @@ struct AmJob {
 
 // dev_a = sum_b chi_ba rho_b + (sum_b omega_b [+ chi12 rho3 + chi23 rho1 + chi13 rho2])/M - omega_a;
 // partial sums of dev_a for the mean (uniform component removal).
-__global__ void k_am_dev(const AmJob *jobs, long nr, double *part)
+static __global__ void k_am_dev(const AmJob *jobs, long nr, double *part)
 {
     __shared__ double red[32];
     const AmJob &J = jobs[blockIdx.y];
@@ -290,7 +290,7 @@ struct AmFix {
     int M;
 };
 
-__global__ void k_am_fix(const AmFix *jobs, long nr, double *part)
+static __global__ void k_am_fix(const AmFix *jobs, long nr, double *part)
 {
     __shared__ double red[32];
     const AmFix &J = jobs[blockIdx.y];
@@ -315,7 +315,7 @@ __global__ void k_am_fix(const AmFix *jobs, long nr, double *part)
     }
 }
 
-__global__ void k_final_max(const double *part, int npart, double *out, int njobs)
+static __global__ void k_final_max(const double *part, int npart, double *out, int njobs)
 {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;
@@ -334,7 +334,7 @@ struct AmDot {
     long len;                           // M * nr
 };
 
-__global__ void k_am_dots(const AmDot *jobs, double *part)
+static __global__ void k_am_dots(const AmDot *jobs, double *part)
 {
     __shared__ double red[32];
     const AmDot &J = jobs[blockIdx.y];
@@ -366,7 +366,7 @@ struct AmMix {
     long len;
 };
 
-__global__ void k_am_mix(const AmMix *jobs)
+static __global__ void k_am_mix(const AmMix *jobs)
 {
     const AmMix &J = jobs[blockIdx.y];
     for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < J.len; r += (long)gridDim.x * blockDim.x) {
@@ -413,7 +413,7 @@ __device__ __forceinline__ double gnorm_dev(int dim, const int Gt[3], const doub
     return s;
 }
 
-__global__ void k_make_geom(const GeomJob *jobs, int dim, int n1, int n2, int n3)
+static __global__ void k_make_geom(const GeomJob *jobs, int dim, int n1, int n2, int n3)
 {
     const GeomJob &J = jobs[blockIdx.y];
     const int n1h = n1 / 2 + 1;
@@ -468,7 +468,7 @@ struct SymJob {
     int M;
 };
 
-__global__ void k_symmetrize(const SymJob *jobs, int n1, int n2, int n3)
+static __global__ void k_symmetrize(const SymJob *jobs, int n1, int n2, int n3)
 {
     const SymJob &J = jobs[blockIdx.y];
     const long nr = (long)n1 * n2 * n3;
@@ -500,7 +500,7 @@ namespace pscfg {
 // Forward r2c of FP64 grid fields into compact half spectra [nk]
 // (layout [z][y][kx]).  Used by the star-weighted free energy.
 // ---------------------------------------------------------------------
-__global__ void k2_fft_fields(const double *const *src, cx<double> *const *dst, PlaneGeom g)
+static __global__ void k2_fft_fields(const double *const *src, cx<double> *const *dst, PlaneGeom g)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<double> *A = (cx<double> *)smem_raw;
@@ -511,7 +511,7 @@ __global__ void k2_fft_fields(const double *const *src, cx<double> *const *dst, 
     store_plane<double>(dst[blockIdx.x], F, g);
 }
 
-__global__ void k3_fft_fields_xy(const double *const *src, cx<double> *const *dst, PlaneGeom g)
+static __global__ void k3_fft_fields_xy(const double *const *src, cx<double> *const *dst, PlaneGeom g)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<double> *A = (cx<double> *)smem_raw;
@@ -525,7 +525,7 @@ __global__ void k3_fft_fields_xy(const double *const *src, cx<double> *const *ds
 }
 
 template <int TC>
-__global__ void k3_fft_fields_z(cx<double> *const *dst, PlaneGeom g)
+static __global__ void k3_fft_fields_z(cx<double> *const *dst, PlaneGeom g)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<double> *A = (cx<double> *)smem_raw;
@@ -555,7 +555,7 @@ struct FeSpecJob {
     int M;
 };
 
-__global__ void k_fe_spectral(const FeSpecJob *jobs, long nk, int n1, double *part)
+static __global__ void k_fe_spectral(const FeSpecJob *jobs, long nk, int n1, double *part)
 {
     __shared__ double red[32];
     const FeSpecJob &J = jobs[blockIdx.y];

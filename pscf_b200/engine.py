@@ -99,6 +99,8 @@ SIGNATURES = {
     "pscfg_stream": (C.c_void_p, [_vp]),
     "pscfg_set_profiling": (C.c_int, [_vp, C.c_int]),
     "pscfg_get_profile": (C.c_int, [_vp, _dp]),
+    "pscfg_propagate_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), _vp, _vp, C.c_double, C.c_double,
+                                          _vp, _vp, C.c_int, _vp]),
     "pscfg_steps_per_density": (C.c_long, [_vp]),
     "pscfg_launch_count": (C.c_long, [_vp]),
 }
