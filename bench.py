@@ -5,14 +5,15 @@ Workload (per GPU): a batch of B instances of the BCC sphere phase,
 space group I m -3 m on a 32^3 grid: AB diblock f_A = 0.25, chi N = 20,
 b_A = b_B = 1, ds = 0.01 (26 + 76 contour steps), cubic cell a = 3.9,
 Anderson mixing with 20 history vectors, cell relaxed by the stress, to a
-residual of 1e-10.  Initial fields from Gaussian sphere densities at the
-BCC sites: g is the max-normalised sum of Gaussians (width 0.3 a) over the
-sites and their images, the A density swing has amplitude 1.0, so
-omega_A - omega_B = -2 chiN (g - <g>) around the uniform values:
-omega_A = chiN phi_B + delta, omega_B = chiN phi_A - delta with
-delta = -chiN (g - <g>), plus seeded N(0, 0.01) noise (seed
-20261203 + 1 + instance).  (A swing of 1.0 in omega itself leads Anderson
-mixing to the disordered state at chiN = 20.)
+residual of 1e-10.  Initial fields from sphere densities at the BCC sites:
+rho_A = (1 - tanh((d - R)/w))/2 with d the distance to the nearest site,
+edge width w = 0.05 a and R set so that <rho_A> = f_A (a density swing of
+1.0), omega_A - omega_B = chiN (1 - 2 rho_A) around the uniform values
+chiN phi_B, chiN phi_A, plus seeded N(0, 0.01) noise (seed
+20261203 + 1 + instance).  Diffuse Gaussians of width 0.3 a do not seed the
+sphere phase at chiN = 20 (Anderson mixing then converges to the
+disordered state); the sharp profile converges to BCC from the starting
+cell a = 3.9 (relaxed cell 1.9232, F = 2.6145888805).
 
 One bench step = one Anderson iteration of the whole batch: density
 (forward and backward MDE sweeps, Simpson contour integrals), stress,
@@ -65,24 +66,29 @@ def make_system():
 
 def initial_omega(system, inst):
     n = system.n[0]
+    a = system.cell_param[0]
     x = np.arange(n) / n
     Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
-    g = np.zeros_like(X)
-    sig = 0.3
+    d = np.full(X.shape, np.inf)
     for c in [(0.0, 0.0, 0.0), (0.5, 0.5, 0.5)]:
-        for sx in (-1, 0, 1):
-            for sy in (-1, 0, 1):
-                for sz in (-1, 0, 1):
-                    dx, dy, dz = X - c[0] - sx, Y - c[1] - sy, Z - c[2] - sz
-                    g += np.exp(-(dx * dx + dy * dy + dz * dz) / (2 * sig * sig))
-    g = g / g.max()
-    delta = -CHI_N * 1.0 * (g - g.mean())
+        dx, dy, dz = X - c[0], Y - c[1], Z - c[2]
+        dx, dy, dz = dx - np.round(dx), dy - np.round(dy), dz - np.round(dz)
+        d = np.minimum(d, a * np.sqrt(dx * dx + dy * dy + dz * dz))
+    w = 0.05 * a
+    lo, hi = 0.0, a
+    for _ in range(60):
+        R = 0.5 * (lo + hi)
+        m = np.mean(0.5 * (1 - np.tanh((d - R) / w)))
+        lo, hi = (R, hi) if m < F_A else (lo, R)
+    rho_a = 0.5 * (1 - np.tanh((d - R) / w))
+    delta = 0.5 * CHI_N * (1.0 - 2.0 * rho_a)
+    delta -= delta.mean()
     rng = np.random.default_rng(SEED + inst)
     w0 = system.omega_uniform()
-    w = np.zeros((2, system.nr))
-    w[0] = w0[0] + delta.ravel() + rng.normal(0.0, 0.01, system.nr)
-    w[1] = w0[1] - delta.ravel() + rng.normal(0.0, 0.01, system.nr)
-    return w
+    out = np.zeros((2, system.nr))
+    out[0] = w0[0] + delta.ravel() + rng.normal(0.0, 0.01, system.nr)
+    out[1] = w0[1] - delta.ravel() + rng.normal(0.0, 0.01, system.nr)
+    return out
 
 
 def bytes_per_step(system, wq=8, ww=8):

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +27,7 @@
 #include "../../include/pscf_gpu.h"
 #include "host_geom.h"
 #include "scf_kernels.cuh"
+#include "kernels3c.cuh"
 
 namespace pscfg {
 
@@ -87,6 +89,7 @@ struct Engine {
     std::string err;
     long launches = 0;
     int n_hist_alloc = 0;
+    bool no_fixed_kernels = false;   // force the run-time sized kernels (tests)
     // optional CUDA-event timing of the phases (ms, accumulated)
     bool profiling = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -234,6 +237,13 @@ static void upload_dft_constants()
     }
     CK(cudaMemcpyToSymbol(c_dft5, t5, sizeof(t5)));
     CK(cudaMemcpyToSymbol(c_dft7, t7, sizeof(t7)));
+    double w64[2][64];
+    for (int m = 0; m < 64; m++) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * m / 64.0L;
+        w64[0][m] = (double)cosl(a);
+        w64[1][m] = (double)sinl(a);
+    }
+    CK(cudaMemcpyToSymbol(c_w64, w64, sizeof(w64)));
 }
 
 // ---------------------------------------------------------------------
@@ -326,6 +336,12 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     E.nr = (long)E.n[0] * E.n[1] * E.n[2];
     E.nk = (long)(E.n[0] / 2 + 1) * E.n[1] * E.n[2];
     E.M = sys[0].n_monomer;
+    // PSCFG_GENERIC_KERNELS=1 forces the run-time sized step kernels (used by
+    // the tests that cross-check the two implementations)
+    {
+        const char *v = std::getenv("PSCFG_GENERIC_KERNELS");
+        E.no_fixed_kernels = v && v[0] && v[0] != '0';
+    }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
     make_geom<double>(E, E.g64);
@@ -384,6 +400,48 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
 // Density
 // ---------------------------------------------------------------------
 static int red_ctas(long n) { return (int)std::min<long>(std::max<long>((n + 255) / 256, 1), 64); }
+
+// One 3-D MDE step of every field with compile-time-shaped kernels.
+template <typename T, int N1, int N2, int N3, int PPC>
+static void step3c(Engine &E, const SweepField<T> *dfl, int nf, int t)
+{
+    constexpr int TC = (N3 >= 64) ? 16 : 32;
+    constexpr int P = N2 * (N1 / 2 + 1);
+    const PlaneGeom &g = E.geom();
+    const int ntile = (P + TC - 1) / TC;
+    const size_t sm = sizeof(cx<T>) * PPC * P;
+    static bool attr[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
+        CK(cudaFuncSetAttribute(k3c_fwd_pair<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(cudaFuncSetAttribute(k3c_inv_mid<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(cudaFuncSetAttribute(k3c_inv_final<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        if (dev >= 0 && dev < 64) attr[dev] = true;
+    }
+    k3c_fwd_pair<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, nf), 256, sm, E.st>>>(dfl, g, t);
+    E.launched();
+    k3c_zconv<T, N1, N2, N3, TC><<<dim3(ntile, nf, 2), 256, 0, E.st>>>(dfl, g, t, 3);
+    E.launched();
+    k3c_inv_mid<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, nf), 256, sm, E.st>>>(dfl, g, t);
+    E.launched();
+    k3c_zconv<T, N1, N2, N3, TC><<<dim3(ntile, nf, 1), 256, 0, E.st>>>(dfl, g, t, 2);
+    E.launched();
+    k3c_inv_final<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, nf), 256, sm, E.st>>>(dfl, g, t);
+    E.launched();
+}
+
+// Returns true if the grid has a compile-time-shaped step (and runs it).
+template <typename T>
+static bool step3_fixed(Engine &E, const SweepField<T> *dfl, int nf, int t)
+{
+    if (E.no_fixed_kernels) return false;
+    const int a = E.n[0], b = E.n[1], c = E.n[2];
+    if (a == 32 && b == 32 && c == 32) { step3c<T, 32, 32, 32, 8>(E, dfl, nf, t); return true; }
+    if (a == 16 && b == 16 && c == 16) { step3c<T, 16, 16, 16, 8>(E, dfl, nf, t); return true; }
+    if (a == 64 && b == 64 && c == 64) { step3c<T, 64, 64, 64, 1>(E, dfl, nf, t); return true; }
+    return false;
+}
 
 template <typename T>
 static void run_sweeps(Engine &E, const std::vector<int> &act)
@@ -466,6 +524,7 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
         const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
         const int txy = 256, tz = 256;
         for (int t = 0; t < ns_max; t++) {
+            if (step3_fixed<T>(E, dfl, nf, t)) continue;
             k3_fwd_pair<T><<<dim3(g.n3, nf), txy, smxy, E.st>>>(dfl, g, t);
             E.launched();
             k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 2), tz, smz, E.st>>>(dfl, g, t, 3);
@@ -606,6 +665,40 @@ static void density_all(Engine &E, const std::vector<int> &act)
 // ---------------------------------------------------------------------
 // Stress
 // ---------------------------------------------------------------------
+template <typename T, int N1, int N2, int N3, int PPC>
+static void stress3c(Engine &E, const StressJob<T> *dj, int s0, int cnt)
+{
+    constexpr int TC = 16;
+    constexpr int P = N2 * (N1 / 2 + 1);
+    const int ntile = (P + TC - 1) / TC;
+    const PlaneGeom &g = E.geom();
+    const size_t sm = sizeof(cx<T>) * PPC * P;
+    static bool attr[64] = {};
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
+        CK(cudaFuncSetAttribute(k3c_stress_xy<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        if (dev >= 0 && dev < 64) attr[dev] = true;
+    }
+    k3c_stress_xy<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, cnt, 2), 256, sm, E.st>>>(dj, g, s0, (cx<T> *)E.spec);
+    E.launched();
+    k3c_stress_z<T, N1, N2, N3, TC><<<dim3(ntile, cnt), 256, 0, E.st>>>(dj, g, s0, (const cx<T> *)E.spec, E.stress_part);
+    E.launched();
+    k3_stress_sum<T><<<cnt, 32, 0, E.st>>>(dj, s0, ntile, E.stress_part);
+    E.launched();
+}
+
+template <typename T>
+static bool stress3_fixed(Engine &E, const StressJob<T> *dj, int s0, int cnt)
+{
+    if (E.no_fixed_kernels) return false;
+    const int a = E.n[0], b = E.n[1], c = E.n[2];
+    if (a == 32 && b == 32 && c == 32) { stress3c<T, 32, 32, 32, 8>(E, dj, s0, cnt); return true; }
+    if (a == 16 && b == 16 && c == 16) { stress3c<T, 16, 16, 16, 8>(E, dj, s0, cnt); return true; }
+    if (a == 64 && b == 64 && c == 64) { stress3c<T, 64, 64, 64, 1>(E, dj, s0, cnt); return true; }
+    return false;
+}
+
 template <typename T>
 static void stress_impl(Engine &E, const std::vector<int> &act)
 {
@@ -662,6 +755,7 @@ static void stress_impl(Engine &E, const std::vector<int> &act)
         for (size_t jb = 0; jb < jobs.size(); jb++) {
             for (int s0 = 0; s0 < jobs[jb].nslices; s0 += cs) {
                 int cnt = std::min(cs, jobs[jb].nslices - s0);
+                if (stress3_fixed<T>(E, dj + jb, s0, cnt)) continue;
                 k3_stress_xy<T><<<dim3(g.n3, cnt, 2), 256, smxy, E.st>>>(dj + jb, g, s0, (cx<T> *)E.spec);
                 E.launched();
                 k3_stress_z<T, Z_TILE><<<dim3(ntile, cnt), 256, smz, E.st>>>(dj + jb, g, s0, (const cx<T> *)E.spec, E.stress_part);
@@ -1304,6 +1398,7 @@ static void propagate_impl(Engine &E, int inst, const double *omega_m, double b,
             const long P = (long)g.n1h * g.n2;
             const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
             for (int t = 0; t < nsteps; t++) {
+                if (step3_fixed<T>(E, dfl, 1, t)) continue;
                 k3_fwd_pair<T><<<dim3(g.n3, 1), 256, smxy, E.st>>>(dfl, g, t);
                 E.launched();
                 k3_zconv<T, Z_TILE><<<dim3(ntile, 1, 2), 256, smz, E.st>>>(dfl, g, t, 3);

@@ -29,6 +29,17 @@ template <typename T> __device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b)
 }
 template <typename T> __device__ __forceinline__ cx<T> conjg(cx<T> a) { return mk(a.x, -a.y); }
 template <typename T> __device__ __forceinline__ cx<T> scale(cx<T> a, T s) { return mk(a.x * s, a.y * s); }
+__device__ __forceinline__ cx<double> __ldg_cx(const cx<double> *p)
+{
+    double2 v = __ldg((const double2 *)p);
+    return mk<double>(v.x, v.y);
+}
+__device__ __forceinline__ cx<float> __ldg_cx(const cx<float> *p)
+{
+    float2 v = __ldg((const float2 *)p);
+    return mk<float>(v.x, v.y);
+}
+
 // multiply by (S * i), S = +1 or -1
 template <int S, typename T> __device__ __forceinline__ cx<T> mul_si(cx<T> a)
 {

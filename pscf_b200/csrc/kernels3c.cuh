@@ -1,0 +1,364 @@
+// kernels3c.cuh -- 3-D MDE step kernels for power-of-two grids with the
+// grid shape fixed at compile time (fft_ct.cuh transforms).
+//
+// Same five launches per step and the same algebra as the run-time sized
+// k3_* kernels (kernels.cuh), but each CTA owns PPC z-planes, every
+// transform is in place (no ping-pong buffer), and all index arithmetic is
+// constant.  Global spectra S1/S2 are stored [z][y'][kx] with y' the
+// transposed order a forward y-transform leaves (perm<N2>).
+#pragma once
+#include "fft_ct.cuh"
+#include "kernels.cuh"
+
+namespace pscfg {
+
+template <int N> __device__ __forceinline__ int iperm(int p)
+{
+    constexpr int P = Split<N>::P, Q = Split<N>::Q;
+    return p / Q + P * (p % Q);
+}
+
+// Lines of a stack of planes: line l of the stack lies at
+// (l / LPP) * PSTR + (l % LPP) * LSTR, elements ESTR apart.
+template <int N, int S, typename T, int NL, int LPP, int PSTR, int LSTR, int ESTR>
+__device__ __forceinline__ void stack_passA(cx<T> *buf, const cx<T> *__restrict__ tw)
+{
+    constexpr int P = Split<N>::P, Q = Split<N>::Q;
+    constexpr bool LF = LSTR < ESTR;   // consecutive threads take consecutive lines
+    for (int w = threadIdx.x; w < NL * Q; w += blockDim.x) {
+        const int l = LF ? w % NL : w / Q, n2 = LF ? w / NL : w % Q;
+        cx<T> *b = buf + (l / LPP) * PSTR + (l % LPP) * LSTR;
+        cx<T> v[P];
+        if (S < 0) {
+#pragma unroll
+            for (int n1 = 0; n1 < P; n1++) v[n1] = b[(Q * n1 + n2) * ESTR];
+            Dft<P, S, T>::run(v);
+            if (Q > 1) {
+#pragma unroll
+                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], __ldg_cx(tw + n2 * k1));
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < P; k1++) b[(Q * k1 + n2) * ESTR] = v[k1];
+        } else {
+#pragma unroll
+            for (int k1 = 0; k1 < P; k1++) v[k1] = b[(Q * k1 + n2) * ESTR];
+            if (Q > 1) {
+#pragma unroll
+                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], conjg(__ldg_cx(tw + n2 * k1)));
+            }
+            Dft<P, S, T>::run(v);
+#pragma unroll
+            for (int n1 = 0; n1 < P; n1++) b[(Q * n1 + n2) * ESTR] = v[n1];
+        }
+    }
+}
+
+template <int N, int S, typename T, int NL, int LPP, int PSTR, int LSTR, int ESTR>
+__device__ __forceinline__ void stack_passB(cx<T> *buf)
+{
+    constexpr int P = Split<N>::P, Q = Split<N>::Q;
+    constexpr bool LF = LSTR < ESTR;
+    if (Q == 1) return;
+    for (int w = threadIdx.x; w < NL * P; w += blockDim.x) {
+        const int l = LF ? w % NL : w / P, k1 = LF ? w / NL : w % P;
+        cx<T> *b = buf + (l / LPP) * PSTR + (l % LPP) * LSTR + Q * k1 * ESTR;
+        cx<T> v[Q];
+#pragma unroll
+        for (int j = 0; j < Q; j++) v[j] = b[j * ESTR];
+        Dft<Q, S, T>::run(v);
+#pragma unroll
+        for (int j = 0; j < Q; j++) b[j * ESTR] = v[j];
+    }
+}
+
+template <int N, int S, typename T, int NL, int LPP, int PSTR, int LSTR, int ESTR>
+__device__ __forceinline__ void stack_fft(cx<T> *buf, const cx<T> *__restrict__ tw)
+{
+    __syncthreads();
+    if (S < 0) {
+        stack_passA<N, S, T, NL, LPP, PSTR, LSTR, ESTR>(buf, tw);
+        if (Split<N>::Q > 1) {
+            __syncthreads();
+            stack_passB<N, S, T, NL, LPP, PSTR, LSTR, ESTR>(buf);
+        }
+    } else {
+        if (Split<N>::Q > 1) {
+            stack_passB<N, S, T, NL, LPP, PSTR, LSTR, ESTR>(buf);
+            __syncthreads();
+        }
+        stack_passA<N, S, T, NL, LPP, PSTR, LSTR, ESTR>(buf, tw);
+    }
+    __syncthreads();
+}
+
+// A stack of PPC x-y planes of an N1 x N2 real grid (N1 even).  Buffer
+// layout: plane p, row y, entry j at buf[p*PS + y*NH + j], NH = N1/2 + 1.
+template <typename T, int N1, int N2, int PPC>
+struct PlaneStack {
+    static constexpr int M = N1 / 2, NH = M + 1, PS = N2 * NH, NP = N1 * N2;
+
+    // packed rows: z[m] = f(2m) + i f(2m+1), natural order
+    template <typename F>
+    __device__ __forceinline__ static void pack(cx<T> *buf, F value)
+    {
+        for (int i = threadIdx.x; i < PPC * N2 * M; i += blockDim.x) {
+            const int p = i / (N2 * M), r = i % (N2 * M), y = r / M, m = r % M;
+            const int e = p * NP + y * N1 + 2 * m;
+            buf[p * PS + y * NH + m] = mk<T>(value(e), value(e + 1));
+        }
+    }
+
+    // natural packed rows -> spectrum [plane][y'][kx].  Each row is
+    // transformed by one thread in registers (length M, natural order) and
+    // untangled there; only the column transform goes through shared memory.
+    __device__ __forceinline__ static void forward(cx<T> *buf, const cx<T> *twM, const cx<T> *twN2, const cx<T> *twN1)
+    {
+        (void)twM;
+        __syncthreads();
+        for (int row = threadIdx.x; row < PPC * N2; row += blockDim.x) {
+            cx<T> *b = buf + row * NH;
+            cx<T> z[M];
+#pragma unroll
+            for (int m = 0; m < M; m++) z[m] = b[m];
+            RegDft<M, -1, T>::run(z);
+            cx<T> x[M + 1];
+#pragma unroll
+            for (int k = 0; k <= M; k++) {
+                const cx<T> zk = z[k % M], zm = conjg(z[(M - k) % M]);
+                const cx<T> w = twc<T>(N1, k);
+                x[k] = scale((zk + zm) + mul_si<-1>(cmul(w, zk - zm)), (T)0.5);
+            }
+#pragma unroll
+            for (int k = 0; k <= M; k++) b[k] = x[k];
+        }
+        stack_fft<N2, -1, T, PPC * NH, NH, PS, 1, NH>(buf, twN2);        // columns (y permuted out)
+    }
+
+    // spectrum [plane][y'][kx] -> natural packed rows of the unnormalised c2r
+    __device__ __forceinline__ static void inverse(cx<T> *buf, const cx<T> *twM, const cx<T> *twN2, const cx<T> *twN1)
+    {
+        (void)twM;
+        stack_fft<N2, 1, T, PPC * NH, NH, PS, 1, NH>(buf, twN2);         // columns (natural y out)
+        for (int row = threadIdx.x; row < PPC * N2; row += blockDim.x) {
+            cx<T> *b = buf + row * NH;
+            cx<T> x[M + 1];
+#pragma unroll
+            for (int k = 0; k <= M; k++) x[k] = b[k];
+            cx<T> z[M];
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                const cx<T> xk = x[k], xm = conjg(x[M - k]);
+                const cx<T> w = conjg(twc<T>(N1, k));
+                z[k] = (xk + xm) + mul_si<1>(cmul(w, xk - xm));
+            }
+            RegDft<M, 1, T>::run(z);
+#pragma unroll
+            for (int m = 0; m < M; m++) b[m] = z[m];
+        }
+        __syncthreads();
+    }
+
+    // real value at plane-stack index e (plane p, x fastest) from packed rows
+    __device__ __forceinline__ static T real_at(const cx<T> *buf, int e)
+    {
+        const int p = e / NP, r = e % NP, y = r / N1, x = r % N1;
+        const cx<T> z = buf[p * PS + y * NH + (x >> 1)];
+        return (x & 1) ? z.y : z.x;
+    }
+
+    __device__ __forceinline__ static void store(cx<T> *dst, const cx<T> *buf)
+    {
+        for (int i = threadIdx.x; i < PPC * PS; i += blockDim.x) dst[i] = buf[i];
+    }
+    __device__ __forceinline__ static void load(cx<T> *buf, const cx<T> *src)
+    {
+        for (int i = threadIdx.x; i < PPC * PS; i += blockDim.x) buf[i] = src[i];
+    }
+};
+
+// K1: S1 = Fxy[eo1 q], S2 = Fxy[eo2 q]   grid = (N3/PPC, nfields)
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(256) k3c_fwd_pair(const SweepField<T> *fields, PlaneGeom g, int t)
+{
+    using PSk = PlaneStack<T, N1, N2, PPC>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3;
+    const int z0 = blockIdx.x * PPC;
+    const T *q = f.slab + (long)src * nr + (long)z0 * PSk::NP;
+    const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP, *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
+    const cx<T> *twM = (const cx<T> *)g.row.tw, *twN2 = (const cx<T> *)g.col.tw, *twN1 = (const cx<T> *)g.rtw;
+    PSk::pack(buf, [&](int e) { return eo1[e] * q[e]; });
+    PSk::forward(buf, twM, twN2, twN1);
+    PSk::store(f.S1 + (long)z0 * PSk::PS, buf);
+    __syncthreads();
+    PSk::pack(buf, [&](int e) { return eo2[e] * q[e]; });
+    PSk::forward(buf, twM, twN2, twN1);
+    PSk::store(f.S2 + (long)z0 * PSk::PS, buf);
+}
+
+// K2/K4: along z on a tile of TC columns: S <- Fz^-1[ek . Fz[S]]
+// which: 1 = S1/ek1, 2 = S2/ek2, 3 = both (grid.z selects)
+template <typename T, int N1, int N2, int N3, int TC>
+__global__ void __launch_bounds__(256) k3c_zconv(const SweepField<T> *fields, PlaneGeom g, int t, int which)
+{
+    constexpr int NH = N1 / 2 + 1, P = N2 * NH;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    const int sel = which == 3 ? (int)blockIdx.z + 1 : which;
+    cx<T> *S = (sel == 1) ? f.S1 : f.S2;
+    const T *ek = (sel == 1) ? f.ek1[blk] : f.ek2[blk];
+    __shared__ __align__(16) cx<T> buf[N3 * TC];
+    const int c0 = blockIdx.x * TC;
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int z = i / TC, c = i % TC;
+        buf[i] = (c0 + c < P) ? S[(long)z * P + c0 + c] : mk<T>((T)0, (T)0);
+    }
+    const cx<T> *twz = (const cx<T> *)g.zp.tw;
+    stack_fft<N3, -1, T, TC, TC, 0, 1, TC>(buf, twz);
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int pz = i / TC, c = i % TC;
+        const int col = c0 + c;
+        if (col < P) {
+            const int py = col / NH, kx = col % NH;
+            const int kz = iperm<N3>(pz), ky = iperm<N2>(py);
+            const T e = ek[kx + NH * (ky + N2 * kz)];
+            buf[i] = mk<T>(e * buf[i].x, e * buf[i].y);
+        }
+    }
+    stack_fft<N3, 1, T, TC, TC, 0, 1, TC>(buf, twz);
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int z = i / TC, c = i % TC;
+        if (c0 + c < P) S[(long)z * P + c0 + c] = buf[i];
+    }
+}
+
+// K3: q1 = eo1 Fxy^-1[S1]/N ; S2 <- Fxy[eo1 Fxy^-1[S2]/N]
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(256) k3c_inv_mid(const SweepField<T> *fields, PlaneGeom g, int t)
+{
+    using PSk = PlaneStack<T, N1, N2, PPC>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const T rn = (T)((long)N1 * N2 * N3);
+    const int z0 = blockIdx.x * PPC;
+    const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP;
+    T *q1 = f.q1 + (long)z0 * PSk::NP;
+    const cx<T> *twM = (const cx<T> *)g.row.tw, *twN2 = (const cx<T> *)g.col.tw, *twN1 = (const cx<T> *)g.rtw;
+    PSk::load(buf, f.S1 + (long)z0 * PSk::PS);
+    PSk::inverse(buf, twM, twN2, twN1);
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) q1[e] = eo1[e] * PSk::real_at(buf, e) / rn;
+    __syncthreads();
+    PSk::load(buf, f.S2 + (long)z0 * PSk::PS);
+    PSk::inverse(buf, twM, twN2, twN1);
+    // h = eo1 y / N, packed in place: entry (p, y, m) <- (h(2m), h(2m+1))
+    for (int i = threadIdx.x; i < PPC * N2 * PSk::M; i += blockDim.x) {
+        const int p = i / (N2 * PSk::M), r = i % (N2 * PSk::M), y = r / PSk::M, m = r % PSk::M;
+        const int e = p * PSk::NP + y * N1 + 2 * m;
+        cx<T> &z = buf[p * PSk::PS + y * PSk::NH + m];
+        z = mk<T>(eo1[e] * z.x / rn, eo1[e + 1] * z.y / rn);
+    }
+    PSk::forward(buf, twM, twN2, twN1);
+    PSk::store(f.S2 + (long)z0 * PSk::PS, buf);
+}
+
+// K5: q_out = (4 eo2 Fxy^-1[S2]/N - q1)/3
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(256) k3c_inv_final(const SweepField<T> *fields, PlaneGeom g, int t)
+{
+    using PSk = PlaneStack<T, N1, N2, PPC>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3;
+    const T rn = (T)nr;
+    const int z0 = blockIdx.x * PPC;
+    const T *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
+    const T *q1 = f.q1 + (long)z0 * PSk::NP;
+    T *out = f.slab + (long)dst * nr + (long)z0 * PSk::NP;
+    const cx<T> *twM = (const cx<T> *)g.row.tw, *twN2 = (const cx<T> *)g.col.tw, *twN1 = (const cx<T> *)g.rtw;
+    PSk::load(buf, f.S2 + (long)z0 * PSk::PS);
+    PSk::inverse(buf, twM, twN2, twN1);
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
+        const T q2 = eo2[e] * PSk::real_at(buf, e) / rn;
+        out[e] = ((T)4 * q2 - q1[e]) / (T)3;
+    }
+}
+
+}  // namespace pscfg
+
+namespace pscfg {
+
+// Stress slice sums with compile-time-shaped transforms (same contract as
+// k3_stress_xy / k3_stress_z / k3_stress_sum in scf_kernels.cuh).
+// Pass 1: xy-forward of PPC planes of slice s (qf or qr) into
+// spec[((s - s0) * 2 + fr)][z][y'][kx].  grid = (N3/PPC, cs, 2).
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(256) k3c_stress_xy(const StressJob<T> *job, PlaneGeom g, int s0, cx<T> *spec)
+{
+    using PSk = PlaneStack<T, N1, N2, PPC>;
+    const StressJob<T> &J = *job;
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3, nk = (long)PSk::PS * N3;
+    const int z0 = blockIdx.x * PPC;
+    const T *q = (blockIdx.z == 0 ? J.qf : J.qr) + (long)s * nr + (long)z0 * PSk::NP;
+    PSk::pack(buf, [&](int e) { return q[e]; });
+    PSk::forward(buf, (const cx<T> *)g.row.tw, (const cx<T> *)g.col.tw, (const cx<T> *)g.rtw);
+    PSk::store(spec + ((long)blockIdx.y * 2 + blockIdx.z) * nk + (long)z0 * PSk::PS, buf);
+}
+
+// Pass 2: z-forward of both spectra on TC columns and the weighted dot
+// products sum_k wdgsq_b(k) Re(F conj R).  grid = (ntiles, cs).
+template <typename T, int N1, int N2, int N3, int TC>
+__global__ void __launch_bounds__(256) k3c_stress_z(const StressJob<T> *job, PlaneGeom g, int s0, const cx<T> *spec,
+                                                    double *part)
+{
+    constexpr int NH = N1 / 2 + 1, P = N2 * NH;
+    const StressJob<T> &J = *job;
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    __shared__ __align__(16) cx<T> F[N3 * TC];
+    __shared__ __align__(16) cx<T> R[N3 * TC];
+    __shared__ double red[32];
+    const long nk = (long)P * N3;
+    const int c0 = blockIdx.x * TC;
+    const cx<T> *sf = spec + ((long)blockIdx.y * 2) * nk, *sr = sf + nk;
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int z = i / TC, c = i % TC;
+        const bool ok = c0 + c < P;
+        F[i] = ok ? sf[(long)z * P + c0 + c] : mk<T>((T)0, (T)0);
+        R[i] = ok ? sr[(long)z * P + c0 + c] : mk<T>((T)0, (T)0);
+    }
+    const cx<T> *twz = (const cx<T> *)g.zp.tw;
+    stack_fft<N3, -1, T, TC, TC, 0, 1, TC>(F, twz);
+    stack_fft<N3, -1, T, TC, TC, 0, 1, TC>(R, twz);
+    for (int b = 0; b < J.ncp; b++) {
+        double acc = 0.0;
+        for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+            const int pz = i / TC, c = i % TC, col = c0 + c;
+            if (col < P) {
+                const int py = col / NH, kx = col % NH;
+                const long k = kx + NH * (iperm<N2>(py) + (long)N2 * iperm<N3>(pz));
+                const cx<T> f = F[i], r = R[i];
+                acc += J.wdgsq[(long)b * nk + k] * ((double)f.x * (double)r.x + (double)f.y * (double)r.y);
+            }
+        }
+        const double tot = block_sum(acc, red);
+        if (threadIdx.x == 0) part[((long)blockIdx.y * gridDim.x + blockIdx.x) * PSCFG_MAXCP + b] = tot;
+        __syncthreads();
+    }
+}
+
+}  // namespace pscfg
