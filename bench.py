@@ -305,6 +305,33 @@ def run_ours(args, rank, world, local_rank):
     else:
         solve_s_all, conv_all = solve_s, float(conv)
 
+    # ---- mixed precision solve of the same batch (FP32 then FP64) ---------
+    from pscf_b200.engine import MIXED
+    em = Engine(systems, MIXED)
+    for i in range(B):
+        em.set_symmetry(i, "I m -3 m")
+    streamm = torch.cuda.ExternalStream(em.stream, device=dev)
+    barrier()
+    ev6, ev7 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev6.record(streamm)
+    em.am_begin(omega0, error_max=ERROR_MAX, max_itr=2000, n_hist=N_HIST, domain=True)
+    while em.am_iterate(8) > 0:
+        pass
+    ev7.record(streamm)
+    barrier()
+    mixed_s = ev6.elapsed_time(ev7) / 1e3
+    _, _, resm = em.am_results(want_fields=False)
+    convm = sum(1 for r in resm if r["converged"])
+    dF = max(abs(a["f_helmholtz"] - b["f_helmholtz"]) for a, b in zip(res, resm))
+    itr32 = float(np.mean([r["itr_fp32"] for r in resm]))
+    tm = torch.tensor([mixed_s, float(convm), dF], dtype=torch.float64, device=dev)
+    if world > 1:
+        for k, op in ((0, dist.ReduceOp.MAX), (1, dist.ReduceOp.SUM), (2, dist.ReduceOp.MAX)):
+            x = tm[k:k + 1].clone()
+            dist.all_reduce(x, op=op)
+            tm[k] = x[0]
+    em.close()
+
     # ---- end to end through the C ABI with host buffers ------------------
     w_pin = torch.from_numpy(omega0.copy()).pin_memory()
     rho_pin = torch.empty_like(w_pin).pin_memory()
@@ -356,6 +383,10 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2 (propagator slabs %.1f GB per GPU)" % (B * 2 * 103 * s0.nr * 8 / 1e9)},
         "solves_per_s": conv_all / solve_s_all, "solve_seconds": solve_s_all, "solves_converged": int(conv_all),
         "solve_iterations": {"min": int(min(itrs)), "max": int(max(itrs)), "mean": float(np.mean(itrs))},
+        "mixed_precision": {"solves_per_s": float(tm[1].item()) / float(tm[0].item()),
+                            "speedup_vs_fp64": (float(tm[1].item()) / float(tm[0].item())) / (conv_all / solve_s_all),
+                            "max_abs_dF_vs_fp64": float(tm[2].item()), "mean_fp32_iterations": itr32,
+                            "solves_converged": int(tm[1].item())},
         "f_helmholtz": {"min": float(min(fvals)), "max": float(max(fvals))},
         "cell_param": {"min": float(min(cells)), "max": float(max(cells))},
         "e2e": {"value": e2e_value, "unit": "MDE steps/s", "api": "pscfg_density + pscfg_stress (host buffers)",

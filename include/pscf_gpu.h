@@ -46,6 +46,9 @@ extern "C" {
 /* precision of the propagator */
 #define PSCFG_FP64 0
 #define PSCFG_FP32 1       /* FP32 propagation + FFT, FP64 contour sums */
+#define PSCFG_MIXED 2      /* Anderson runs start in FP32 and switch each instance
+                              to FP64 once its error is below the switch error or
+                              stops improving; other calls run in FP64 */
 
 /* crystal systems (src/unit_cell_mod.f90:309-664) */
 #define PSCFG_LAMELLAR 0
@@ -94,11 +97,13 @@ typedef struct pscfg_am_param {
     int n_hist;
     int domain;              /* 1: relax the unit cell (stress -> 0) */
     double error_max;
+    double switch_error;     /* PSCFG_MIXED: FP32 -> FP64 below this error (0: 1e-5) */
 } pscfg_am_param;
 
 /* Per-instance result of pscfg_iterate_am. */
 typedef struct pscfg_am_result {
     int itr;
+    int itr_fp32;            /* PSCFG_MIXED: iterations run with FP32 propagation */
     int converged;           /* 1 converged, 0 not (max_itr or diverged) */
     double error;            /* max(|dev|, |stress|) at exit */
     double f_helmholtz;      /* free energy per monomer / kT */

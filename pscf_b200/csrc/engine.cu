@@ -70,6 +70,7 @@ struct Inst {
     double *stress_dev = nullptr; // [MAXCP]
     double Q[PSCFG_MAXC] = {}, Qs[PSCFG_MAXS] = {};
     bool have_density = false;
+    int prec_now = PSCFG_FP64;    // propagation precision of the next density call
     // Anderson
     double *om_hist = nullptr, *dev_hist = nullptr;
     // space group imposed on omega (0 ops: none)
@@ -139,8 +140,9 @@ struct Engine {
         return p;
     }
 
-    size_t tsize() const { return prec == PSCFG_FP64 ? sizeof(double) : sizeof(float); }
-    const PlaneGeom &geom() const { return prec == PSCFG_FP64 ? g64 : g32; }
+    int cur = PSCFG_FP64;          // precision of the kernels being launched
+    size_t tsize() const { return prec == PSCFG_FP32 ? sizeof(float) : sizeof(double); }
+    const PlaneGeom &geom() const { return cur == PSCFG_FP32 ? g32 : g64; }
 
     void *desc(size_t bytes)
     {
@@ -326,7 +328,8 @@ struct PhaseTimer {
 static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int precision)
 {
     if (n_inst < 1) throw Err(PSCFG_EINVAL, "n_inst must be >= 1");
-    if (precision != PSCFG_FP64 && precision != PSCFG_FP32) throw Err(PSCFG_EINVAL, "unknown precision");
+    if (precision != PSCFG_FP64 && precision != PSCFG_FP32 && precision != PSCFG_MIXED)
+        throw Err(PSCFG_EINVAL, "unknown precision");
     E.prec = precision;
     E.dim = sys[0].dim;
     if (E.dim < 1 || E.dim > 3) throw Err(PSCFG_EINVAL, "dim must be 1, 2 or 3");
@@ -345,7 +348,7 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
     make_geom<double>(E, E.g64);
-    if (precision == PSCFG_FP32) make_geom<float>(E, E.g32);
+    if (precision != PSCFG_FP64) make_geom<float>(E, E.g32);
 
     const size_t ts = E.tsize();
     E.inst.resize(n_inst);
@@ -356,6 +359,7 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         if (s.n_monomer != E.M) throw Err(PSCFG_EINVAL, "all instances must have the same n_monomer");
         Inst &I = E.inst[i];
         I.sys = s;
+        I.prec_now = (precision == PSCFG_FP32) ? PSCFG_FP32 : PSCFG_FP64;
         I.omega = (double *)E.dalloc(sizeof(double) * E.M * E.nr);
         I.rho = (double *)E.dalloc(sizeof(double) * E.M * E.nr);
         I.ksq = (double *)E.dalloc(sizeof(double) * E.nk);
@@ -566,11 +570,14 @@ static void run_contour(Engine &E, const std::vector<int> &act)
         k_final_sum_ptr<<<(unsigned)((qp.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, dq, (int)qp.size());
         E.launched();
     }
-    // solvents (src/scf_mod.fp.f90:193-200, 251-295)
-    bool any_solvent = false;
+    // solvents (src/scf_mod.fp.f90:193-200, 251-295): Q_s = <exp(-v w)>,
+    // rho_alpha = phi_s exp(-v w)/Q_s added before the chain densities
+    bool any_solvent = false, any_grand = false;
     std::vector<SolventJob> sj;
+    std::vector<double *> qsout;
     for (int i : act) {
         Inst &I = E.inst[i];
+        if (I.sys.ensemble == 1) any_grand = true;
         for (int s = 0; s < I.sys.n_solvent; s++) {
             SolventJob j;
             int m = I.sys.solvent_monomer[s];
@@ -582,7 +589,47 @@ static void run_contour(Engine &E, const std::vector<int> &act)
             j.mu = I.sys.mu_solvent[s];
             j.grand = I.sys.ensemble == 1;
             sj.push_back(j);
+            qsout.push_back(I.Qsolv + s);
             any_solvent = true;
+        }
+    }
+    std::vector<int> with_solvent;
+    if (any_solvent) {
+        for (int i : act) {
+            Inst &I = E.inst[i];
+            if (I.sys.n_solvent > 0) {
+                k_zero<<<(unsigned)std::min<long>((E.M * E.nr + 255) / 256, 1024), 256, 0, E.st>>>(I.rho, (long)E.M * E.nr);
+                E.launched();
+                with_solvent.push_back(i);
+            }
+        }
+        SolventJob *dsj0 = E.upload(sj, off);
+        off += ((sj.size() * sizeof(SolventJob) + 255) / 256) * 256;
+        double **dqs = (double **)E.upload(qsout, off);
+        off += ((qsout.size() * sizeof(void *) + 255) / 256) * 256;
+        double *part = E.part((size_t)nct * sj.size());
+        k_solvent_boltz_partial<<<dim3(nct, (unsigned)sj.size()), 256, 0, E.st>>>(dsj0, E.nr, part);
+        E.launched();
+        k_final_sum_ptr<<<(unsigned)((sj.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, dqs, (int)sj.size());
+        E.launched();
+        k_solvent_rho<<<(unsigned)std::min<long>((E.nr + 255) / 256, 1024), 256, 0, E.st>>>(dsj0, (int)sj.size(), E.nr);
+        E.launched();
+    }
+    // grand ensemble: phi = Q exp(mu) (mu_phi_chain/mu_phi_solvent,
+    // src/scf_mod.fp.f90:202-209) is needed by the chain weights below
+    if (any_grand) {
+        for (int i : act) {
+            Inst &I = E.inst[i];
+            if (I.sys.ensemble != 1) continue;
+            CK(cudaMemcpyAsync(I.Q, I.Qdev, sizeof(double) * PSCFG_MAXC, cudaMemcpyDeviceToHost, E.st));
+            CK(cudaMemcpyAsync(I.Qs, I.Qsolv, sizeof(double) * PSCFG_MAXS, cudaMemcpyDeviceToHost, E.st));
+        }
+        CK(cudaStreamSynchronize(E.st));
+        for (int i : act) {
+            Inst &I = E.inst[i];
+            if (I.sys.ensemble != 1) continue;
+            for (int c = 0; c < I.sys.n_chain; c++) I.sys.phi_chain[c] = I.Q[c] * std::exp(I.sys.mu_chain[c]);
+            for (int s = 0; s < I.sys.n_solvent; s++) I.sys.phi_solvent[s] = I.Qs[s] * std::exp(I.sys.mu_solvent[s]);
         }
     }
     // Simpson jobs grouped by instance
@@ -607,18 +654,13 @@ static void run_contour(Engine &E, const std::vector<int> &act)
                 j.bds[b] = I.bds[c][b];
             }
             j.n_monomer = I.sys.n_monomer;
+            j.accumulate = I.sys.n_solvent > 0 ? 1 : 0;
             simp.push_back(j);
         }
+        if (I.sys.n_chain == 0 && I.sys.n_solvent == 0)
+            throw Err(PSCFG_EINVAL, "an instance needs at least one chain or solvent species");
     }
     start.push_back((int)simp.size());
-    if (any_solvent) {
-        // grand-ensemble chain phi = Q exp(mu) needs the device Q: pull Q now
-        throw Err(PSCFG_EINVAL, "solvent species are not supported by this build of the engine");
-    }
-    for (int i : act) {
-        Inst &I = E.inst[i];
-        if (I.sys.ensemble != 0) throw Err(PSCFG_EINVAL, "only the canonical ensemble is supported by this build");
-    }
     SimpsonJob *dsj = E.upload(simp, off);
     off += ((simp.size() * sizeof(SimpsonJob) + 255) / 256) * 256;
     int *dst = E.upload(start, off);
@@ -644,21 +686,42 @@ static void density_impl(Engine &E, const std::vector<int> &act)
     run_contour<T>(E, act);
 }
 
+static void split_prec(Engine &E, const std::vector<int> &act, std::vector<int> &a64, std::vector<int> &a32)
+{
+    for (int i : act) (E.inst[i].prec_now == PSCFG_FP32 ? a32 : a64).push_back(i);
+}
+
 static void density_all(Engine &E, const std::vector<int> &act)
 {
-    if (E.prec == PSCFG_FP64) density_impl<double>(E, act);
-    else density_impl<float>(E, act);
+    std::vector<int> a64, a32;
+    split_prec(E, act, a64, a32);
+    if (!a64.empty()) {
+        E.cur = PSCFG_FP64;
+        density_impl<double>(E, a64);
+    }
+    if (!a32.empty()) {
+        E.cur = PSCFG_FP32;
+        density_impl<float>(E, a32);
+    }
     // pull Q to the host (needed for mu and for the caller)
     for (int i : act) {
         Inst &I = E.inst[i];
         CK(cudaMemcpyAsync(I.Q, I.Qdev, sizeof(double) * PSCFG_MAXC, cudaMemcpyDeviceToHost, E.st));
+        CK(cudaMemcpyAsync(I.Qs, I.Qsolv, sizeof(double) * PSCFG_MAXS, cudaMemcpyDeviceToHost, E.st));
     }
     CK(cudaStreamSynchronize(E.st));
     for (int i : act) {
         Inst &I = E.inst[i];
         I.have_density = true;
-        // mu_phi_chain (src/scf_mod.fp.f90:768-785), canonical ensemble
-        for (int c = 0; c < I.sys.n_chain; c++) I.sys.mu_chain[c] = std::log(I.sys.phi_chain[c] / I.Q[c]);
+        // mu_phi_chain / mu_phi_solvent (src/scf_mod.fp.f90:768-820)
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            if (I.sys.ensemble == 0) I.sys.mu_chain[c] = std::log(I.sys.phi_chain[c] / I.Q[c]);
+            else I.sys.phi_chain[c] = I.Q[c] * std::exp(I.sys.mu_chain[c]);
+        }
+        for (int s = 0; s < I.sys.n_solvent; s++) {
+            if (I.sys.ensemble == 0) I.sys.mu_solvent[s] = std::log(I.sys.phi_solvent[s] / I.Qs[s]);
+            else I.sys.phi_solvent[s] = I.Qs[s] * std::exp(I.sys.mu_solvent[s]);
+        }
     }
 }
 
@@ -800,8 +863,16 @@ static void stress_all(Engine &E, const std::vector<int> &act)
     for (int i : act)
         if (!E.inst[i].have_density) throw Err(PSCFG_ESTATE, "stress requires a preceding density call");
     PhaseTimer pt(E, &E.t_stress);
-    if (E.prec == PSCFG_FP64) stress_impl<double>(E, act);
-    else stress_impl<float>(E, act);
+    std::vector<int> a64, a32;
+    split_prec(E, act, a64, a32);
+    if (!a64.empty()) {
+        E.cur = PSCFG_FP64;
+        stress_impl<double>(E, a64);
+    }
+    if (!a32.empty()) {
+        E.cur = PSCFG_FP32;
+        stress_impl<float>(E, a32);
+    }
 }
 
 // ---------------------------------------------------------------------
@@ -948,6 +1019,9 @@ static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<
 // ---------------------------------------------------------------------
 struct AmState {
     int itr = 0;
+    int itr_fp32 = 0;          // iterations run with FP32 propagation
+    double best = INFINITY;    // best FP32 error so far (stall detection)
+    int since_best = 0;
     bool done = false;
     bool converged = false;
     double error = 0;
@@ -1034,6 +1108,7 @@ static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
     }
     R.prm = prm;
     R.st.assign(ninst, AmState());
+    for (auto &I : E.inst) I.prec_now = (E.prec == PSCFG_FP64) ? PSCFG_FP64 : PSCFG_FP32;
     std::vector<int> all(ninst);
     std::vector<double *> scratch(ninst);
     for (int i = 0; i < ninst; i++) {
@@ -1054,7 +1129,7 @@ static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
             for (int b = 0; b < I.sys.n_block[c]; b++)
                 phi_mon[I.sys.block_monomer[c][b]] += I.sys.phi_chain[c] * I.sys.block_length[c][b] / I.length[c];
         for (int sv = 0; sv < I.sys.n_solvent; sv++) phi_mon[I.sys.solvent_monomer[sv]] += I.sys.phi_solvent[sv];
-        for (int a = 0; a < E.M; a++) {
+        for (int a = 0; a < E.M && I.sys.ensemble == 0; a++) {
             double w0 = 0;
             for (int b = 0; b < E.M; b++) w0 = w0 + I.sys.chi[a][b] * phi_mon[b];
             double m = 0;
@@ -1198,7 +1273,23 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
             for (int b = 0; b < ncp; b++) e2 = std::max(e2, std::fabs(s.stress[b]));
             s.error = std::max(e1, e2);
             s.nstore = nst;
-            if (s.error < prm.error_max) { s.converged = true; s.done = true; continue; }
+            // mixed precision: an FP32 iteration never counts as converged; the
+            // instance moves to FP64 once its error is below the switch error
+            // or has not improved by 10% for 10 iterations
+            const bool was32 = I.prec_now == PSCFG_FP32;
+            if (was32) {
+                s.itr_fp32++;
+                const double sw = prm.switch_error > 0 ? prm.switch_error : 1e-5;
+                bool go = s.error < sw || s.error < prm.error_max;
+                if (s.error < 0.9 * s.best) {
+                    s.best = s.error;
+                    s.since_best = 0;
+                } else if (++s.since_best >= 10) {
+                    go = true;
+                }
+                if (go && E.prec == PSCFG_MIXED) I.prec_now = PSCFG_FP64;
+            }
+            if (!(was32 && E.prec == PSCFG_MIXED) && s.error < prm.error_max) { s.converged = true; s.done = true; continue; }
             if (s.itr > prm.max_itr || !(s.error <= 100.0 * large)) { s.done = true; continue; }
 
             // lambda and history depth (src/iterate_mod.fp.f90:1147-1153)
@@ -1305,6 +1396,7 @@ static void am_results(Engine &E, AmRun &R, std::vector<pscfg_am_result> &res)
         AmState &s = R.st[i];
         Inst &I = E.inst[i];
         r.itr = s.itr;
+        r.itr_fp32 = s.itr_fp32;
         r.converged = s.converged ? 1 : 0;
         r.error = s.error;
         r.f_helmholtz = s.f;
@@ -1525,7 +1617,8 @@ static int density_common(pscfg_engine *e, const double *omega, double *rho, dou
         if (q)
             for (int c = 0; c < PSCFG_MAXC; c++) q[(long)i * PSCFG_MAXC + c] = (c < E.inst[i].sys.n_chain) ? E.inst[i].Q[c] : 0.0;
         if (qs)
-            for (int s = 0; s < PSCFG_MAXS; s++) qs[(long)i * PSCFG_MAXS + s] = E.inst[i].Qs[s];
+            for (int s = 0; s < PSCFG_MAXS; s++)
+                qs[(long)i * PSCFG_MAXS + s] = (s < E.inst[i].sys.n_solvent) ? E.inst[i].Qs[s] : 0.0;
     }
     ABI_END(e)
 }
@@ -1745,8 +1838,13 @@ int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, 
     if (!e || !omega_m || !q_in || !q_out || nsteps < 1) return PSCFG_EINVAL;
     ABI_BEGIN
     if (inst < 0 || inst >= (int)e->E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
-    if (e->E.prec == PSCFG_FP64) propagate_impl<double>(e->E, inst, omega_m, b, ds, q_in, q_out, nsteps);
-    else propagate_impl<float>(e->E, inst, omega_m, b, ds, q_in, q_out, nsteps);
+    if (e->E.prec == PSCFG_FP32) {
+        e->E.cur = PSCFG_FP32;
+        propagate_impl<float>(e->E, inst, omega_m, b, ds, q_in, q_out, nsteps);
+    } else {
+        e->E.cur = PSCFG_FP64;
+        propagate_impl<double>(e->E, inst, omega_m, b, ds, q_in, q_out, nsteps);
+    }
     ABI_END(e)
 }
 
@@ -1764,7 +1862,7 @@ int pscfg_get_propagators(pscfg_engine *e, int inst, int chain, double *qf, doub
         double *dst = d == 0 ? qf : qr;
         if (!dst) continue;
         const void *src = d == 0 ? I.qf[chain] : I.qr[chain];
-        if (E.prec == PSCFG_FP64) {
+        if (I.prec_now != PSCFG_FP32) {
             CK(cudaMemcpyAsync(dst, src, sizeof(double) * E.nr * ns, cudaMemcpyDeviceToHost, E.st));
             CK(cudaStreamSynchronize(E.st));
         } else {

@@ -350,7 +350,7 @@ struct SimpsonJob {
     int bgn[PSCFG_MAXB + 1];
     int mon[PSCFG_MAXB];
     double bds[PSCFG_MAXB];
-    int first;                  // 1: this job also zeroes rho (first chain of the instance)
+    int accumulate;             // 1: add to the existing rho (solvent terms already there)
     int n_monomer;
 };
 
@@ -363,6 +363,8 @@ __global__ void k_simpson(const SimpsonJob *jobs, const int *job_start, long nr)
     const int j0 = job_start[inst], j1 = job_start[inst + 1];
     for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += (long)gridDim.x * blockDim.x) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        if (j1 > j0 && jobs[j0].accumulate)
+            for (int a = 0; a < jobs[j0].n_monomer; a++) acc[a] = jobs[j0].rho[(long)a * nr + r];
         for (int jb = j0; jb < j1; jb++) {
             const SimpsonJob &J = jobs[jb];
             const T *qf = (const T *)J.qf, *qr = (const T *)J.qr;
@@ -380,8 +382,10 @@ __global__ void k_simpson(const SimpsonJob *jobs, const int *job_start, long nr)
                 acc[J.mon[b]] = acc[J.mon[b]] + J.phi * s;
             }
         }
-        const SimpsonJob &J0 = jobs[j0];
-        for (int a = 0; a < J0.n_monomer; a++) J0.rho[(long)a * nr + r] = acc[a];
+        if (j1 > j0) {
+            const SimpsonJob &J0 = jobs[j0];
+            for (int a = 0; a < J0.n_monomer; a++) J0.rho[(long)a * nr + r] = acc[a];
+        }
     }
 }
 

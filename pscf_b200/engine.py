@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libpscfgpu.so")
 
 FP64 = 0
 FP32 = 1
+MIXED = 2
 
 OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENOTCONV = 0, 1, 2, 3, 4, 5
 
@@ -59,12 +60,14 @@ class PscfgAmParam(C.Structure):
         ("n_hist", C.c_int),
         ("domain", C.c_int),
         ("error_max", C.c_double),
+        ("switch_error", C.c_double),
     ]
 
 
 class PscfgAmResult(C.Structure):
     _fields_ = [
         ("itr", C.c_int),
+        ("itr_fp32", C.c_int),
         ("converged", C.c_int),
         ("error", C.c_double),
         ("f_helmholtz", C.c_double),
@@ -219,7 +222,9 @@ class Engine:
         w = np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
         rho = np.zeros_like(w)
         q = np.zeros((self.n_inst, MAX_CHAIN))
-        self._check(self.lib.pscfg_density(self._h, _ptr(w), _ptr(rho), _ptr(q), None))
+        qs = np.zeros((self.n_inst, MAX_SOLVENT))
+        self._check(self.lib.pscfg_density(self._h, _ptr(w), _ptr(rho), _ptr(q), _ptr(qs)))
+        self.q_solvent = qs
         return rho, q
 
     def density_device(self, omega_dev_ptr: int, rho_dev_ptr: int):
@@ -253,11 +258,12 @@ class Engine:
         self._check(self.lib.pscfg_get_propagators(self._h, inst, chain, _ptr(qf), _ptr(qr), None))
         return qf, qr
 
-    def iterate_am(self, omega: np.ndarray, error_max=1e-10, max_itr=1000, n_hist=20, domain=False):
+    def iterate_am(self, omega: np.ndarray, error_max=1e-10, max_itr=1000, n_hist=20, domain=False,
+                   switch_error=0.0):
         """Anderson-mixing solve of every instance; returns (omega, rho, results)."""
         w = np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr).copy()
         rho = np.zeros_like(w)
-        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max)
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error)
         res = (PscfgAmResult * self.n_inst)()
         self._check(self.lib.pscfg_iterate_am(self._h, _ptr(w), C.byref(prm), _ptr(rho), res), allow=(ENOTCONV,))
         return w, rho, self._results(res, domain)
@@ -280,7 +286,7 @@ class Engine:
         for i, r in enumerate(res):
             ncp = len(self.systems[i].cell_param)
             nch = len(self.systems[i].chains)
-            out.append(dict(itr=r.itr, converged=bool(r.converged), error=r.error,
+            out.append(dict(itr=r.itr, itr_fp32=r.itr_fp32, converged=bool(r.converged), error=r.error,
                             f_helmholtz=r.f_helmholtz, pressure=r.pressure,
                             stress=list(r.stress)[:ncp], cell_param=list(r.cell_param)[:ncp],
                             q=list(r.q)[:nch], mu_chain=list(r.mu_chain)[:nch]))
@@ -288,10 +294,10 @@ class Engine:
                 self.systems[i].cell_param = list(r.cell_param)[:ncp]
         return out
 
-    def am_begin(self, omega, error_max=1e-10, max_itr=1000, n_hist=20, domain=False):
+    def am_begin(self, omega, error_max=1e-10, max_itr=1000, n_hist=20, domain=False, switch_error=0.0):
         w = None if omega is None else np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
         self._am_domain = domain
-        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max)
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error)
         self._check(self.lib.pscfg_am_begin(self._h, None if w is None else _ptr(w), C.byref(prm)))
 
     def am_iterate(self, iters: int = 1) -> int:

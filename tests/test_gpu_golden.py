@@ -106,3 +106,23 @@ def test_symmetry_projection_keeps_symmetric_solution():
     assert r[0]["converged"]
     for a in range(2):
         np.testing.assert_allclose(G.symmetrize(w[0, a], "I m -3 m", [16, 16, 16]), w[0, a], atol=1e-12)
+
+
+def test_mixed_precision_matches_fp64_solution():
+    """FP32 propagation until the residual nears 1e-5, then FP64 to 1e-11:
+    the converged free energy equals the FP64 solve to 1e-10 per monomer."""
+    from pscf_b200.engine import MIXED
+    ss = _bcc_systems()[:4]
+    w0 = np.stack([sphere_guess(s, s.chains[0].block_length[0], width=0.05) for s in ss])
+    res = {}
+    for prec in (FP64, MIXED):
+        e = Engine(ss, prec)
+        for i in range(len(ss)):
+            e.set_symmetry(i, "I m -3 m")
+        w, rho, r = e.iterate_am(w0, error_max=1e-11, max_itr=800)
+        assert all(x["converged"] for x in r)
+        res[prec] = r
+    for a, b, g in zip(res[FP64], res[MIXED], GOLD["bcc_sweep"]):
+        assert b["itr_fp32"] > 0
+        assert abs(a["f_helmholtz"] - b["f_helmholtz"]) < 1e-10
+        assert abs(b["f_helmholtz"] - g["f_Helmholtz"][0]) < 2e-10

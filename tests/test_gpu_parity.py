@@ -129,3 +129,32 @@ def test_fixed_shape_kernels_match_generic(n, monkeypatch):
         e3 = Engine([s], prec)
         c = e3.propagate(0, w, 1.0, 0.01, q0, 3)
         assert rel_err(c, a) < tol
+
+
+def _blend(ensemble):
+    """AB diblock + A homopolymer + B-selective solvent (three species)."""
+    from pscf_b200.system import Chain, Solvent, System
+    chains = [Chain([0, 1], [0.4, 0.6], phi=0.7, mu=2.0), Chain([0], [0.5], phi=0.2, mu=1.5)]
+    solvents = [Solvent(monomer=1, size=0.1, phi=0.1, mu=0.3)]
+    return System(dim=2, ngrid=[16, 16], crystal_system="hexagonal", cell_param=[1.7], kuhn=[1.0, 1.2],
+                  chi=[[0, 14.0], [14.0, 0]], chains=chains, solvents=solvents, ds=0.02, ensemble=ensemble)
+
+
+@pytest.mark.parametrize("ensemble", [0, 1])
+def test_solvent_and_ensemble_parity(ensemble):
+    s = _blend(ensemble)
+    w = omega_guess(s, 31, 1.5)
+    o = O.Oracle(s)
+    rho_ref, q_ref = o.density(w)
+    st_ref = o.stress()
+    f_ref, p_ref = o.free_energy(w, rho_ref)
+    mu_ref, phi_ref = o.mu_phi()
+    e = Engine([s], FP64)
+    rho, q = e.density(w[None])
+    assert rel_err(rho[0], rho_ref) < 1e-12
+    assert rel_err(q[0, :2], q_ref) < 1e-12
+    st = e.scf_stress()[0, :1]
+    np.testing.assert_allclose(st, st_ref, rtol=1e-10, atol=1e-12)
+    f, p, mu = e.free_energy()
+    assert abs(f[0] - f_ref) < 1e-11 and abs(p[0] - p_ref) < 1e-11
+    np.testing.assert_allclose(mu[0, :2], mu_ref, rtol=1e-12)
