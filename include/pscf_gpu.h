@@ -163,6 +163,20 @@ int pscfg_free_energy(pscfg_engine *e, double *out, double *mu_chain);
 int pscfg_iterate_am(pscfg_engine *e, double *omega, const pscfg_am_param *prm, double *rho,
                      pscfg_am_result *results);
 
+/* Reverse-mode derivative of the last density call (no counterpart
+ * routine in the reference; it differentiates the reference's discrete
+ * algorithm: step_exp src/step_mod.f90:146-176, Simpson sums
+ * src/scf_mod.fp.f90:364-426, bigQ :359).  Given upstream gradients
+ * grad_rho [n_inst][n_monomer][nr] = dL/drho and, optionally,
+ * grad_lnq [n_inst][PSCFG_MAXC] = dL/dlnQ, writes
+ * grad_omega [n_inst][n_monomer][nr] = dL/domega (per grid point).  Two
+ * adjoint sweeps per chain run through the same step kernels.  FP64
+ * propagators only.  Host arrays; the _device form takes device arrays
+ * (grad_lnq stays on the host). */
+int pscfg_density_adjoint(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega);
+int pscfg_density_adjoint_device(pscfg_engine *e, const double *grad_rho_dev, const double *grad_lnq,
+                                 double *grad_omega_dev);
+
 /* Stepwise form of pscfg_iterate_am for callers that interleave their own
  * work or time single iterations: pscfg_am_begin loads omega (host, or
  * NULL to keep the engine's fields) and runs the initial density;

@@ -28,6 +28,7 @@
 #include "host_geom.h"
 #include "scf_kernels.cuh"
 #include "kernels3c.cuh"
+#include "adjoint.cuh"
 
 namespace pscfg {
 
@@ -73,6 +74,12 @@ struct Inst {
     int prec_now = PSCFG_FP64;    // propagation precision of the next density call
     // Anderson
     double *om_hist = nullptr, *dev_hist = nullptr;
+    // adjoint scratch per (chain, direction): lambda ping-pong, step
+    // intermediates of lambda and of the stored slice, spectra, gradient
+    void *adj_real[PSCFG_MAXC][2] = {};   // 10 fields of nr T
+    void *adj_spec[PSCFG_MAXC][2] = {};   // 4 spectra of nk cx<T>
+    double *adj_grad[PSCFG_MAXC][2] = {}; // [M][nr]
+    double *adj_coef[PSCFG_MAXC] = {};    // [ns+1][MAXM] device
     // space group imposed on omega (0 ops: none)
     int nops = 0;
     int *d_ops = nullptr;
@@ -1413,6 +1420,270 @@ static void am_results(Engine &E, AmRun &R, std::vector<pscfg_am_result> &res)
 }
 
 // ---------------------------------------------------------------------
+// Adjoint of density() with respect to omega (adjoint.cuh)
+// ---------------------------------------------------------------------
+// Simpson weights of slice j summed over the blocks that contain it, per
+// monomer: wsum_j[m] = sum_{b ∋ j, m_b = m} (ds_b / 3) w_j^b.
+static void simpson_weights(const Inst &I, int c, std::vector<double> &w)
+{
+    const int ns = I.ns[c];
+    w.assign((size_t)(ns + 1) * PSCFG_MAXM, 0.0);
+    for (int b = 0; b < I.sys.n_block[c]; b++) {
+        const int ib = I.bgn[c][b], ie = I.bgn[c][b + 1], m = I.sys.block_monomer[c][b];
+        for (int j = ib; j <= ie; j++) {
+            double wt = (j == ib || j == ie) ? 1.0 : (((j - ib) % 2 == 1) ? 4.0 : 2.0);
+            w[(size_t)j * PSCFG_MAXM + m] += I.bds[c][b] / 3.0 * wt;
+        }
+    }
+}
+
+static int seg_block(const Inst &I, int c, int j)   // block of the segment (j, j+1)
+{
+    int b = 0;
+    while (b < I.sys.n_block[c] - 1 && j >= I.bgn[c][b + 1]) b++;
+    return b;
+}
+
+template <typename T>
+static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vector<const double *> &G,
+                         const std::vector<const double *> &gQ, const std::vector<double *> &grad)
+{
+    const size_t ts = sizeof(T);
+    const long nr = E.nr, nk = E.nk;
+    struct Sweep {
+        int inst, c, d, ns;
+        T *lam[2];
+        T *p1[2], *h[2], *p2[2], *dummy[2];
+        cx<T> *S1[2], *S2[2];
+        double *gbuf;
+        std::vector<double> coef;   // [ns+1][MAXM] incl. phi/(L Q)
+    };
+    std::vector<Sweep> sw;
+    const int nct = red_ctas(nr);
+    // coefficients, overlaps S_c
+    std::vector<AdjOverlap> ov;
+    std::vector<std::pair<int, int>> ov_ic;
+    size_t off = 0;
+    for (size_t k = 0; k < act.size(); k++) {
+        Inst &I = E.inst[act[k]];
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            std::vector<double> w;
+            simpson_weights(I, c, w);
+            const double cphi = (I.sys.ensemble == 0) ? I.sys.phi_chain[c] / (I.length[c] * I.Q[c])
+                                                      : std::exp(I.sys.mu_chain[c]) / I.length[c];
+            for (auto &x : w) x *= cphi;
+            if (!I.adj_coef[c]) I.adj_coef[c] = (double *)E.dalloc(sizeof(double) * w.size());
+            CK(cudaMemcpyAsync(I.adj_coef[c], w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice, E.st));
+            for (int d = 0; d < 2; d++) {
+                if (!I.adj_real[c][d]) {
+                    I.adj_real[c][d] = E.dalloc(ts * nr * 10);
+                    I.adj_spec[c][d] = E.dalloc(2 * ts * nk * 4);
+                    I.adj_grad[c][d] = (double *)E.dalloc(sizeof(double) * E.M * nr);
+                }
+                Sweep S;
+                S.inst = act[k];
+                S.c = c;
+                S.d = d;
+                S.ns = I.ns[c];
+                T *R = (T *)I.adj_real[c][d];
+                cx<T> *SP = (cx<T> *)I.adj_spec[c][d];
+                S.lam[0] = R;
+                S.lam[1] = R + nr;
+                for (int f = 0; f < 2; f++) {
+                    S.p1[f] = R + (2 + 4 * f) * nr;
+                    S.h[f] = R + (3 + 4 * f) * nr;
+                    S.p2[f] = R + (4 + 4 * f) * nr;
+                    S.dummy[f] = R + (5 + 4 * f) * nr;
+                    S.S1[f] = SP + (2 * f) * nk;
+                    S.S2[f] = SP + (2 * f + 1) * nk;
+                }
+                S.gbuf = I.adj_grad[c][d];
+                S.coef = w;
+                k_zero<<<(unsigned)std::min<long>((E.M * nr + 255) / 256, 1024), 256, 0, E.st>>>(S.gbuf, (long)E.M * nr);
+                E.launched();
+                sw.push_back(S);
+            }
+            AdjOverlap o;
+            o.qf = I.qf[c];
+            o.qr = I.qr[c];
+            o.G = G[k];
+            o.coef = I.adj_coef[c];
+            o.nslices = I.ns[c] + 1;
+            o.M = E.M;
+            ov.push_back(o);
+            ov_ic.push_back({(int)k, c});
+        }
+    }
+    if (sw.empty()) return;
+    std::vector<double> Sc(ov.size());
+    {
+        AdjOverlap *dov = E.upload(ov, off);
+        off += ((ov.size() * sizeof(AdjOverlap) + 255) / 256) * 256;
+        double *part = E.part((size_t)nct * ov.size());
+        k_adj_overlap<T><<<dim3(nct, (unsigned)ov.size()), 256, 0, E.st>>>(dov, nr, part);
+        E.launched();
+        k_final_sum<<<(unsigned)((ov.size() + 127) / 128), 128, 0, E.st>>>(part, nct, 1.0, E.d_small, (int)ov.size());
+        E.launched();
+        CK(cudaMemcpyAsync(Sc.data(), E.d_small, sizeof(double) * ov.size(), cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+    }
+    // initial adjoint states
+    {
+        std::vector<AdjInit> ini;
+        size_t oi = 0;
+        for (auto &S : sw) {
+            Inst &I = E.inst[S.inst];
+            size_t k = 0;
+            while (act[k] != S.inst) k++;
+            const int j = (S.d == 0) ? S.ns : 0;
+            AdjInit a;
+            std::memset(&a, 0, sizeof(a));
+            a.lam = S.lam[0];
+            a.G = G[k];
+            a.other = (S.d == 0) ? (const T *)I.qr[S.c] + (long)j * nr : (const T *)I.qf[S.c] + (long)j * nr;
+            for (int m = 0; m < E.M; m++) a.coef[m] = S.coef[(size_t)j * PSCFG_MAXM + m];
+            a.M = E.M;
+            if (S.d == 0) {
+                while (!(ov_ic[oi].first == (int)k && ov_ic[oi].second == S.c)) oi++;
+                const double g = gQ[k] ? gQ[k][S.c] : 0.0;
+                const double sterm = (I.sys.ensemble == 0) ? Sc[oi] : 0.0;
+                a.cst = (g - sterm) / (I.Q[S.c] * (double)nr);
+                oi = 0;
+            }
+            ini.push_back(a);
+        }
+        AdjInit *di = E.upload(ini, 0);
+        k_adj_init<T><<<dim3((unsigned)std::min<long>((nr + 255) / 256, 256), (unsigned)ini.size()), 256, 0, E.st>>>(di, nr);
+        E.launched();
+    }
+    int ns_max = 0;
+    for (auto &S : sw) ns_max = std::max(ns_max, S.ns);
+    const PlaneGeom &g = E.geom();
+    for (int t = 0; t < ns_max; t++) {
+        std::vector<SweepField<T>> fl;
+        std::vector<AdjPoint> pts;
+        for (auto &S : sw) {
+            if (t >= S.ns) continue;
+            Inst &I = E.inst[S.inst];
+            size_t k = 0;
+            while (act[k] != S.inst) k++;
+            const int cur = t & 1;
+            int qslice, newslice, blk;
+            const T *qsrc, *other;
+            if (S.d == 0) {
+                qslice = S.ns - 1 - t;            // step qf_j -> qf_{j+1}
+                newslice = qslice;
+                blk = seg_block(I, S.c, qslice);
+                qsrc = (const T *)I.qf[S.c] + (long)qslice * nr;
+                other = (const T *)I.qr[S.c] + (long)newslice * nr;
+            } else {
+                qslice = t + 1;                   // step qr_s -> qr_{s-1}
+                newslice = qslice;
+                blk = seg_block(I, S.c, qslice - 1);
+                qsrc = (const T *)I.qr[S.c] + (long)qslice * nr;
+                other = (const T *)I.qf[S.c] + (long)newslice * nr;
+            }
+            for (int f = 0; f < 2; f++) {
+                SweepField<T> F;
+                std::memset(&F, 0, sizeof(F));
+                F.slab = S.dummy[f];
+                F.ns = 1;
+                F.dir = 1;
+                F.nblk = 1;
+                F.bgn[0] = 0;
+                F.bgn[1] = 1;
+                F.eo1[0] = (const T *)I.eo1[S.c][blk];
+                F.eo2[0] = (const T *)I.eo2[S.c][blk];
+                F.ek1[0] = (const T *)I.ek1[S.c][blk];
+                F.ek2[0] = (const T *)I.ek2[S.c][blk];
+                F.S1 = S.S1[f];
+                F.S2 = S.S2[f];
+                F.q1 = S.p1[f];
+                F.in = (f == 0) ? S.lam[cur] : qsrc;
+                F.out = S.dummy[f];
+                F.h_out = S.h[f];
+                F.q2_out = S.p2[f];
+                fl.push_back(F);
+            }
+            AdjPoint a;
+            std::memset(&a, 0, sizeof(a));
+            a.lam = S.lam[cur];
+            a.p1l = S.p1[0];
+            a.hl = S.h[0];
+            a.p2l = S.p2[0];
+            a.q = qsrc;
+            a.p1q = S.p1[1];
+            a.hq = S.h[1];
+            a.p2q = S.p2[1];
+            a.eo1 = I.eo1[S.c][blk];
+            a.ds = I.bds[S.c][blk];
+            a.grad = S.gbuf + (long)I.sys.block_monomer[S.c][blk] * nr;
+            a.lam_new = S.lam[cur ^ 1];
+            a.G = G[k];
+            a.other = other;
+            for (int m = 0; m < E.M; m++) a.coef[m] = S.coef[(size_t)newslice * PSCFG_MAXM + m];
+            a.M = E.M;
+            pts.push_back(a);
+        }
+        SweepField<T> *dfl = E.upload(fl, 0);
+        size_t o2 = ((fl.size() * sizeof(SweepField<T>) + 255) / 256) * 256;
+        AdjPoint *dpt = E.upload(pts, o2);
+        const int nf = (int)fl.size();
+        if (E.dim <= 2) {
+            size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)nr * sizeof(T);
+            CK(cudaFuncSetAttribute(k_sweep_plane<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            int threads = (int)std::min<long>(256, std::max<long>(32, ((nr / 2 + 31) / 32) * 32));
+            k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, 1);
+            E.launched();
+        } else if (!step3_fixed<T>(E, dfl, nf, 0)) {
+            size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
+            size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
+            CK(cudaFuncSetAttribute(k3_fwd_pair<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(cudaFuncSetAttribute(k3_inv_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(cudaFuncSetAttribute(k3_inv_final<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(cudaFuncSetAttribute(k3_zconv<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+            const long P = (long)g.n1h * g.n2;
+            const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+            k3_fwd_pair<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
+            E.launched();
+            k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 2), 256, smz, E.st>>>(dfl, g, 0, 3);
+            E.launched();
+            k3_inv_mid<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
+            E.launched();
+            k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 1), 256, smz, E.st>>>(dfl, g, 0, 2);
+            E.launched();
+            k3_inv_final<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
+            E.launched();
+        }
+        k_adj_point<T><<<dim3((unsigned)std::min<long>((nr + 255) / 256, 256), (unsigned)pts.size()), 256, 0, E.st>>>(dpt, nr);
+        E.launched();
+    }
+    // grad = sum over sweeps of the instance, fixed order
+    for (size_t k = 0; k < act.size(); k++) {
+        CK(cudaMemsetAsync(grad[k], 0, sizeof(double) * E.M * nr, E.st));
+        std::vector<const double *> parts;
+        for (auto &S : sw)
+            if (S.inst == act[k]) parts.push_back(S.gbuf);
+        for (const double *p : parts) {
+            k_axpy<<<(unsigned)std::min<long>((E.M * nr + 255) / 256, 1024), 256, 0, E.st>>>(grad[k], p, (long)E.M * nr);
+            E.launched();
+        }
+    }
+}
+
+static void adjoint_all(Engine &E, const std::vector<int> &act, const std::vector<const double *> &G,
+                        const std::vector<const double *> &gQ, const std::vector<double *> &grad)
+{
+    for (int i : act)
+        if (!E.inst[i].have_density) throw Err(PSCFG_ESTATE, "the adjoint requires a preceding density call");
+    std::vector<int> a64, a32;
+    split_prec(E, act, a64, a32);
+    if (!a32.empty()) throw Err(PSCFG_EINVAL, "the adjoint runs on FP64 propagators (use PSCFG_FP64 or PSCFG_MIXED)");
+    E.cur = PSCFG_FP64;
+    adjoint_impl<double>(E, act, G, gQ, grad);
+}
+
+// ---------------------------------------------------------------------
 // Single-field propagation (parity checks of step_exp)
 // ---------------------------------------------------------------------
 template <typename T>
@@ -1802,6 +2073,59 @@ int pscfg_set_symmetry(pscfg_engine *e, int inst, int nops, const int *ops)
 }
 
 void *pscfg_stream(const pscfg_engine *e) { return e ? (void *)e->E.st : nullptr; }
+
+static int adjoint_common(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega, bool device)
+{
+    if (!e || !grad_rho || !grad_omega) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    const int ni = (int)E.inst.size();
+    const long fl = (long)E.M * E.nr;
+    std::vector<int> all(ni);
+    std::vector<const double *> G(ni), gQ(ni);
+    std::vector<double *> out(ni);
+    double *tmp = nullptr;
+    if (!device) {
+        // stage host arrays in one device buffer: G then grad
+        CK(cudaMalloc(&tmp, sizeof(double) * fl * ni * 2));
+    }
+    for (int i = 0; i < ni; i++) {
+        all[i] = i;
+        if (device) {
+            G[i] = grad_rho + (long)i * fl;
+            out[i] = grad_omega + (long)i * fl;
+        } else {
+            CK(cudaMemcpyAsync(tmp + (long)i * fl, grad_rho + (long)i * fl, sizeof(double) * fl, cudaMemcpyHostToDevice, E.st));
+            G[i] = tmp + (long)i * fl;
+            out[i] = tmp + (long)(ni + i) * fl;
+        }
+        gQ[i] = grad_lnq ? grad_lnq + (long)i * PSCFG_MAXC : nullptr;
+    }
+    try {
+        adjoint_all(E, all, G, gQ, out);
+        if (!device) {
+            for (int i = 0; i < ni; i++)
+                CK(cudaMemcpyAsync(grad_omega + (long)i * fl, out[i], sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
+        }
+        CK(cudaStreamSynchronize(E.st));
+    } catch (...) {
+        if (tmp) cudaFree(tmp);
+        throw;
+    }
+    if (tmp) cudaFree(tmp);
+    ABI_END(e)
+}
+
+int pscfg_density_adjoint(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega)
+{
+    return adjoint_common(e, grad_rho, grad_lnq, grad_omega, false);
+}
+
+int pscfg_density_adjoint_device(pscfg_engine *e, const double *grad_rho_dev, const double *grad_lnq,
+                                 double *grad_omega_dev)
+{
+    return adjoint_common(e, grad_rho_dev, grad_lnq, grad_omega_dev, true);
+}
 
 int pscfg_set_profiling(pscfg_engine *e, int on)
 {

@@ -29,7 +29,25 @@ struct SweepField {
     // scratch for the multi-pass 3-D step (unused for dim <= 2)
     cx<T> *S1, *S2;
     T *q1;
+    // optional single-step overrides (adjoint): read `in` instead of the
+    // source slice, write `out` instead of the destination slice, and store
+    // the step intermediates P1 x (into q1), h = E1 C2 E2 x and P2 x
+    const T *in;
+    T *out;
+    T *h_out;
+    T *q2_out;
 };
+
+template <typename T>
+__device__ __forceinline__ const T *src_slice(const SweepField<T> &f, int src, long nr)
+{
+    return f.in ? f.in : f.slab + (long)src * nr;
+}
+template <typename T>
+__device__ __forceinline__ T *dst_slice(const SweepField<T> &f, int dst, long nr)
+{
+    return f.out ? f.out : f.slab + (long)dst * nr;
+}
 
 // Block index and source/destination slices of step t (0-based).
 template <typename T>
@@ -119,7 +137,10 @@ __global__ void k_sweep_plane(const SweepField<T> *fields, PlaneGeom g, int t0, 
 
     int blk, src, dst;
     if (!step_slices(f, t0, blk, src, dst)) return;
-    for (int i = threadIdx.x; i < nr; i += blockDim.x) q[i] = f.slab[(long)src * nr + i];
+    {
+        const T *qs = src_slice(f, src, nr);
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) q[i] = qs[i];
+    }
     __syncthreads();
 
     for (int t = t0; t < t1; t++) {
@@ -130,7 +151,11 @@ __global__ void k_sweep_plane(const SweepField<T> *fields, PlaneGeom g, int t0, 
         cx<T> *F = plane_forward<T>(A, B, g);
         mul_spec<T>(F, ek1, g, 0);
         cx<T> *Z = plane_inverse<T>(F, F == A ? B : A, g);
-        for (int i = threadIdx.x; i < nr; i += blockDim.x) q1[i] = eo1[i] * unpack_real<T>(Z, g, i) / rn;
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+            const T v = eo1[i] * unpack_real<T>(Z, g, i) / rn;
+            q1[i] = v;
+            if (f.q1) f.q1[i] = v;
+        }
         __syncthreads();
         // two half steps
         pack_rows<T>(A, g, [&](int r) { return eo2[r] * q[r]; });
@@ -138,16 +163,19 @@ __global__ void k_sweep_plane(const SweepField<T> *fields, PlaneGeom g, int t0, 
         mul_spec<T>(F, ek2, g, 0);
         Z = plane_inverse<T>(F, F == A ? B : A, g);
         cx<T> *O = (Z == A) ? B : A;
+        if (f.h_out)
+            for (int i = threadIdx.x; i < nr; i += blockDim.x) f.h_out[i] = eo1[i] * unpack_real<T>(Z, g, i) / rn;
         pack_rows<T>(O, g, [&](int r) { return eo1[r] * unpack_real<T>(Z, g, r) / rn; });
         F = plane_forward<T>(O, Z, g);
         mul_spec<T>(F, ek2, g, 0);
         Z = plane_inverse<T>(F, F == A ? B : A, g);
-        T *out = f.slab + (long)dst * nr;
+        T *out = dst_slice(f, dst, nr);
         for (int i = threadIdx.x; i < nr; i += blockDim.x) {
             T q2 = eo2[i] * unpack_real<T>(Z, g, i) / rn;
             T v = ((T)4 * q2 - q1[i]) / (T)3;
             q[i] = v;
             out[i] = v;
+            if (f.q2_out) f.q2_out[i] = q2;
         }
         __syncthreads();
     }
@@ -188,7 +216,7 @@ __global__ void k3_fwd_pair(const SweepField<T> *fields, PlaneGeom g, int t)
     const int z = blockIdx.x;
     const long np = (long)g.n1 * g.n2, nkp = (long)g.n1h * g.n2;
     const long nr = np * g.n3;
-    const T *q = f.slab + (long)src * nr + z * np;
+    const T *q = src_slice(f, src, nr) + z * np;
     const T *eo1 = f.eo1[blk] + z * np, *eo2 = f.eo2[blk] + z * np;
     pack_rows<T>(A, g, [&](int r) { return eo1[r] * q[r]; });
     cx<T> *F = plane_forward<T>(A, B, g);
@@ -257,6 +285,8 @@ __global__ void k3_inv_mid(const SweepField<T> *fields, PlaneGeom g, int t)
     load_plane<T>(A, f.S2 + z * nkp, g);
     Z = plane_inverse<T>(A, B, g);
     cx<T> *O = (Z == A) ? B : A;
+    if (f.h_out)
+        for (int i = threadIdx.x; i < (int)np; i += blockDim.x) f.h_out[z * np + i] = eo1[i] * unpack_real<T>(Z, g, i) / rn;
     pack_rows<T>(O, g, [&](int r) { return eo1[r] * unpack_real<T>(Z, g, r) / rn; });
     cx<T> *F = plane_forward<T>(O, Z, g);
     store_plane<T>(f.S2 + z * nkp, F, g);
@@ -278,12 +308,13 @@ __global__ void k3_inv_final(const SweepField<T> *fields, PlaneGeom g, int t)
     const T rn = (T)nr;
     const T *eo2 = f.eo2[blk] + z * np;
     const T *q1 = f.q1 + z * np;
-    T *out = f.slab + (long)dst * nr + z * np;
+    T *out = dst_slice(f, dst, nr) + z * np;
     load_plane<T>(A, f.S2 + z * nkp, g);
     cx<T> *Z = plane_inverse<T>(A, B, g);
     for (int i = threadIdx.x; i < (int)np; i += blockDim.x) {
         T q2 = eo2[i] * unpack_real<T>(Z, g, i) / rn;
         out[i] = ((T)4 * q2 - q1[i]) / (T)3;
+        if (f.q2_out) f.q2_out[z * np + i] = q2;
     }
 }
 

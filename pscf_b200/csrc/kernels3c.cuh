@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(256) k3c_fwd_pair(const SweepField<T> *fields,
     cx<T> *buf = (cx<T> *)smem_raw;
     const long nr = (long)N1 * N2 * N3;
     const int z0 = blockIdx.x * PPC;
-    const T *q = f.slab + (long)src * nr + (long)z0 * PSk::NP;
+    const T *q = src_slice(f, src, nr) + (long)z0 * PSk::NP;
     const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP, *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
     const cx<T> *twM = (const cx<T> *)g.row.tw, *twN2 = (const cx<T> *)g.col.tw, *twN1 = (const cx<T> *)g.rtw;
     PSk::pack(buf, [&](int e) { return eo1[e] * q[e]; });
@@ -259,11 +259,16 @@ __global__ void __launch_bounds__(256) k3c_inv_mid(const SweepField<T> *fields, 
     PSk::load(buf, f.S2 + (long)z0 * PSk::PS);
     PSk::inverse(buf, twM, twN2, twN1);
     // h = eo1 y / N, packed in place: entry (p, y, m) <- (h(2m), h(2m+1))
+    T *hout = f.h_out ? f.h_out + (long)z0 * PSk::NP : nullptr;
     for (int i = threadIdx.x; i < PPC * N2 * PSk::M; i += blockDim.x) {
         const int p = i / (N2 * PSk::M), r = i % (N2 * PSk::M), y = r / PSk::M, m = r % PSk::M;
         const int e = p * PSk::NP + y * N1 + 2 * m;
         cx<T> &z = buf[p * PSk::PS + y * PSk::NH + m];
         z = mk<T>(eo1[e] * z.x / rn, eo1[e + 1] * z.y / rn);
+        if (hout) {
+            hout[e] = z.x;
+            hout[e + 1] = z.y;
+        }
     }
     PSk::forward(buf, twM, twN2, twN1);
     PSk::store(f.S2 + (long)z0 * PSk::PS, buf);
@@ -284,13 +289,15 @@ __global__ void __launch_bounds__(256) k3c_inv_final(const SweepField<T> *fields
     const int z0 = blockIdx.x * PPC;
     const T *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
     const T *q1 = f.q1 + (long)z0 * PSk::NP;
-    T *out = f.slab + (long)dst * nr + (long)z0 * PSk::NP;
+    T *out = dst_slice(f, dst, nr) + (long)z0 * PSk::NP;
+    T *q2o = f.q2_out ? f.q2_out + (long)z0 * PSk::NP : nullptr;
     const cx<T> *twM = (const cx<T> *)g.row.tw, *twN2 = (const cx<T> *)g.col.tw, *twN1 = (const cx<T> *)g.rtw;
     PSk::load(buf, f.S2 + (long)z0 * PSk::PS);
     PSk::inverse(buf, twM, twN2, twN1);
     for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
         const T q2 = eo2[e] * PSk::real_at(buf, e) / rn;
         out[e] = ((T)4 * q2 - q1[e]) / (T)3;
+        if (q2o) q2o[e] = q2;
     }
 }
 

@@ -208,6 +208,11 @@ static __global__ void k_solvent_rho(const SolventJob *jobs, int njobs, long nr)
     }
 }
 
+static __global__ void k_axpy(double *y, const double *x, long n)
+{
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) y[i] += x[i];
+}
+
 static __global__ void k_zero(double *p, long n)
 {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) p[i] = 0.0;

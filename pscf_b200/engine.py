@@ -104,6 +104,8 @@ SIGNATURES = {
     "pscfg_get_profile": (C.c_int, [_vp, _dp]),
     "pscfg_propagate_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), _vp, _vp, C.c_double, C.c_double,
                                           _vp, _vp, C.c_int, _vp]),
+    "pscfg_density_adjoint": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "pscfg_density_adjoint_device": (C.c_int, [_vp, _vp, _dp, _vp]),
     "pscfg_steps_per_density": (C.c_long, [_vp]),
     "pscfg_launch_count": (C.c_long, [_vp]),
 }
@@ -231,6 +233,18 @@ class Engine:
         q = np.zeros((self.n_inst, MAX_CHAIN))
         self._check(self.lib.pscfg_density_device(self._h, _vp(omega_dev_ptr), _vp(rho_dev_ptr), _ptr(q), None))
         return q
+
+    def density_adjoint(self, grad_rho, grad_lnq=None) -> np.ndarray:
+        """dL/domega for upstream dL/drho [n_inst][M][nr] and dL/dlnQ [n_inst][n_chain]."""
+        G = np.ascontiguousarray(grad_rho, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
+        gq = None
+        if grad_lnq is not None:
+            gq = np.zeros((self.n_inst, MAX_CHAIN))
+            a = np.asarray(grad_lnq, dtype=np.float64).reshape(self.n_inst, -1)
+            gq[:, : a.shape[1]] = a
+        out = np.zeros_like(G)
+        self._check(self.lib.pscfg_density_adjoint(self._h, _ptr(G), None if gq is None else _ptr(gq), _ptr(out)))
+        return out
 
     def scf_stress(self) -> np.ndarray:
         out = np.zeros((self.n_inst, MAX_CELL_PARAM))
