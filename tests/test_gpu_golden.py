@@ -126,3 +126,27 @@ def test_mixed_precision_matches_fp64_solution():
         assert b["itr_fp32"] > 0
         assert abs(a["f_helmholtz"] - b["f_helmholtz"]) < 1e-10
         assert abs(b["f_helmholtz"] - g["f_Helmholtz"][0]) < 2e-10
+
+
+def test_newton_bcc_golden_batched_jacobian():
+    """iterate_NR on the engine: the 290 finite-difference Jacobian columns
+    of the BCC fixture (146 stars) are one batched density call."""
+    from pscf_b200.basis import StarBasis
+    from pscf_b200.newton import EngineProvider, iterate_nr
+    g = GOLD["bcc_sweep"][0]
+    s = diblock(3, [20, 20, 20], "cubic", g["cell_param"], fA=g["block_length"][0], chiN=g["chi"][0])
+    basis = StarBasis("I m -3 m", [20, 20, 20])
+    assert basis.n_star == int(g["N_star"][0])
+    # start from a partly converged Anderson state, as the reference's
+    # sweep starts from the previous point
+    e = Engine([s])
+    e.set_symmetry(0, "I m -3 m")
+    w0, _, _ = e.iterate_am(sphere_guess(s, s.chains[0].block_length[0], width=0.05)[None], error_max=1e-3,
+                            max_itr=200)
+    prov = EngineProvider(s, "I m -3 m", max_batch=146)
+    w, rho, r = iterate_nr(prov, basis, s, w0[0], error_max=1e-10, max_itr=40)
+    assert r["converged"], r["error"]
+    e.density(w[None])
+    f, p, mu = e.free_energy()
+    assert abs(f[0] - g["f_Helmholtz"][0]) < 2e-10
+    assert abs(mu[0, 0] - g["mu_chain"][0]) < 2e-10
