@@ -91,6 +91,42 @@ def initial_omega(system, inst):
     return out
 
 
+def c4_batches(seed_base):
+    """The mixed batch: 96 lamellae (64 points, group -1), 96 hexagonal
+    cylinders (p 6 m m, 64 x 64), 64 BCC spheres (I m -3 m, 32^3); AB diblocks
+    with f_A ~ U[0.2, 0.5], chiN ~ U[12, 30], ds = 0.01; starting cells from
+    strong-segregation scaling (chiN/20)^(1/6) times d = 1.7, a_hex = 1.9,
+    a_bcc = 1.95 (half the 3.9 of the single-instance workload, which lies
+    beyond the sphere phase's cell at these chiN)."""
+    from pscf_b200 import guess
+    from pscf_b200.batch import ShapeBatch
+    from pscf_b200.system import Chain, System
+    rng = np.random.default_rng(seed_base)
+    out = []
+    for kind, count in (("lam", 96), ("hex", 96), ("bcc", 64)):
+        systems, omegas = [], []
+        for i in range(count):
+            fA = float(rng.uniform(0.2, 0.5))
+            chiN = float(rng.uniform(12.0, 30.0))
+            sc = (chiN / 20.0) ** (1.0 / 6.0)
+            chi = [[0.0, chiN], [chiN, 0.0]]
+            ch = [Chain([0, 1], [fA, 1.0 - fA])]
+            if kind == "lam":
+                s = System(1, [64], "lamellar", [1.7 * sc], [1.0, 1.0], chi, ch, DS)
+                w = guess.lamellar(s, fA, noise=0.01, seed=seed_base + i)
+            elif kind == "hex":
+                s = System(2, [64, 64], "hexagonal", [1.9 * sc], [1.0, 1.0], chi, ch, DS)
+                w = guess.cylinders(s, fA, noise=0.01, seed=seed_base + i)
+            else:
+                s = System(3, [32, 32, 32], "cubic", [1.95 * sc], [1.0, 1.0], chi, ch, DS)
+                w = guess.spheres_bcc(s, fA, noise=0.01, seed=seed_base + i)
+            systems.append(s)
+            omegas.append(w)
+        group = {"lam": "-1", "hex": "p 6 m m", "bcc": "I m -3 m"}[kind]
+        out.append(ShapeBatch(systems, np.stack(omegas), group))
+    return out
+
+
 def bytes_per_step(system, wq=8, ww=8):
     """Algorithmic HBM bytes of one MDE step: read q(s), write q(s +- ds),
     read the block's omega: N_r (2 w_q + w_omega)."""
@@ -281,6 +317,8 @@ def run_ours(args, rank, world, local_rank):
     value = total_steps / elapsed
 
     # ---- converged solves/s: fresh full solve of the batch ---------------
+    for i in range(B):                     # back to the starting cell a = 3.9
+        e.set_cell_param(i, [CELL])
     barrier()
     ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev2.record(stream)
@@ -359,6 +397,31 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * n_e2e * e.steps_per_density / float(te.item())
 
+    # ---- the mixed-shape batch (lamellae + cylinders + spheres) -----------
+    c4 = None
+    if not args.no_c4:
+        from pscf_b200.batch import solve_batches
+        batches = c4_batches(20261203 + 3 + 1000 * rank)
+        barrier()
+        t0 = time.perf_counter()
+        results = solve_batches(batches, error_max=1e-9, max_itr=1000, n_hist=20, domain=True)
+        torch.cuda.synchronize()
+        c4_s = time.perf_counter() - t0
+        nconv = sum(1 for rs in results for r in rs if r["converged"])
+        ninst = sum(len(rs) for rs in results)
+        tc = torch.tensor([c4_s, float(nconv), float(ninst)], dtype=torch.float64, device=dev)
+        if world > 1:
+            for k, op in ((0, dist.ReduceOp.MAX), (1, dist.ReduceOp.SUM), (2, dist.ReduceOp.SUM)):
+                x = tc[k:k + 1].clone()
+                dist.all_reduce(x, op=op)
+                tc[k] = x[0]
+        c4 = {"instances": int(tc[2].item()), "converged": int(tc[1].item()), "seconds": float(tc[0].item()),
+              "solves_per_s": float(tc[1].item()) / float(tc[0].item()),
+              "per_shape_converged": [sum(1 for r in rs if r["converged"]) for rs in results],
+              "note": "wall clock of concurrent engines (one host thread and stream per grid shape)"}
+        for b in batches:
+            b.engine.close()
+
     if rank != 0:
         return
     s0 = systems[0]
@@ -396,6 +459,7 @@ def run_ours(args, rank, world, local_rank):
                      "traffic": traffic, "kernel": "MDE step (sweep kernels)",
                      "bytes_per_step": bstep, "sweep_ms": prof["sweep_ms"], "steps": steps_done},
         "phase_ms": {k: prof[k] for k in ("sweep_ms", "contour_ms", "stress_ms")},
+        "mixed_shape_batch": c4,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": cpu,
@@ -411,6 +475,7 @@ def main():
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-c4", action="store_true", help="skip the mixed-shape batch leg")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

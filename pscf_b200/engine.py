@@ -10,6 +10,7 @@ raises, there is no CPU fallback.
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
 import os
 from typing import List, Sequence
@@ -178,7 +179,8 @@ class Engine:
         self.lib = load_library()
         if isinstance(systems, System):
             systems = [systems]
-        self.systems: List[System] = list(systems)
+        # private copies: cell relaxation updates these, never the caller's objects
+        self.systems: List[System] = [copy.deepcopy(s) for s in systems]
         arr = (PscfgSystem * len(self.systems))(*[to_c(s) for s in self.systems])
         h = _vp()
         rc = self.lib.pscfg_create(arr, len(self.systems), precision, C.byref(h))

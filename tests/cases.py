@@ -82,46 +82,9 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-BCC_SITES = [(0.0, 0.0, 0.0), (0.5, 0.5, 0.5)]
-HEX_SITES = [(0.0, 0.0)]
+from pscf_b200.guess import BCC_SITES, HEX_SITES, site_density, omega_from_density  # noqa: E402
 
 
 def sphere_guess(system, fA, sites=BCC_SITES, width=0.08, chiN=None):
-    """omega from a target A density of tanh-edged spheres at `sites`.
-
-    rho_A = 1/2 (1 - tanh((d - R)/w)) with d the minimum-image distance
-    (in Cartesian cell units) to the nearest site and R set so that the mean
-    of rho_A is fA; then omega_A - omega_B = chi (1 - 2 rho_A) around the
-    uniform values chi . phi_mon.
-    """
-    import math
-    n = system.n
-    dim = system.dim
-    G, _, _ = system.unit_cell()
-    R = 2 * math.pi * np.linalg.inv(G[:dim, :dim]).T   # rows: Bravais vectors
-    axes = [np.arange(n[d]) / n[d] for d in range(dim)]
-    grids = np.meshgrid(*axes[::-1], indexing="ij")[::-1]   # x fastest
-    frac = np.stack([g.ravel() for g in grids], axis=1)     # [nr, dim]
-    dmin = np.full(frac.shape[0], np.inf)
-    for c in sites:
-        df = frac - np.array(c[:dim])
-        df -= np.round(df)
-        for shift in np.array(np.meshgrid(*[[-1, 0, 1]] * dim)).T.reshape(-1, dim):
-            v = (df + shift) @ R
-            dmin = np.minimum(dmin, np.sqrt((v * v).sum(axis=1)))
-    scale = float(np.abs(np.linalg.det(R))) ** (1.0 / dim)
-    w = width * scale
-    lo, hi = 0.0, scale
-    for _ in range(60):
-        Rs = 0.5 * (lo + hi)
-        m = np.mean(0.5 * (1 - np.tanh((dmin - Rs) / w)))
-        lo, hi = (Rs, hi) if m < fA else (lo, Rs)
-    rhoA = 0.5 * (1 - np.tanh((dmin - Rs) / w))
-    chi = system.chi[0, 1] if chiN is None else chiN
-    w0 = system.omega_uniform()
-    d = chi * (1 - 2 * rhoA)
-    d -= d.mean()
-    out = np.zeros((2, system.nr))
-    out[0] = w0[0] + 0.5 * d
-    out[1] = w0[1] - 0.5 * d
-    return out
+    """omega from tanh-edged spheres at `sites` (pscf_b200.guess)."""
+    return omega_from_density(system, site_density(system, fA, sites, width))

@@ -150,3 +150,25 @@ def test_newton_bcc_golden_batched_jacobian():
     f, p, mu = e.free_energy()
     assert abs(f[0] - g["f_Helmholtz"][0]) < 2e-10
     assert abs(mu[0, 0] - g["mu_chain"][0]) < 2e-10
+
+
+def test_mixed_shape_batches_concurrent():
+    """Lamellae, cylinders and spheres as three engines driven concurrently
+    give the same converged results as each solved on its own."""
+    from pscf_b200 import guess
+    from pscf_b200.batch import ShapeBatch, solve_batches
+    lam = [diblock(1, [64], "lamellar", [1.7], fA=0.5, chiN=20.0), diblock(1, [64], "lamellar", [1.8], fA=0.45, chiN=22.0)]
+    hexs = [diblock(2, [32, 32], "hexagonal", [1.9], fA=0.3, chiN=20.0)]
+    bcc = [diblock(3, [16, 16, 16], "cubic", [1.95], fA=0.25, chiN=20.0)]
+    mk = lambda: [ShapeBatch(lam, np.stack([guess.lamellar(s, s.chains[0].block_length[0]) for s in lam]), "-1"),
+                  ShapeBatch(hexs, np.stack([guess.cylinders(s, 0.3) for s in hexs]), "p 6 m m"),
+                  ShapeBatch(bcc, np.stack([guess.spheres_bcc(s, 0.25) for s in bcc]), "I m -3 m")]
+    together = solve_batches(mk(), error_max=1e-9, max_itr=800, domain=True)
+    alone = []
+    for b in mk():
+        _, _, r = b.engine.iterate_am(b.omega0, error_max=1e-9, max_itr=800, domain=True)
+        alone.append(r)
+    for rs1, rs2 in zip(together, alone):
+        for r1, r2 in zip(rs1, rs2):
+            assert r1["converged"] and r2["converged"]
+            assert r1["f_helmholtz"] == r2["f_helmholtz"] and r1["itr"] == r2["itr"]
