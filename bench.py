@@ -316,7 +316,58 @@ def run_ours(args, rank, world, local_rank):
         elapsed, total_steps = ms / 1e3, float(steps_done)
     value = total_steps / elapsed
 
-    # ---- converged solves/s: fresh full solve of the batch ---------------
+    # ---- converged solves/s, mixed precision, end to end, mixed shapes ----
+    solve = None if args.no_solve else solve_legs(e, systems, omega0, B, stream, barrier, dev, world)
+    e2e_value, e2e_bytes = e2e_leg(e, omega0, B, args, stream, barrier, dev, world)
+    c4 = None if args.no_c4 else c4_leg(rank, world, barrier, dev)
+
+    if rank != 0:
+        return
+    s0 = systems[0]
+    bstep = bytes_per_step(s0)
+    peak, peak_kind = measured_peaks()
+    sweep_s = prof["sweep_ms"] / 1e3
+    achieved = steps_done * bstep / sweep_s / 1e9 if sweep_s > 0 else None
+    traffic = ncu_traffic_per_step()
+    cpu = None
+    if world == 1 and not args.no_cpu:
+        nthreads = os.cpu_count() or 1
+        rate, dt = cpu_mde_rate(nthreads, 4)
+        cpu = {"value": rate, "unit": "MDE steps/s", "cores": nthreads, "kind": "port",
+               "sample": f"{nthreads} threads x 4 step_exp calls of the FP64 C oracle on the 32^3 grid "
+                         f"({dt:.1f} s)"}
+    line = {
+        "metric": "MDE steps/s", "value": value, "unit": "MDE steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "batch_per_gpu": B, "grid": [N_GRID] * 3,
+                   "contour_steps_per_chain": s0.contour_steps(), "parallelism": f"instances x{world}",
+                   "l2": "inputs larger than L2 (propagator slabs %.1f GB per GPU)" % (B * 2 * 103 * s0.nr * 8 / 1e9)},
+    }
+    if solve is not None:
+        line.update(solve)
+    line.update({
+        "e2e": {"value": e2e_value, "unit": "MDE steps/s", "api": "pscfg_density + pscfg_stress (host buffers)",
+                "h2d_bytes_per_step": e2e_bytes[0], "d2h_bytes_per_step": e2e_bytes[1]},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
+                     "traffic": traffic, "kernel": "MDE step (sweep kernels)",
+                     "bytes_per_step": bstep, "sweep_ms": prof["sweep_ms"], "steps": steps_done},
+        "phase_ms": {k: prof[k] for k in ("sweep_ms", "contour_ms", "stress_ms")},
+        "mixed_shape_batch": c4,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    })
+    print(json.dumps(line), flush=True)
+
+
+def solve_legs(e, systems, omega0, B, stream, barrier, dev, world):
+    """Full solves of the batch from the starting cell: FP64, then mixed
+    FP32 -> FP64 in a second engine.  Returns the JSON keys of both."""
+    import torch
+    import torch.distributed as dist
+    from pscf_b200.engine import Engine, MIXED
     for i in range(B):                     # back to the starting cell a = 3.9
         e.set_cell_param(i, [CELL])
     barrier()
@@ -343,8 +394,6 @@ def run_ours(args, rank, world, local_rank):
     else:
         solve_s_all, conv_all = solve_s, float(conv)
 
-    # ---- mixed precision solve of the same batch (FP32 then FP64) ---------
-    from pscf_b200.engine import MIXED
     em = Engine(systems, MIXED)
     for i in range(B):
         em.set_symmetry(i, "I m -3 m")
@@ -369,12 +418,28 @@ def run_ours(args, rank, world, local_rank):
             dist.all_reduce(x, op=op)
             tm[k] = x[0]
     em.close()
+    mixed_rate = float(tm[1].item()) / float(tm[0].item())
+    return {
+        "solves_per_s": conv_all / solve_s_all, "solve_seconds": solve_s_all, "solves_converged": int(conv_all),
+        "solve_iterations": {"min": int(min(itrs)), "max": int(max(itrs)), "mean": float(np.mean(itrs))},
+        "mixed_precision": {"solves_per_s": mixed_rate, "speedup_vs_fp64": mixed_rate / (conv_all / solve_s_all),
+                            "max_abs_dF_vs_fp64": float(tm[2].item()), "mean_fp32_iterations": itr32,
+                            "solves_converged": int(tm[1].item())},
+        "f_helmholtz": {"min": float(min(fvals)), "max": float(max(fvals))},
+        "cell_param": {"min": float(min(cells)), "max": float(max(cells))},
+    }
 
-    # ---- end to end through the C ABI with host buffers ------------------
+
+def e2e_leg(e, omega0, B, args, stream, barrier, dev, world):
+    """MDE steps/s through the C ABI (pscfg_density + pscfg_stress) with
+    pinned host buffers: host->device fields and device->host densities,
+    Q and stress inside the timed region.  Returns (value, (h2d, d2h))."""
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
     w_pin = torch.from_numpy(omega0.copy()).pin_memory()
     rho_pin = torch.empty_like(w_pin).pin_memory()
     q = np.zeros((B, 4))
-    import ctypes as C
     lib = e.lib
     dp = C.POINTER(C.c_double)
     wp = C.cast(w_pin.data_ptr(), dp)
@@ -395,76 +460,37 @@ def run_ours(args, rank, world, local_rank):
     te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n_e2e * e.steps_per_density / float(te.item())
+    value = world * n_e2e * e.steps_per_density / float(te.item())
+    return value, (int(omega0.nbytes), int(omega0.nbytes + q.nbytes + stress.nbytes))
 
-    # ---- the mixed-shape batch (lamellae + cylinders + spheres) -----------
-    c4 = None
-    if not args.no_c4:
-        from pscf_b200.batch import solve_batches
-        batches = c4_batches(20261203 + 3 + 1000 * rank)
-        barrier()
-        t0 = time.perf_counter()
-        results = solve_batches(batches, error_max=1e-9, max_itr=1000, n_hist=20, domain=True)
-        torch.cuda.synchronize()
-        c4_s = time.perf_counter() - t0
-        nconv = sum(1 for rs in results for r in rs if r["converged"])
-        ninst = sum(len(rs) for rs in results)
-        tc = torch.tensor([c4_s, float(nconv), float(ninst)], dtype=torch.float64, device=dev)
-        if world > 1:
-            for k, op in ((0, dist.ReduceOp.MAX), (1, dist.ReduceOp.SUM), (2, dist.ReduceOp.SUM)):
-                x = tc[k:k + 1].clone()
-                dist.all_reduce(x, op=op)
-                tc[k] = x[0]
-        c4 = {"instances": int(tc[2].item()), "converged": int(tc[1].item()), "seconds": float(tc[0].item()),
-              "solves_per_s": float(tc[1].item()) / float(tc[0].item()),
-              "per_shape_converged": [sum(1 for r in rs if r["converged"]) for rs in results],
-              "note": "wall clock of concurrent engines (one host thread and stream per grid shape)"}
-        for b in batches:
-            b.engine.close()
 
-    if rank != 0:
-        return
-    s0 = systems[0]
-    bstep = bytes_per_step(s0)
-    peak, peak_kind = measured_peaks()
-    sweep_s = prof["sweep_ms"] / 1e3
-    achieved = steps_done * bstep / sweep_s / 1e9 if sweep_s > 0 else None
-    traffic = ncu_traffic_per_step()
-    cpu = None
-    if world == 1 and not args.no_cpu:
-        nthreads = os.cpu_count() or 1
-        rate, dt = cpu_mde_rate(nthreads, 4)
-        cpu = {"value": rate, "unit": "MDE steps/s", "cores": nthreads, "kind": "port",
-               "sample": f"{nthreads} threads x 4 step_exp calls of the FP64 C oracle on the 32^3 grid "
-                         f"({dt:.1f} s)"}
-    line = {
-        "metric": "MDE steps/s", "value": value, "unit": "MDE steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "batch_per_gpu": B, "grid": [N_GRID] * 3,
-                   "contour_steps_per_chain": s0.contour_steps(), "parallelism": f"instances x{world}",
-                   "l2": "inputs larger than L2 (propagator slabs %.1f GB per GPU)" % (B * 2 * 103 * s0.nr * 8 / 1e9)},
-        "solves_per_s": conv_all / solve_s_all, "solve_seconds": solve_s_all, "solves_converged": int(conv_all),
-        "solve_iterations": {"min": int(min(itrs)), "max": int(max(itrs)), "mean": float(np.mean(itrs))},
-        "mixed_precision": {"solves_per_s": float(tm[1].item()) / float(tm[0].item()),
-                            "speedup_vs_fp64": (float(tm[1].item()) / float(tm[0].item())) / (conv_all / solve_s_all),
-                            "max_abs_dF_vs_fp64": float(tm[2].item()), "mean_fp32_iterations": itr32,
-                            "solves_converged": int(tm[1].item())},
-        "f_helmholtz": {"min": float(min(fvals)), "max": float(max(fvals))},
-        "cell_param": {"min": float(min(cells)), "max": float(max(cells))},
-        "e2e": {"value": e2e_value, "unit": "MDE steps/s", "api": "pscfg_density + pscfg_stress (host buffers)",
-                "h2d_bytes_per_step": int(omega0.nbytes), "d2h_bytes_per_step": int(omega0.nbytes + q.nbytes + stress.nbytes)},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "peak_kind": peak_kind,
-                     "traffic": traffic, "kernel": "MDE step (sweep kernels)",
-                     "bytes_per_step": bstep, "sweep_ms": prof["sweep_ms"], "steps": steps_done},
-        "phase_ms": {k: prof[k] for k in ("sweep_ms", "contour_ms", "stress_ms")},
-        "mixed_shape_batch": c4,
-        "gpu_launches": int(launches),
-        "clocks": clocks,
-        "cpu_baseline": cpu,
-    }
-    print(json.dumps(line), flush=True)
+def c4_leg(rank, world, barrier, dev):
+    """Concurrent solve of the mixed-shape batch (one engine and stream per
+    grid shape), wall clock."""
+    import torch
+    import torch.distributed as dist
+    from pscf_b200.batch import solve_batches
+    batches = c4_batches(20261203 + 3 + 1000 * rank)
+    barrier()
+    t0 = time.perf_counter()
+    results = solve_batches(batches, error_max=1e-9, max_itr=1000, n_hist=20, domain=True)
+    torch.cuda.synchronize()
+    c4_s = time.perf_counter() - t0
+    nconv = sum(1 for rs in results for r in rs if r["converged"])
+    ninst = sum(len(rs) for rs in results)
+    tc = torch.tensor([c4_s, float(nconv), float(ninst)], dtype=torch.float64, device=dev)
+    if world > 1:
+        for k, op in ((0, dist.ReduceOp.MAX), (1, dist.ReduceOp.SUM), (2, dist.ReduceOp.SUM)):
+            x = tc[k:k + 1].clone()
+            dist.all_reduce(x, op=op)
+            tc[k] = x[0]
+    out = {"instances": int(tc[2].item()), "converged": int(tc[1].item()), "seconds": float(tc[0].item()),
+           "solves_per_s": float(tc[1].item()) / float(tc[0].item()),
+           "per_shape_converged": [sum(1 for r in rs if r["converged"]) for rs in results],
+           "note": "wall clock of concurrent engines (one host thread and stream per grid shape)"}
+    for b in batches:
+        b.engine.close()
+    return out
 
 
 def main():
@@ -476,6 +502,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c4", action="store_true", help="skip the mixed-shape batch leg")
+    ap.add_argument("--no-solve", action="store_true",
+                    help="time the Anderson iterations only (no full FP64 / mixed solves; profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -26,9 +26,11 @@
 
 #include "../../include/pscf_gpu.h"
 #include "host_geom.h"
+#include "launch_util.h"
 #include "scf_kernels.cuh"
 #include "kernels3c.cuh"
 #include "adjoint.cuh"
+#include "kernels3x.cuh"
 
 namespace pscfg {
 
@@ -82,7 +84,9 @@ struct Inst {
     double *adj_coef[PSCFG_MAXC] = {};    // [ns+1][MAXM] device
     // space group imposed on omega (0 ops: none)
     int nops = 0;
-    int *d_ops = nullptr;
+    int *d_orb_perm = nullptr;   // real-space orbits of the group on the grid
+    int *d_orb_start = nullptr;
+    int norb = 0;
     double *kweight = nullptr;    // [nk] star weights (nullptr: exact Parseval weights)
 };
 
@@ -98,6 +102,7 @@ struct Engine {
     long launches = 0;
     int n_hist_alloc = 0;
     bool no_fixed_kernels = false;   // force the run-time sized kernels (tests)
+    bool cluster_step = false;       // one-launch cluster step for 32^3 (PSCFG_CLUSTER_STEP=1)
     // optional CUDA-event timing of the phases (ms, accumulated)
     bool profiling = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -351,6 +356,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     {
         const char *v = std::getenv("PSCFG_GENERIC_KERNELS");
         E.no_fixed_kernels = v && v[0] && v[0] != '0';
+        const char *c = std::getenv("PSCFG_CLUSTER_STEP");
+        E.cluster_step = c && c[0] && c[0] != '0';
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
@@ -421,15 +428,9 @@ static void step3c(Engine &E, const SweepField<T> *dfl, int nf, int t)
     const PlaneGeom &g = E.geom();
     const int ntile = (P + TC - 1) / TC;
     const size_t sm = sizeof(cx<T>) * PPC * P;
-    static bool attr[64] = {};
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64 || !attr[dev]) {
-        CK(cudaFuncSetAttribute(k3c_fwd_pair<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        CK(cudaFuncSetAttribute(k3c_inv_mid<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        CK(cudaFuncSetAttribute(k3c_inv_final<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        if (dev >= 0 && dev < 64) attr[dev] = true;
-    }
+    CK(allow_dyn_smem((const void *)k3c_fwd_pair<T, N1, N2, N3, PPC>));
+    CK(allow_dyn_smem((const void *)k3c_inv_mid<T, N1, N2, N3, PPC>));
+    CK(allow_dyn_smem((const void *)k3c_inv_final<T, N1, N2, N3, PPC>));
     k3c_fwd_pair<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, nf), 256, sm, E.st>>>(dfl, g, t);
     E.launched();
     k3c_zconv<T, N1, N2, N3, TC><<<dim3(ntile, nf, 2), 256, 0, E.st>>>(dfl, g, t, 3);
@@ -448,7 +449,17 @@ static bool step3_fixed(Engine &E, const SweepField<T> *dfl, int nf, int t)
 {
     if (E.no_fixed_kernels) return false;
     const int a = E.n[0], b = E.n[1], c = E.n[2];
-    if (a == 32 && b == 32 && c == 32) { step3c<T, 32, 32, 32, 8>(E, dfl, nf, t); return true; }
+    if (a == 32 && b == 32 && c == 32) {
+        if (E.cluster_step) {
+            const size_t sm = Cl32<T>::smem_bytes();
+            CK(allow_dyn_smem((const void *)k3x_step32<T>));
+            k3x_step32<T><<<dim3(8 * nf), 512, sm, E.st>>>(dfl, E.geom(), t);
+            E.launched();
+            return true;
+        }
+        step3c<T, 32, 32, 32, 8>(E, dfl, nf, t);
+        return true;
+    }
     if (a == 16 && b == 16 && c == 16) { step3c<T, 16, 16, 16, 8>(E, dfl, nf, t); return true; }
     if (a == 64 && b == 64 && c == 64) { step3c<T, 64, 64, 64, 1>(E, dfl, nf, t); return true; }
     return false;
@@ -519,7 +530,7 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
     if (E.dim <= 2) {
         size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)E.nr * sizeof(T);
         if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
-        CK(cudaFuncSetAttribute(k_sweep_plane<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
         int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
         k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, ns_max);
         E.launched();
@@ -527,10 +538,10 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
         size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
         size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
         if (smxy > 227 * 1024 || smz > 227 * 1024) throw Err(PSCFG_EINVAL, "grid plane too large");
-        CK(cudaFuncSetAttribute(k3_fwd_pair<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-        CK(cudaFuncSetAttribute(k3_inv_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-        CK(cudaFuncSetAttribute(k3_inv_final<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-        CK(cudaFuncSetAttribute(k3_zconv<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+        CK(allow_dyn_smem((const void *)k3_fwd_pair<T>));
+        CK(allow_dyn_smem((const void *)k3_inv_mid<T>));
+        CK(allow_dyn_smem((const void *)k3_inv_final<T>));
+        CK(allow_dyn_smem((const void *)k3_zconv<T, Z_TILE>));
         const long P = (long)g.n1h * g.n2;
         const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
         const int txy = 256, tz = 256;
@@ -743,13 +754,7 @@ static void stress3c(Engine &E, const StressJob<T> *dj, int s0, int cnt)
     const int ntile = (P + TC - 1) / TC;
     const PlaneGeom &g = E.geom();
     const size_t sm = sizeof(cx<T>) * PPC * P;
-    static bool attr[64] = {};
-    int dev = 0;
-    CK(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64 || !attr[dev]) {
-        CK(cudaFuncSetAttribute(k3c_stress_xy<T, N1, N2, N3, PPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        if (dev >= 0 && dev < 64) attr[dev] = true;
-    }
+    CK(allow_dyn_smem((const void *)k3c_stress_xy<T, N1, N2, N3, PPC>));
     k3c_stress_xy<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, cnt, 2), 256, sm, E.st>>>(dj, g, s0, (cx<T> *)E.spec);
     E.launched();
     k3c_stress_z<T, N1, N2, N3, TC><<<dim3(ntile, cnt), 256, 0, E.st>>>(dj, g, s0, (const cx<T> *)E.spec, E.stress_part);
@@ -795,7 +800,7 @@ static void stress_impl(Engine &E, const std::vector<int> &act)
         for (auto &j : jobs) maxs = std::max(maxs, j.nslices);
         size_t sm = 4 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
         if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the plane stress kernel");
-        CK(cudaFuncSetAttribute(k2_stress_slices<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        CK(allow_dyn_smem((const void *)k2_stress_slices<T>));
         int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
         k2_stress_slices<T><<<dim3(maxs, (unsigned)jobs.size()), threads, sm, E.st>>>(dj, g);
         E.launched();
@@ -804,8 +809,8 @@ static void stress_impl(Engine &E, const std::vector<int> &act)
         const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
         size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
         size_t smz = 4 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
-        CK(cudaFuncSetAttribute(k3_stress_xy<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-        CK(cudaFuncSetAttribute(k3_stress_z<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+        CK(allow_dyn_smem((const void *)k3_stress_xy<T>));
+        CK(allow_dyn_smem((const void *)k3_stress_z<T, Z_TILE>));
         // chunk of slices so that the spectra scratch stays below ~1 GB
         const size_t per_slice = 2 * (size_t)E.nk * sizeof(cx<T>);
         int cs = (int)std::max<size_t>(1, std::min<size_t>(256, ((size_t)1 << 30) / per_slice));
@@ -935,7 +940,7 @@ static void fe_spectral(Engine &E, const std::vector<int> &which, std::vector<do
         const int nf = (int)src.size();
         size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<double>);
         if (E.dim <= 2) {
-            CK(cudaFuncSetAttribute(k2_fft_fields, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
+            CK(allow_dyn_smem((const void *)k2_fft_fields));
             int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
             k2_fft_fields<<<nf, threads, smxy, E.st>>>(dsrc, ddst, g);
             E.launched();
@@ -943,8 +948,8 @@ static void fe_spectral(Engine &E, const std::vector<int> &which, std::vector<do
             const long P = (long)g.n1h * g.n2;
             const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
             size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<double>);
-            CK(cudaFuncSetAttribute(k3_fft_fields_xy, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-            CK(cudaFuncSetAttribute(k3_fft_fields_z<Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+            CK(allow_dyn_smem((const void *)k3_fft_fields_xy));
+            CK(allow_dyn_smem((const void *)k3_fft_fields_z<Z_TILE>));
             k3_fft_fields_xy<<<dim3(g.n3, nf), 256, smxy, E.st>>>(dsrc, ddst, g);
             E.launched();
             k3_fft_fields_z<Z_TILE><<<dim3(ntile, nf), 256, smz, E.st>>>(ddst, g);
@@ -1071,31 +1076,28 @@ struct AmRun {
     std::vector<AmState> st;
 };
 
-// Space-group projection of omega for the given instances, into dst slots
-// (dst[i] may alias nothing of omega); then copied back into omega.
-static void symmetrize_omega(Engine &E, const std::vector<int> &which, const std::vector<double *> &dst)
+// Space-group projection of omega for the given instances, in place.
+static void symmetrize_omega(Engine &E, const std::vector<int> &which)
 {
     std::vector<SymJob> jobs;
-    std::vector<std::pair<double *, double *>> back;
-    for (size_t k = 0; k < which.size(); k++) {
-        Inst &I = E.inst[which[k]];
+    int maxorb = 0;
+    for (int i : which) {
+        Inst &I = E.inst[i];
         if (I.nops <= 0) continue;
         SymJob j;
-        j.src = I.omega;
-        j.dst = dst[k];
-        j.ops = I.d_ops;
-        j.nops = I.nops;
+        j.f = I.omega;
+        j.perm = I.d_orb_perm;
+        j.start = I.d_orb_start;
+        j.norb = I.norb;
         j.M = E.M;
         jobs.push_back(j);
-        back.push_back({I.omega, dst[k]});
+        maxorb = std::max(maxorb, I.norb);
     }
     if (jobs.empty()) return;
     SymJob *dj = E.upload(jobs, E.geom_off + ((size_t)1 << 20));
-    dim3 grid((unsigned)std::min<long>((E.nr + 255) / 256, 512), (unsigned)jobs.size());
-    k_symmetrize<<<grid, 256, 0, E.st>>>(dj, E.n[0], E.n[1], E.n[2]);
+    dim3 grid((unsigned)std::max(1, std::min((maxorb + 127) / 128, 256)), (unsigned)jobs.size());
+    k_symmetrize<<<grid, 128, 0, E.st>>>(dj, E.nr);
     E.launched();
-    const long fl = (long)E.M * E.nr;
-    for (auto &b : back) CK(cudaMemcpyAsync(b.first, b.second, sizeof(double) * fl, cudaMemcpyDeviceToDevice, E.st));
 }
 
 static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
@@ -1117,13 +1119,9 @@ static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
     R.st.assign(ninst, AmState());
     for (auto &I : E.inst) I.prec_now = (E.prec == PSCFG_FP64) ? PSCFG_FP64 : PSCFG_FP32;
     std::vector<int> all(ninst);
-    std::vector<double *> scratch(ninst);
-    for (int i = 0; i < ninst; i++) {
-        all[i] = i;
-        scratch[i] = E.inst[i].om_hist;
-    }
+    for (int i = 0; i < ninst; i++) all[i] = i;
     // symmetric initial guess, then the first density (src/iterate_mod.fp.f90:1123)
-    symmetrize_omega(E, all, scratch);
+    symmetrize_omega(E, all);
     density_all(E, all);
     // uniform component of omega (set_omega_uniform, src/scf_mod.fp.f90:724-750)
     std::vector<double> w(fl);
@@ -1367,12 +1365,10 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
                 for (int b = 0; b < E.inst[i].cell.ncp; b++) s.cph[s.head][b] = E.inst[i].sys.cell_param[b];
             }
             // symmetric omega (the reference's star basis), recorded in the history
-            symmetrize_omega(E, mix_inst, slots);
-            for (size_t k = 0; k < mix_inst.size(); k++) {
-                Inst &I = E.inst[mix_inst[k]];
-                if (I.nops <= 0)
-                    CK(cudaMemcpyAsync(slots[k], I.omega, sizeof(double) * fl, cudaMemcpyDeviceToDevice, E.st));
-            }
+            symmetrize_omega(E, mix_inst);
+            for (size_t k = 0; k < mix_inst.size(); k++)
+                CK(cudaMemcpyAsync(slots[k], E.inst[mix_inst[k]].omega, sizeof(double) * fl,
+                                   cudaMemcpyDeviceToDevice, E.st));
             if (prm.domain) update_cells(E, mix_inst);
         }
         remaining = 0;
@@ -1631,17 +1627,17 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
         const int nf = (int)fl.size();
         if (E.dim <= 2) {
             size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)nr * sizeof(T);
-            CK(cudaFuncSetAttribute(k_sweep_plane<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
             int threads = (int)std::min<long>(256, std::max<long>(32, ((nr / 2 + 31) / 32) * 32));
             k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, 1);
             E.launched();
         } else if (!step3_fixed<T>(E, dfl, nf, 0)) {
             size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
             size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
-            CK(cudaFuncSetAttribute(k3_fwd_pair<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-            CK(cudaFuncSetAttribute(k3_inv_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-            CK(cudaFuncSetAttribute(k3_inv_final<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-            CK(cudaFuncSetAttribute(k3_zconv<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+            CK(allow_dyn_smem((const void *)k3_fwd_pair<T>));
+            CK(allow_dyn_smem((const void *)k3_inv_mid<T>));
+            CK(allow_dyn_smem((const void *)k3_inv_final<T>));
+            CK(allow_dyn_smem((const void *)k3_zconv<T, Z_TILE>));
             const long P = (long)g.n1h * g.n2;
             const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
             k3_fwd_pair<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
@@ -1747,17 +1743,17 @@ static void propagate_impl(Engine &E, int inst, const double *omega_m, double b,
         if (E.dim <= 2) {
             size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)E.nr * sizeof(T);
             if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
-            CK(cudaFuncSetAttribute(k_sweep_plane<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
             int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
             k_sweep_plane<T><<<1, threads, sm, E.st>>>(dfl, g, 0, nsteps);
             E.launched();
         } else {
             size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
             size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
-            CK(cudaFuncSetAttribute(k3_fwd_pair<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-            CK(cudaFuncSetAttribute(k3_inv_mid<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-            CK(cudaFuncSetAttribute(k3_inv_final<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-            CK(cudaFuncSetAttribute(k3_zconv<T, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+            CK(allow_dyn_smem((const void *)k3_fwd_pair<T>));
+            CK(allow_dyn_smem((const void *)k3_inv_mid<T>));
+            CK(allow_dyn_smem((const void *)k3_inv_final<T>));
+            CK(allow_dyn_smem((const void *)k3_zconv<T, Z_TILE>));
             const long P = (long)g.n1h * g.n2;
             const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
             for (int t = 0; t < nsteps; t++) {
@@ -2027,8 +2023,40 @@ int pscfg_set_symmetry(pscfg_engine *e, int inst, int nops, const int *ops)
     Inst &I = E.inst[inst];
     if (nops > 1024) throw Err(PSCFG_EINVAL, "too many group elements");
     if (nops > 0) {
-        I.d_ops = (int *)E.dalloc(sizeof(int) * 12 * nops);
-        CK(cudaMemcpyAsync(I.d_ops, ops, sizeof(int) * 12 * nops, cudaMemcpyHostToDevice, E.st));
+        // real-space orbits r -> M r + t (mod n), grouped for the projection
+        {
+            std::vector<int> perm, start, img(nops);
+            std::vector<char> seen_r(E.nr, 0);
+            perm.reserve(E.nr);
+            for (long r = 0; r < E.nr; r++) {
+                if (seen_r[r]) continue;
+                start.push_back((int)perm.size());
+                const int i[3] = {(int)(r % E.n[0]), (int)((r / E.n[0]) % E.n[1]), (int)(r / ((long)E.n[0] * E.n[1]))};
+                for (int k = 0; k < nops; k++) {
+                    const int *o = ops + 12 * k;
+                    long j[3];
+                    for (int a = 0; a < 3; a++) {
+                        long v = o[9 + a] + (long)o[3 * a] * i[0] + (long)o[3 * a + 1] * i[1] + (long)o[3 * a + 2] * i[2];
+                        v %= E.n[a];
+                        if (v < 0) v += E.n[a];
+                        j[a] = v;
+                    }
+                    const long rr = j[0] + (long)E.n[0] * (j[1] + (long)E.n[1] * j[2]);
+                    if (!seen_r[rr]) {
+                        seen_r[rr] = 1;
+                        perm.push_back((int)rr);
+                    }
+                }
+                if (!seen_r[r]) throw Err(PSCFG_EINVAL, "group elements do not include the identity");
+            }
+            start.push_back((int)perm.size());
+            if (!I.d_orb_perm) I.d_orb_perm = (int *)E.dalloc(sizeof(int) * E.nr);
+            if (!I.d_orb_start) I.d_orb_start = (int *)E.dalloc(sizeof(int) * (E.nr + 1));
+            I.norb = (int)start.size() - 1;
+            CK(cudaMemcpyAsync(I.d_orb_perm, perm.data(), sizeof(int) * E.nr, cudaMemcpyHostToDevice, E.st));
+            CK(cudaMemcpyAsync(I.d_orb_start, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, E.st));
+            CK(cudaStreamSynchronize(E.st));
+        }
         // Star weights: a star is the orbit of a wave G under the point
         // group (G -> G.m, src/group_mod.f90:77-78) on the FFT grid; the
         // reference normalises its star coefficients with a single-precision

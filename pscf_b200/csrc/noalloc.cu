@@ -25,6 +25,7 @@
 #include "../../include/pscf_gpu.h"
 #include "host_geom.h"
 #include "kernels.cuh"
+#include "launch_util.h"
 
 namespace pscfg {
 void set_global_error(const std::string &msg);   // engine.cu
@@ -213,13 +214,13 @@ extern "C" int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_
     const size_t smpl = smxy + 2 * (size_t)nr * sizeof(double);
     if (dim <= 2) {
         if (smpl > 227 * 1024) return fail(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
-        CKN(cudaFuncSetAttribute(k_sweep_plane<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smpl));
+        CKN(allow_dyn_smem((const void *)k_sweep_plane<double>));
     } else {
         if (smxy > 227 * 1024 || smz > 227 * 1024) return fail(PSCFG_EINVAL, "grid plane too large");
-        CKN(cudaFuncSetAttribute(k3_fwd_pair<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-        CKN(cudaFuncSetAttribute(k3_inv_mid<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-        CKN(cudaFuncSetAttribute(k3_inv_final<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smxy));
-        CKN(cudaFuncSetAttribute(k3_zconv<double, Z_TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz));
+        CKN(allow_dyn_smem((const void *)k3_fwd_pair<double>));
+        CKN(allow_dyn_smem((const void *)k3_inv_mid<double>));
+        CKN(allow_dyn_smem((const void *)k3_inv_final<double>));
+        CKN(allow_dyn_smem((const void *)k3_zconv<double, Z_TILE>));
     }
     const int threads = (int)std::min<long>(256, std::max<long>(32, ((nr / 2 + 31) / 32) * 32));
     for (int s = 0; s < nsteps; s++) {

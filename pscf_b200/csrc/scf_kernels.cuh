@@ -466,34 +466,29 @@ static __global__ void k_make_geom(const GeomJob *jobs, int dim, int n1, int n2,
 // ops: [nops][12] = 9 entries of M (row major) + 3 of t.
 // ---------------------------------------------------------------------
 struct SymJob {
-    const double *src;
-    double *dst;
-    const int *ops;
-    int nops;
+    double *f;              // [M][nr], projected in place
+    const int *perm;        // grid points grouped by orbit
+    const int *start;       // orbit o = perm[start[o] .. start[o+1])
+    int norb;
     int M;
 };
 
-static __global__ void k_symmetrize(const SymJob *jobs, int n1, int n2, int n3)
+// Space-group projection f <- (1/|G|) sum_g f(g r) as the orbit mean: a
+// point's images under the group cover its orbit |G|/|orbit| times each.
+// One thread per orbit reads and rewrites all of its points.
+static __global__ void k_symmetrize(const SymJob *jobs, long nr)
 {
     const SymJob &J = jobs[blockIdx.y];
-    const long nr = (long)n1 * n2 * n3;
-    const int n[3] = {n1, n2, n3};
-    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += (long)gridDim.x * blockDim.x) {
-        const int i[3] = {(int)(r % n1), (int)((r / n1) % n2), (int)(r / ((long)n1 * n2))};
-        double acc[PSCFG_MAXM] = {0.0, 0.0, 0.0, 0.0};
-        for (int k = 0; k < J.nops; k++) {
-            const int *o = J.ops + 12 * k;
-            int j[3];
-            for (int a = 0; a < 3; a++) {
-                int v = o[9 + a] + o[3 * a] * i[0] + o[3 * a + 1] * i[1] + o[3 * a + 2] * i[2];
-                v %= n[a];
-                if (v < 0) v += n[a];
-                j[a] = v;
-            }
-            const long rr = j[0] + (long)n1 * (j[1] + (long)n2 * j[2]);
-            for (int a = 0; a < J.M; a++) acc[a] += J.src[(long)a * nr + rr];
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < J.norb; o += gridDim.x * blockDim.x) {
+        const int b = J.start[o], e = J.start[o + 1];
+        const double inv = 1.0 / (double)(e - b);
+        for (int a = 0; a < J.M; a++) {
+            double *f = J.f + (long)a * nr;
+            double acc = 0.0;
+            for (int k = b; k < e; k++) acc += f[J.perm[k]];
+            acc *= inv;
+            for (int k = b; k < e; k++) f[J.perm[k]] = acc;
         }
-        for (int a = 0; a < J.M; a++) J.dst[(long)a * nr + r] = acc[a] / (double)J.nops;
     }
 }
 

@@ -111,6 +111,29 @@ def test_density_fp32_close():
     assert rel_err(q[0, :1], q_ref) < 2e-5
 
 
+def test_cluster_step_matches_five_launch_step(monkeypatch):
+    """The one-launch cluster step (32^3) agrees with the five-launch
+    compile-time-shaped step, for propagation, the full density and the
+    adjoint (which stores the step intermediates)."""
+    s = diblock(3, [32, 32, 32], "cubic", [1.95], fA=0.3, ds=0.05)
+    w = 7.5 + smooth_field(s, 5, 3.0)
+    q0 = 1.0 + 0.3 * smooth_field(s, 6, 1.0)
+    wf = omega_guess(s, 8, 2.0)
+    g = smooth_field(s, 9, 1.0)
+    grad = np.stack([g, -0.5 * g])[None]
+    out = []
+    for flag in ("0", "1"):
+        monkeypatch.setenv("PSCFG_CLUSTER_STEP", flag)
+        e = Engine([s], FP64)
+        a = e.propagate(0, w, 1.0, 0.01, q0, 3)
+        r, q = e.density(wf[None])
+        gw = e.density_adjoint(grad)
+        out.append((a, r, q[:, :1], gw))
+        e.close()
+    for x, y in zip(out[0], out[1]):
+        assert rel_err(x, y) < 1e-13
+
+
 @pytest.mark.parametrize("n", [16, 32, 64])
 def test_fixed_shape_kernels_match_generic(n, monkeypatch):
     """The compile-time-shaped 3-D step kernels agree with the run-time sized
@@ -158,3 +181,34 @@ def test_solvent_and_ensemble_parity(ensemble):
     f, p, mu = e.free_energy()
     assert abs(f[0] - f_ref) < 1e-11 and abs(p[0] - p_ref) < 1e-11
     np.testing.assert_allclose(mu[0, :2], mu_ref, rtol=1e-12)
+
+
+def test_concurrent_engines_with_different_plane_sizes():
+    """Engines of different grid shapes driven from separate host threads
+    (small lamellar and large hexagonal plane kernels launched together)
+    give the same densities as when run alone."""
+    import threading
+    lam = diblock(1, [64], "lamellar", [1.7], fA=0.4, ds=0.02)
+    hexs = diblock(2, [64, 64], "hexagonal", [1.9], fA=0.3, ds=0.02)
+    wl, wh = omega_guess(lam, 1, 2.0), omega_guess(hexs, 2, 2.0)
+    ref = [Engine([lam], FP64).density(wl[None])[0], Engine([hexs], FP64).density(wh[None])[0]]
+    engines = [Engine([lam], FP64), Engine([hexs], FP64)]
+    outs = [[], []]
+    errs = []
+
+    def run(k, w):
+        try:
+            for _ in range(40):
+                outs[k].append(engines[k].density(w[None])[0])
+        except Exception as ex:      # surfaced below
+            errs.append(ex)
+
+    th = [threading.Thread(target=run, args=(0, wl)), threading.Thread(target=run, args=(1, wh))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for k in range(2):
+        for r in outs[k]:
+            assert rel_err(r, ref[k]) < 1e-14
