@@ -97,7 +97,9 @@ typedef struct pscfg_am_param {
     int n_hist;
     int domain;              /* 1: relax the unit cell (stress -> 0) */
     double error_max;
-    double switch_error;     /* PSCFG_MIXED: FP32 -> FP64 below this error (0: 1e-5) */
+    double switch_error;     /* PSCFG_MIXED: FP32 -> FP64 below this error (0: 1e-3), on
+                                stagnation within 1000x of it, when the error rises to 10x the
+                                best FP32 error, or after 500 FP32 iterations */
 } pscfg_am_param;
 
 /* Per-instance result of pscfg_iterate_am. */
@@ -176,6 +178,26 @@ int pscfg_iterate_am(pscfg_engine *e, double *omega, const pscfg_am_param *prm, 
 int pscfg_density_adjoint(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega);
 int pscfg_density_adjoint_device(pscfg_engine *e, const double *grad_rho_dev, const double *grad_lnq,
                                  double *grad_omega_dev);
+
+/* Ideal-gas linear response of instance `inst` to Bloch perturbations
+ * (replaces drho_domega_id's loop over perturbations, calc_q0 / calc_delq /
+ * calc_delrho, src/response_mod.f90:389-468, 697-1186, with the steps of
+ * src/response_step_mod.f90:114-219 at the order the reference uses, 1).
+ * Perturbation p adds exp(i k.r) W_p(r) to the field of monomer
+ * pert_monomer[p]; W_p is given on the grid (pert_field: host
+ * [n_pert][nr][2], re/im interleaved; the reference builds it from one
+ * basis function, calc_perturb_field :1275-1291).  kvec: k in units of
+ * the reciprocal basis vectors (3 entries, those beyond dim ignored);
+ * ktrans_sq is added to every |G+k|^2 (calc_ksqgrid_new :1203-1238).
+ * For every perturbation and monomer m the periodic part of the density
+ * response is transformed (fftc(+1), /N) and read at n_read waves:
+ * out[p][m][j] = Re(FFT(drho_m)[read_index[j]] / read_coef[j])
+ * (kgrid_to_basis with no_parity, src/grid_basis_mod.f90:146-200);
+ * read_coef: [n_read][2].  Uses the propagators of the preceding
+ * pscfg_density call (FP64).  Host arrays. */
+int pscfg_response(pscfg_engine *e, int inst, const double *kvec, double ktrans_sq, int n_pert,
+                   const int *pert_monomer, const double *pert_field, int n_read, const int *read_index,
+                   const double *read_coef, double *out);
 
 /* Stepwise form of pscfg_iterate_am for callers that interleave their own
  * work or time single iterations: pscfg_am_begin loads omega (host, or

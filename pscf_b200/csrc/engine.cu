@@ -31,6 +31,7 @@
 #include "kernels3c.cuh"
 #include "adjoint.cuh"
 #include "kernels3x.cuh"
+#include "response.cuh"
 
 namespace pscfg {
 
@@ -73,6 +74,7 @@ struct Inst {
     double *stress_dev = nullptr; // [MAXCP]
     double Q[PSCFG_MAXC] = {}, Qs[PSCFG_MAXS] = {};
     bool have_density = false;
+    int dens_prec = PSCFG_FP64;   // precision of the stored propagators
     int prec_now = PSCFG_FP64;    // propagation precision of the next density call
     // Anderson
     double *om_hist = nullptr, *dev_hist = nullptr;
@@ -731,6 +733,7 @@ static void density_all(Engine &E, const std::vector<int> &act)
     for (int i : act) {
         Inst &I = E.inst[i];
         I.have_density = true;
+        I.dens_prec = I.prec_now;
         // mu_phi_chain / mu_phi_solvent (src/scf_mod.fp.f90:768-820)
         for (int c = 0; c < I.sys.n_chain; c++) {
             if (I.sys.ensemble == 0) I.sys.mu_chain[c] = std::log(I.sys.phi_chain[c] / I.Q[c]);
@@ -1279,17 +1282,21 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
             s.error = std::max(e1, e2);
             s.nstore = nst;
             // mixed precision: an FP32 iteration never counts as converged; the
-            // instance moves to FP64 once its error is below the switch error
-            // or has not improved by 10% for 10 iterations
+            // instance moves to FP64 once its error is below the switch error,
+            // or once it is within 1000x of it and has not improved by 10% for
+            // 10 iterations (the FP32 noise floor), or as soon as its error
+            // rises to 10x the best FP32 error (an FP32 run drifting away), or
+            // after 500 FP32 iterations
             const bool was32 = I.prec_now == PSCFG_FP32;
             if (was32) {
                 s.itr_fp32++;
-                const double sw = prm.switch_error > 0 ? prm.switch_error : 1e-5;
-                bool go = s.error < sw || s.error < prm.error_max;
+                const double sw = prm.switch_error > 0 ? prm.switch_error : 1e-3;
+                bool go = s.error < sw || s.error < prm.error_max || s.itr_fp32 >= 500 ||
+                          !(s.error <= 10.0 * s.best);
                 if (s.error < 0.9 * s.best) {
                     s.best = s.error;
                     s.since_best = 0;
-                } else if (++s.since_best >= 10) {
+                } else if (++s.since_best >= 10 && s.error < 1e3 * sw) {
                     go = true;
                 }
                 if (go && E.prec == PSCFG_MIXED) I.prec_now = PSCFG_FP64;
@@ -1438,6 +1445,41 @@ static int seg_block(const Inst &I, int c, int j)   // block of the segment (j, 
     int b = 0;
     while (b < I.sys.n_block[c] - 1 && j >= I.bgn[c][b + 1]) b++;
     return b;
+}
+
+// One step of every field in dfl (fields with ns = 1 and in/out overrides),
+// on whichever step kernels the grid has.
+template <typename T>
+static void run_single_steps(Engine &E, const SweepField<T> *dfl, int nf)
+{
+    const PlaneGeom &g = E.geom();
+    const long nr = E.nr;
+    if (E.dim <= 2) {
+        size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)nr * sizeof(T);
+        CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
+        int threads = (int)std::min<long>(256, std::max<long>(32, ((nr / 2 + 31) / 32) * 32));
+        k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, 1);
+        E.launched();
+    } else if (!step3_fixed<T>(E, dfl, nf, 0)) {
+        size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
+        size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
+        CK(allow_dyn_smem((const void *)k3_fwd_pair<T>));
+        CK(allow_dyn_smem((const void *)k3_inv_mid<T>));
+        CK(allow_dyn_smem((const void *)k3_inv_final<T>));
+        CK(allow_dyn_smem((const void *)k3_zconv<T, Z_TILE>));
+        const long P = (long)g.n1h * g.n2;
+        const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+        k3_fwd_pair<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
+        E.launched();
+        k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 2), 256, smz, E.st>>>(dfl, g, 0, 3);
+        E.launched();
+        k3_inv_mid<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
+        E.launched();
+        k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 1), 256, smz, E.st>>>(dfl, g, 0, 2);
+        E.launched();
+        k3_inv_final<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
+        E.launched();
+    }
 }
 
 template <typename T>
@@ -1624,33 +1666,7 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
         SweepField<T> *dfl = E.upload(fl, 0);
         size_t o2 = ((fl.size() * sizeof(SweepField<T>) + 255) / 256) * 256;
         AdjPoint *dpt = E.upload(pts, o2);
-        const int nf = (int)fl.size();
-        if (E.dim <= 2) {
-            size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)nr * sizeof(T);
-            CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
-            int threads = (int)std::min<long>(256, std::max<long>(32, ((nr / 2 + 31) / 32) * 32));
-            k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, 1);
-            E.launched();
-        } else if (!step3_fixed<T>(E, dfl, nf, 0)) {
-            size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
-            size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
-            CK(allow_dyn_smem((const void *)k3_fwd_pair<T>));
-            CK(allow_dyn_smem((const void *)k3_inv_mid<T>));
-            CK(allow_dyn_smem((const void *)k3_inv_final<T>));
-            CK(allow_dyn_smem((const void *)k3_zconv<T, Z_TILE>));
-            const long P = (long)g.n1h * g.n2;
-            const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
-            k3_fwd_pair<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
-            E.launched();
-            k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 2), 256, smz, E.st>>>(dfl, g, 0, 3);
-            E.launched();
-            k3_inv_mid<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
-            E.launched();
-            k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 1), 256, smz, E.st>>>(dfl, g, 0, 2);
-            E.launched();
-            k3_inv_final<T><<<dim3(g.n3, nf), 256, smxy, E.st>>>(dfl, g, 0);
-            E.launched();
-        }
+        run_single_steps<T>(E, dfl, (int)fl.size());
         k_adj_point<T><<<dim3((unsigned)std::min<long>((nr + 255) / 256, 256), (unsigned)pts.size()), 256, 0, E.st>>>(dpt, nr);
         E.launched();
     }
@@ -1677,6 +1693,364 @@ static void adjoint_all(Engine &E, const std::vector<int> &act, const std::vecto
     if (!a32.empty()) throw Err(PSCFG_EINVAL, "the adjoint runs on FP64 propagators (use PSCFG_FP64 or PSCFG_MIXED)");
     E.cur = PSCFG_FP64;
     adjoint_impl<double>(E, act, G, gQ, grad);
+}
+
+// ---------------------------------------------------------------------
+// Linear response of a periodic state (RESPONSE, src/response_mod.f90)
+// ---------------------------------------------------------------------
+// Device buffers owned by one call.
+struct CallScratch {
+    std::vector<void *> p;
+    void *get(size_t bytes)
+    {
+        void *d = nullptr;
+        cudaError_t e = cudaMalloc(&d, std::max(bytes, (size_t)16));
+        if (e != cudaSuccess) throw Err(PSCFG_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+        p.push_back(d);
+        return d;
+    }
+    ~CallScratch()
+    {
+        for (void *d : p) cudaFree(d);
+    }
+};
+
+// Line passes of one complex transform of every job (k_cline).  step: the
+// fftc_step E IFFT[K FFT[E x]]; otherwise the forward transform / N.
+static void run_cpasses(Engine &E, const CJob *djobs, int njobs, bool step, const LinePlan plans[3])
+{
+    const int dim = E.dim;
+    std::vector<CPass> passes;
+    auto mk_pass = [&](int a) {
+        CPass P;
+        std::memset(&P, 0, sizeof(P));
+        P.axis = a;
+        P.L = E.n[a];
+        P.nl = (int)(E.nr / P.L);
+        P.TL = std::max(1, std::min(32, 2048 / P.L));
+        P.TL = std::min(P.TL, P.nl);
+        P.plan = plans[a];
+        return P;
+    };
+    for (int a = 0; a < dim; a++) {
+        CPass P = mk_pass(a);
+        P.fwd = 1;
+        if (a == 0) P.first = 1;
+        if (a == dim - 1) {
+            P.kmul = 1;
+            if (step) P.inv = 1;
+        }
+        passes.push_back(P);
+    }
+    if (step) {
+        for (int a = dim - 2; a >= 0; a--) {
+            CPass P = mk_pass(a);
+            P.inv = 1;
+            passes.push_back(P);
+        }
+        passes.back().last = 1;
+    }
+    CK(allow_dyn_smem((const void *)k_cline));
+    const double inv_n = 1.0 / (double)E.nr;
+    for (const CPass &P : passes) {
+        const size_t sm = 2 * sizeof(cx<double>) * (size_t)P.TL * P.L;
+        const unsigned gx = (unsigned)((P.nl + P.TL - 1) / P.TL);
+        for (int j0 = 0; j0 < njobs; j0 += 65535) {
+            const int nj = std::min(65535, njobs - j0);
+            k_cline<<<dim3(gx, nj), 128, sm, E.st>>>(djobs + j0, P, E.n[0], E.n[1], inv_n);
+            E.launched();
+        }
+    }
+}
+
+static void response_impl(Engine &E, int inst, const double kvec[3], double ktrans_sq, int n_pert,
+                          const int *pert_monomer, const double *pert_field, int n_read, const int *read_index,
+                          const double *read_coef, double *out)
+{
+    Inst &I = E.inst[inst];
+    if (!I.have_density) throw Err(PSCFG_ESTATE, "the response requires a preceding density call");
+    if (E.prec == PSCFG_FP32 || I.dens_prec != PSCFG_FP64)
+        throw Err(PSCFG_EINVAL, "the response runs on FP64 propagators");
+    for (int p = 0; p < n_pert; p++)
+        if (pert_monomer[p] < 0 || pert_monomer[p] >= E.M) throw Err(PSCFG_EINVAL, "perturbed monomer out of range");
+    for (int k = 0; k < n_read; k++)
+        if (read_index[k] < 0 || read_index[k] >= E.nr) throw Err(PSCFG_EINVAL, "readout index out of range");
+    E.cur = PSCFG_FP64;
+    const long nr = E.nr, nk = E.nk;
+    const int M = E.M, nch = I.sys.n_chain;
+    const PlaneGeom &g = E.g64;
+    CallScratch cs;
+    E.desc((size_t)64 << 20);
+    const unsigned ngrid = (unsigned)std::min<long>((nr + 255) / 256, 1024);
+
+    // 1. unperturbed step intermediates of every step of both sweeps
+    //    (calc_q0): P1 q (chains0 order 0), the half-step midpoint and
+    //    P2 q (chains0 order 1), from the stored propagators
+    struct Inter { double *q1, *h, *q2; };
+    Inter it[PSCFG_MAXC][2];
+    for (int c = 0; c < nch; c++) {
+        const int ns = I.ns[c];
+        for (int d = 0; d < 2; d++) {
+            it[c][d].q1 = (double *)cs.get(sizeof(double) * nr * (ns + 1));
+            it[c][d].h = (double *)cs.get(sizeof(double) * nr * (ns + 1));
+            it[c][d].q2 = (double *)cs.get(sizeof(double) * nr * (ns + 1));
+        }
+    }
+    {
+        const int FCH = 64;
+        double *dummy = (double *)cs.get(sizeof(double) * nr * FCH);
+        cx<double> *S12 = E.dim == 3 ? (cx<double> *)cs.get(sizeof(cx<double>) * nk * 2 * FCH) : nullptr;
+        std::vector<SweepField<double>> fl;
+        std::vector<CDiv> dv;
+        auto flush = [&]() {
+            if (fl.empty()) return;
+            SweepField<double> *dfl = E.upload(fl, 0);
+            run_single_steps<double>(E, dfl, (int)fl.size());
+            CDiv *ddv = E.upload(dv, (size_t)4 << 20);
+            k_resp_div<<<dim3(ngrid, (unsigned)dv.size()), 256, 0, E.st>>>(ddv, nr);
+            E.launched();
+            fl.clear();
+            dv.clear();
+        };
+        for (int c = 0; c < nch; c++) {
+            const int ns = I.ns[c];
+            for (int d = 0; d < 2; d++)
+                for (int j = (d == 0 ? 1 : 0); j <= (d == 0 ? ns : ns - 1); j++) {
+                    const int blk = seg_block(I, c, d == 0 ? j - 1 : j);
+                    const int slot = (int)fl.size();
+                    SweepField<double> F;
+                    std::memset(&F, 0, sizeof(F));
+                    F.slab = dummy + (long)slot * nr;
+                    F.ns = 1;
+                    F.dir = 1;
+                    F.nblk = 1;
+                    F.bgn[0] = 0;
+                    F.bgn[1] = 1;
+                    F.eo1[0] = (const double *)I.eo1[c][blk];
+                    F.eo2[0] = (const double *)I.eo2[c][blk];
+                    F.ek1[0] = (const double *)I.ek1[c][blk];
+                    F.ek2[0] = (const double *)I.ek2[c][blk];
+                    if (S12) {
+                        F.S1 = S12 + (long)(2 * slot) * nk;
+                        F.S2 = S12 + (long)(2 * slot + 1) * nk;
+                    }
+                    F.in = d == 0 ? (const double *)I.qf[c] + (long)(j - 1) * nr
+                                  : (const double *)I.qr[c] + (long)(j + 1) * nr;
+                    F.out = dummy + (long)slot * nr;
+                    F.q1 = it[c][d].q1 + (long)j * nr;
+                    F.h_out = it[c][d].h + (long)j * nr;
+                    F.q2_out = it[c][d].q2 + (long)j * nr;
+                    fl.push_back(F);
+                    CDiv v;
+                    v.x = it[c][d].h + (long)j * nr;
+                    v.d = (const double *)I.eo2[c][blk];
+                    dv.push_back(v);
+                    if ((int)fl.size() == FCH) flush();
+                }
+        }
+        flush();
+    }
+
+    // 2. |G+k|^2 and the exp tables of levels ds, ds/2, ds/4 per block
+    std::vector<double> kq;
+    ksq_bloch(E.dim, E.n, I.cell.G, kvec, ktrans_sq, kq);
+    double *ksq_new = (double *)cs.get(sizeof(double) * nr);
+    CK(cudaMemcpyAsync(ksq_new, kq.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, E.st));
+    const double *Et[PSCFG_MAXC][PSCFG_MAXB][3], *Kt[PSCFG_MAXC][PSCFG_MAXB][3];
+    {
+        std::vector<CTab> tj;
+        for (int c = 0; c < nch; c++)
+            for (int b = 0; b < I.sys.n_block[c]; b++) {
+                const int m = I.sys.block_monomer[c][b];
+                double dsl = I.bds[c][b];
+                for (int l = 0; l < 3; l++) {
+                    CTab t;
+                    t.w = I.omega + (long)m * nr;
+                    t.ksq = ksq_new;
+                    t.E = (double *)cs.get(sizeof(double) * nr);
+                    t.K = (double *)cs.get(sizeof(double) * nr);
+                    t.ds = dsl;
+                    t.b2 = I.sys.kuhn[m] * I.sys.kuhn[m];
+                    Et[c][b][l] = t.E;
+                    Kt[c][b][l] = t.K;
+                    tj.push_back(t);
+                    dsl /= 2.0;
+                }
+            }
+        CTab *dtj = E.upload(tj, 0);
+        k_resp_tables<<<dim3(ngrid, (unsigned)tj.size()), 256, 0, E.st>>>(dtj, nr);
+        E.launched();
+    }
+    // Simpson coefficients per slice and monomer, times phi/(N Q)
+    // (calc_delrho, src/response_mod.f90:1107-1182)
+    std::vector<double> coef[PSCFG_MAXC];
+    for (int c = 0; c < nch; c++) {
+        simpson_weights(I, c, coef[c]);
+        const double f = I.sys.phi_chain[c] / (I.length[c] * I.Q[c]);
+        for (auto &x : coef[c]) x *= f;
+    }
+    LinePlan plans[3] = {g.row, g.col, g.zp};
+    plans[0].n = E.n[0];
+    if (!plan_radices(E.n[0], plans[0].rad, plans[0].nst)) throw Err(PSCFG_EINVAL, "grid size not supported");
+    plans[0].tw = g.rtw;
+
+    // 3. perturbations in chunks bounded by memory
+    const int nsd = 2 * nch;                       // sweeps per perturbation
+    const size_t per = sizeof(cx<double>) * nr * ((size_t)nsd * (7 + M) + 1 + M);
+    size_t fr = 0, tot = 0;
+    CK(cudaMemGetInfo(&fr, &tot));
+    const size_t budget = std::min((size_t)8 << 30, fr / 4);
+    // the job descriptors of one segment must fit the pre-grown descriptor
+    // scratch (an upload that grew it would free descriptors already queued)
+    const size_t per_desc = (size_t)nsd * (6 * sizeof(CJob) + sizeof(CCombine)) + 2 * M * sizeof(CJob) + 256;
+    const size_t desc_cap = ((size_t)48 << 20) / per_desc;
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(std::min<size_t>((size_t)n_pert, budget / per), desc_cap));
+    double *dout = (double *)cs.get(sizeof(double) * (size_t)chunk * M * std::max(n_read, 1));
+    int *didx = (int *)cs.get(sizeof(int) * std::max(n_read, 1));
+    double *dcoef = (double *)cs.get(sizeof(double) * 2 * std::max(n_read, 1));
+    if (n_read > 0) {
+        CK(cudaMemcpyAsync(didx, read_index, sizeof(int) * n_read, cudaMemcpyHostToDevice, E.st));
+        CK(cudaMemcpyAsync(dcoef, read_coef, sizeof(double) * 2 * n_read, cudaMemcpyHostToDevice, E.st));
+    }
+    cx<double> *W = (cx<double> *)cs.get(sizeof(cx<double>) * nr * chunk);
+    cx<double> *state = (cx<double> *)cs.get(sizeof(cx<double>) * nr * (size_t)chunk * nsd * (7 + M));
+    cx<double> *drho = (cx<double> *)cs.get(sizeof(cx<double>) * nr * (size_t)chunk * M);
+    int ns_max = 0;
+    for (int c = 0; c < nch; c++) ns_max = std::max(ns_max, I.ns[c]);
+
+    for (int p0 = 0; p0 < n_pert; p0 += chunk) {
+        const int np = std::min(chunk, n_pert - p0);
+        CK(cudaMemcpyAsync(W, pert_field + (size_t)p0 * 2 * nr, sizeof(cx<double>) * nr * np, cudaMemcpyHostToDevice,
+                           E.st));
+        CK(cudaMemsetAsync(state, 0, sizeof(cx<double>) * nr * (size_t)np * nsd * (7 + M), E.st));
+        auto buf = [&](int p, int sd, int k) { return state + nr * (((size_t)p * nsd + sd) * (7 + M) + k); };
+        for (int t = 0; t < ns_max; t++) {
+            std::vector<CJob> ja, jb;
+            std::vector<CCombine> cb;
+            for (int p = 0; p < np; p++) {
+                const int pm = pert_monomer[p0 + p];
+                for (int c = 0; c < nch; c++) {
+                    const int ns = I.ns[c], nblk = I.sys.n_block[c];
+                    if (t >= ns) continue;
+                    for (int d = 0; d < 2; d++) {
+                        const int sd = 2 * c + d;
+                        const int jn = d == 0 ? t + 1 : ns - 1 - t;          // new node
+                        const int jp = d == 0 ? t : ns - t;                  // previous node
+                        const int blk = seg_block(I, c, d == 0 ? t : jn);
+                        const int m = I.sys.block_monomer[c][blk];
+                        const bool src = m == pm;
+                        // no source yet: the perturbed propagator is still zero
+                        if (!src && ((d == 0 && blk == 0) || (d == 1 && blk == nblk - 1))) continue;
+                        const double ds = I.bds[c][blk];
+                        const double *qprev = (const double *)(d == 0 ? I.qf[c] : I.qr[c]) + (long)jp * nr;
+                        const double *q1e = it[c][d].q1 + (long)jn * nr;
+                        const double *hm = it[c][d].h + (long)jn * nr;
+                        const double *q2e = it[c][d].q2 + (long)jn * nr;
+                        cx<double> *dq = buf(p, sd, 0), *A1 = buf(p, sd, 1), *A2 = buf(p, sd, 2), *A3 = buf(p, sd, 3);
+                        cx<double> *A4 = buf(p, sd, 4), *A5 = buf(p, sd, 5), *B = buf(p, sd, 6);
+                        cx<double> *acc = buf(p, sd, 7);
+                        const cx<double> *Wp = W + (long)p * nr;
+                        auto job = [&](const cx<double> *a, const cx<double> *bb, double cbv, const double *qa,
+                                       const double *qb, int l, cx<double> *o) {
+                            CJob J;
+                            std::memset(&J, 0, sizeof(J));
+                            J.A = a;
+                            J.ca = 1.0;
+                            J.B = bb;
+                            J.cb = cbv;
+                            if (qa) {
+                                J.W = Wp;
+                                J.cw = 1.0;
+                                J.qa = qa;
+                                J.qb = qb;
+                            }
+                            J.E = Et[c][blk][l];
+                            J.K = Kt[c][blk][l];
+                            J.out = o;
+                            return J;
+                        };
+                        // ps_propagate order 0 and order 1 (src/response_step_mod.f90:135-151)
+                        ja.push_back(job(dq, nullptr, 0.0, nullptr, nullptr, 0, A1));
+                        ja.push_back(job(dq, nullptr, 0.0, nullptr, nullptr, 1, A3));
+                        if (src) {
+                            ja.push_back(job(nullptr, nullptr, 0.0, qprev, q1e, 1, A2));
+                            ja.push_back(job(nullptr, nullptr, 0.0, qprev, hm, 2, A4));
+                            ja.push_back(job(nullptr, nullptr, 0.0, hm, q2e, 2, A5));
+                        }
+                        jb.push_back(job(A3, src ? A4 : nullptr, -ds / 2.0, nullptr, nullptr, 1, B));
+                        CCombine k;
+                        std::memset(&k, 0, sizeof(k));
+                        k.dq = dq;
+                        k.A1 = A1;
+                        k.A2 = src ? A2 : nullptr;
+                        k.A5 = src ? A5 : nullptr;
+                        k.B = B;
+                        k.ds = ds;
+                        k.other = (const double *)(d == 0 ? I.qr[c] : I.qf[c]) + (long)jn * nr;
+                        k.acc = acc;
+                        for (int mm = 0; mm < M; mm++) k.coef[mm] = coef[c][(size_t)jn * PSCFG_MAXM + mm];
+                        k.M = M;
+                        cb.push_back(k);
+                    }
+                }
+            }
+            if (cb.empty()) continue;
+            size_t off = 0;
+            const CJob *dja = E.upload(ja, off);
+            off += ((ja.size() * sizeof(CJob) + 255) / 256) * 256;
+            const CJob *djb = E.upload(jb, off);
+            off += ((jb.size() * sizeof(CJob) + 255) / 256) * 256;
+            const CCombine *dcb = E.upload(cb, off);
+            run_cpasses(E, dja, (int)ja.size(), true, plans);
+            run_cpasses(E, djb, (int)jb.size(), true, plans);
+            for (size_t j0 = 0; j0 < cb.size(); j0 += 65535) {
+                const unsigned nj = (unsigned)std::min<size_t>(65535, cb.size() - j0);
+                k_resp_combine<<<dim3(ngrid, nj), 256, 0, E.st>>>(dcb + j0, nr);
+                E.launched();
+            }
+        }
+        // 4. drho of every perturbation: sum over sweeps, forward transform / N,
+        //    basis readout (kgrid_to_basis with no_parity)
+        std::vector<CSum> sums;
+        for (int p = 0; p < np; p++)
+            for (int mm = 0; mm < M; mm++) {
+                CSum sj;
+                std::memset(&sj, 0, sizeof(sj));
+                sj.dst = drho + nr * ((size_t)p * M + mm);
+                for (int sd = 0; sd < nsd; sd++) sj.src[sj.n++] = buf(p, sd, 7) + (long)mm * nr;
+                sums.push_back(sj);
+            }
+        const CSum *dsm = E.upload(sums, 0);
+        k_csum<<<dim3(ngrid, (unsigned)sums.size()), 256, 0, E.st>>>(dsm, nr);
+        E.launched();
+        std::vector<CJob> fj;
+        std::vector<CRead> rd;
+        for (int q = 0; q < np * M; q++) {
+            CJob J;
+            std::memset(&J, 0, sizeof(J));
+            J.A = drho + nr * (size_t)q;
+            J.ca = 1.0;
+            J.out = drho + nr * (size_t)q;
+            fj.push_back(J);
+            CRead r;
+            r.spec = drho + nr * (size_t)q;
+            r.out = dout + (size_t)q * std::max(n_read, 1);
+            rd.push_back(r);
+        }
+        size_t off = ((sums.size() * sizeof(CSum) + 255) / 256) * 256;
+        const CJob *dfj = E.upload(fj, off);
+        off += ((fj.size() * sizeof(CJob) + 255) / 256) * 256;
+        const CRead *drd = E.upload(rd, off);
+        run_cpasses(E, dfj, (int)fj.size(), false, plans);
+        if (n_read > 0) {
+            k_resp_readout<<<dim3((unsigned)std::min(1024, (n_read + 127) / 128), (unsigned)rd.size()), 128, 0, E.st>>>(
+                drd, didx, dcoef, n_read);
+            E.launched();
+            CK(cudaMemcpyAsync(out + (size_t)p0 * M * n_read, dout, sizeof(double) * (size_t)np * M * n_read,
+                               cudaMemcpyDeviceToHost, E.st));
+        }
+        CK(cudaStreamSynchronize(E.st));
+    }
 }
 
 // ---------------------------------------------------------------------
@@ -2153,6 +2527,21 @@ int pscfg_density_adjoint_device(pscfg_engine *e, const double *grad_rho_dev, co
                                  double *grad_omega_dev)
 {
     return adjoint_common(e, grad_rho_dev, grad_lnq, grad_omega_dev, true);
+}
+
+int pscfg_response(pscfg_engine *e, int inst, const double *kvec, double ktrans_sq, int n_pert,
+                   const int *pert_monomer, const double *pert_field, int n_read, const int *read_index,
+                   const double *read_coef, double *out)
+{
+    if (!e || !kvec || n_pert < 0 || n_read < 0 || (n_pert > 0 && (!pert_monomer || !pert_field)) ||
+        (n_read > 0 && (!read_index || !read_coef || !out)))
+        return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    if (inst < 0 || inst >= (int)E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
+    if (n_pert > 0) response_impl(E, inst, kvec, ktrans_sq, n_pert, pert_monomer, pert_field, n_read, read_index,
+                                  read_coef, out);
+    ABI_END(e)
 }
 
 int pscfg_set_profiling(pscfg_engine *e, int on)

@@ -149,6 +149,37 @@ inline void g_to_bz(int dim, const int n[3], const double Gb[3][3], const int G[
     out[2] = Gmin[2];
 }
 
+// |G + k|^2 on the full grid for a Bloch wave vector k in reciprocal-basis
+// units (calc_ksqgrid_new, src/response_mod.f90:1203-1238): every grid index
+// shifted by k is folded by Greal_to_bz (src/grid_mod.f90:286-345, images
+// +1, 0, -1 per used dimension, a later image wins only if shorter by more
+// than 1e-8); components beyond dim are dropped and ktrans_sq is added.
+inline void ksq_bloch(int dim, const int n[3], const double Gb[3][3], const double kvec[3], double ktrans_sq,
+                      std::vector<double> &out)
+{
+    out.assign((size_t)n[0] * n[1] * n[2], 0.0);
+    int hi[3] = {0, 0, 0};
+    for (int d = 0; d < dim; d++) hi[d] = 1;
+    for (int i3 = 0; i3 < n[2]; i3++)
+        for (int i2 = 0; i2 < n[1]; i2++)
+            for (int i1 = 0; i1 < n[0]; i1++) {
+                const double g[3] = {i1 + kvec[0], i2 + kvec[1], i3 + kvec[2]};
+                double best = 1.0e10;
+                for (int s1 = hi[0]; s1 >= -hi[0]; s1--)
+                    for (int s2 = hi[1]; s2 >= -hi[1]; s2--)
+                        for (int s3 = hi[2]; s3 >= -hi[2]; s3--) {
+                            const double t[3] = {g[0] + s1 * n[0], g[1] + s2 * n[1], g[2] + s3 * n[2]};
+                            double v[3] = {0, 0, 0};
+                            for (int j = 0; j < dim; j++)
+                                for (int i = 0; i < dim; i++) v[j] += t[i] * Gb[i][j];
+                            double q = 0;
+                            for (int j = 0; j < dim; j++) q += v[j] * v[j];
+                            if (q < best - 1.0e-8) best = q;
+                        }
+                out[i1 + (size_t)n[0] * (i2 + (size_t)n[1] * i3)] = best + ktrans_sq;
+            }
+}
+
 // k^2 on the half grid (make_ksq, src/grid_mod.f90:141-160) and the stress
 // weights w(k) * Gbz^T dGG_b Gbz (make_dGsq, src/basis_mod.f90:1993-2014),
 // w = 1 on the kx = 0 and kx = n1/2 planes, 2 elsewhere (each interior half

@@ -106,6 +106,8 @@ SIGNATURES = {
     "pscfg_propagate_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), _vp, _vp, C.c_double, C.c_double,
                                           _vp, _vp, C.c_int, _vp]),
     "pscfg_density_adjoint": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "pscfg_response": (C.c_int, [_vp, C.c_int, _dp, C.c_double, C.c_int, C.POINTER(C.c_int), _dp, C.c_int,
+                                 C.POINTER(C.c_int), _dp, _dp]),
     "pscfg_density_adjoint_device": (C.c_int, [_vp, _vp, _dp, _vp]),
     "pscfg_steps_per_density": (C.c_long, [_vp]),
     "pscfg_launch_count": (C.c_long, [_vp]),
@@ -246,6 +248,27 @@ class Engine:
             gq[:, : a.shape[1]] = a
         out = np.zeros_like(G)
         self._check(self.lib.pscfg_density_adjoint(self._h, _ptr(G), None if gq is None else _ptr(gq), _ptr(out)))
+        return out
+
+    def response_raw(self, inst: int, kvec, ktrans_sq: float, pert_monomer, pert_field, read_index, read_coef):
+        """pscfg_response: density response of instance `inst` to the Bloch
+        perturbations exp(ik.r) pert_field[p] of monomer pert_monomer[p],
+        read at the waves read_index (complex coefficients read_coef).
+        Returns out [n_pert][n_monomer][n_read]."""
+        pm = np.ascontiguousarray(pert_monomer, dtype=np.int32)
+        P = len(pm)
+        W = np.ascontiguousarray(np.asarray(pert_field, dtype=np.complex128).reshape(P, self.nr))
+        ri = np.ascontiguousarray(read_index, dtype=np.int32)
+        rc = np.ascontiguousarray(np.asarray(read_coef, dtype=np.complex128).reshape(len(ri)))
+        k = np.zeros(3)
+        kv = np.asarray(kvec, dtype=np.float64).ravel()
+        k[: min(3, kv.size)] = kv[:3]
+        out = np.zeros((P, self.M, len(ri)))
+        ip = C.POINTER(C.c_int)
+        self._check(self.lib.pscfg_response(self._h, inst, _ptr(k), float(ktrans_sq), P, pm.ctypes.data_as(ip),
+                                            W.view(np.float64).ctypes.data_as(_dp), len(ri),
+                                            ri.ctypes.data_as(ip), rc.view(np.float64).ctypes.data_as(_dp),
+                                            _ptr(out)))
         return out
 
     def scf_stress(self) -> np.ndarray:

@@ -95,7 +95,12 @@ def _signed_permutations() -> List[str]:
 
 # Generators (International Tables for Crystallography, Vol. A).
 _GENERATORS: Dict[str, Tuple[int, List[str]]] = {
+    "1": (1, ["x"]),
     "-1": (1, ["-x"]),
+    "p 1": (2, ["x,y"]),
+    "p 2": (2, ["-x,-y"]),
+    "P 1": (3, ["x,y,z"]),
+    "P -1": (3, ["-x,-y,-z"]),
     "p 6 m m": (2, ["x-y,x", "-y,-x"]),
     "I m -3 m": (3, _signed_permutations() + ["x+1/2,y+1/2,z+1/2"]),
     "I a -3 d": (3, ["-x+1/2,-y,z+1/2", "-x,y+1/2,-z+1/2", "z,x,y", "y+3/4,x+1/4,-z+1/4",
@@ -104,12 +109,20 @@ _GENERATORS: Dict[str, Tuple[int, List[str]]] = {
                         "x,y+1/2,z+1/2", "x+1/2,y,z+1/2", "x+1/2,y+1/2,z"]),
 }
 
-ALIASES = {"P -1": "-1", "p -1": "-1", "P 6 m m": "p 6 m m", "229": "I m -3 m", "230": "I a -3 d",
-           "70": "F d d d : 2", "17": "p 6 m m"}
+ALIASES = {"P 6 m m": "p 6 m m", "229": "I m -3 m", "230": "I a -3 d", "70": "F d d d : 2", "17": "p 6 m m"}
+# 1-D names as the reference spells them in 3-D notation (response_startup
+# maps 'P 1' to '1' for dim = 1, src/response_mod.f90:227)
+ALIASES_1D = {"P 1": "1", "P -1": "-1", "p -1": "-1"}
 
 
-def group(name: str) -> List[Op]:
-    name = ALIASES.get(name, name)
+def resolve(name: str, dim: int = None) -> str:
+    if dim == 1 and name in ALIASES_1D:
+        return ALIASES_1D[name]
+    return ALIASES.get(name, name)
+
+
+def group(name: str, dim: int = None) -> List[Op]:
+    name = resolve(name, dim)
     if name not in _GENERATORS:
         raise KeyError(f"space group {name!r} is not tabulated here")
     d, gens = _GENERATORS[name]
@@ -128,7 +141,7 @@ def grid_ops(name: str, ngrid: Sequence[int]):
     Raises ValueError if the grid is not mapped onto itself (a translation
     not a multiple of 1/n, or a rotation mixing axes of different extent).
     """
-    ops = group(name)
+    ops = group(name, len(ngrid))
     d = len(ops[0][0])
     if d != len(ngrid):
         raise ValueError(f"group {name!r} is {d}-dimensional, grid is {len(ngrid)}-dimensional")

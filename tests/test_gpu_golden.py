@@ -109,8 +109,9 @@ def test_symmetry_projection_keeps_symmetric_solution():
 
 
 def test_mixed_precision_matches_fp64_solution():
-    """FP32 propagation until the residual nears 1e-5, then FP64 to 1e-11:
-    the converged free energy equals the FP64 solve to 1e-10 per monomer."""
+    """FP32 propagation until the residual nears the switch error (1e-3 by
+    default), then FP64 to 1e-11: the converged free energy equals the FP64
+    solve to 1e-10 per monomer."""
     from pscf_b200.engine import MIXED
     ss = _bcc_systems()[:4]
     w0 = np.stack([sphere_guess(s, s.chains[0].block_length[0], width=0.05) for s in ss])
