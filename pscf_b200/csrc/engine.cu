@@ -105,6 +105,7 @@ struct Engine {
     int n_hist_alloc = 0;
     bool no_fixed_kernels = false;   // force the run-time sized kernels (tests)
     bool cluster_step = false;       // one-launch cluster step for 32^3 (PSCFG_CLUSTER_STEP=1)
+    bool smem_zconv = false;         // shared-memory z pass instead of register columns (PSCFG_SMEM_ZCONV=1)
     // optional CUDA-event timing of the phases (ms, accumulated)
     bool profiling = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -360,6 +361,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         E.no_fixed_kernels = v && v[0] && v[0] != '0';
         const char *c = std::getenv("PSCFG_CLUSTER_STEP");
         E.cluster_step = c && c[0] && c[0] != '0';
+        const char *z = std::getenv("PSCFG_SMEM_ZCONV");
+        E.smem_zconv = z && z[0] && z[0] != '0';
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
@@ -435,11 +438,25 @@ static void step3c(Engine &E, const SweepField<T> *dfl, int nf, int t)
     CK(allow_dyn_smem((const void *)k3c_inv_final<T, N1, N2, N3, PPC>));
     k3c_fwd_pair<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, nf), 256, sm, E.st>>>(dfl, g, t);
     E.launched();
-    k3c_zconv<T, N1, N2, N3, TC><<<dim3(ntile, nf, 2), 256, 0, E.st>>>(dfl, g, t, 3);
+    // z pass: register columns for N3 <= 32 (a 64-point column does not fit
+    // a thread's registers in FP64), shared-memory tiles otherwise
+    constexpr bool REGZ = N3 <= 32;
+    const bool regz = REGZ && !E.smem_zconv;
+    const unsigned rtile = (unsigned)((P + 127) / 128);
+    auto zpass = [&](int which, int nz) {
+        if constexpr (REGZ) {
+            if (regz) {
+                k3r_zconv<T, N1, N2, N3><<<dim3(rtile, nf, nz), 128, 0, E.st>>>(dfl, t, which);
+                return;
+            }
+        }
+        k3c_zconv<T, N1, N2, N3, TC><<<dim3(ntile, nf, nz), 256, 0, E.st>>>(dfl, g, t, which);
+    };
+    zpass(3, 2);
     E.launched();
     k3c_inv_mid<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, nf), 256, sm, E.st>>>(dfl, g, t);
     E.launched();
-    k3c_zconv<T, N1, N2, N3, TC><<<dim3(ntile, nf, 1), 256, 0, E.st>>>(dfl, g, t, 2);
+    zpass(2, 1);
     E.launched();
     k3c_inv_final<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, nf), 256, sm, E.st>>>(dfl, g, t);
     E.launched();
@@ -1285,14 +1302,15 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
             // instance moves to FP64 once its error is below the switch error,
             // or once it is within 1000x of it and has not improved by 10% for
             // 10 iterations (the FP32 noise floor), or as soon as its error
-            // rises to 10x the best FP32 error (an FP32 run drifting away), or
-            // after 500 FP32 iterations
+            // rises to 1000x the best FP32 error or stops being finite (an FP32
+            // run blowing up; smaller rises are normal early in Anderson
+            // mixing), or after 500 FP32 iterations
             const bool was32 = I.prec_now == PSCFG_FP32;
             if (was32) {
                 s.itr_fp32++;
                 const double sw = prm.switch_error > 0 ? prm.switch_error : 1e-3;
                 bool go = s.error < sw || s.error < prm.error_max || s.itr_fp32 >= 500 ||
-                          !(s.error <= 10.0 * s.best);
+                          !(s.error <= 1.0e3 * s.best);
                 if (s.error < 0.9 * s.best) {
                     s.best = s.error;
                     s.since_best = 0;

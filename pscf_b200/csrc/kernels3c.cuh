@@ -237,6 +237,37 @@ __global__ void __launch_bounds__(256) k3c_zconv(const SweepField<T> *fields, Pl
     }
 }
 
+// K2/K4 with register columns: one thread owns a whole z column of the
+// spectrum (N3 values, loaded coalesced across the warp: consecutive threads
+// take consecutive columns), transforms it in registers in natural order,
+// multiplies by ek and transforms back.  No shared memory, no barriers.
+// grid = (ceil(P / 128), nfields, 1 or 2); which as in k3c_zconv.
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(128) k3r_zconv(const SweepField<T> *fields, int t, int which)
+{
+    constexpr int NH = N1 / 2 + 1, P = N2 * NH;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= P) return;
+    const int sel = which == 3 ? (int)blockIdx.z + 1 : which;
+    cx<T> *S = ((sel == 1) ? f.S1 : f.S2) + col;
+    const T *ek = ((sel == 1) ? f.ek1[blk] : f.ek2[blk]) + (col % NH) + NH * iperm<N2>(col / NH);
+    cx<T> v[N3];
+#pragma unroll
+    for (int z = 0; z < N3; z++) v[z] = S[(long)z * P];
+    RegDft<N3, -1, T>::run(v);
+#pragma unroll
+    for (int k = 0; k < N3; k++) {
+        const T e = __ldg(ek + (long)k * P);
+        v[k] = mk<T>(e * v[k].x, e * v[k].y);
+    }
+    RegDft<N3, 1, T>::run(v);
+#pragma unroll
+    for (int z = 0; z < N3; z++) S[(long)z * P] = v[z];
+}
+
 // K3: q1 = eo1 Fxy^-1[S1]/N ; S2 <- Fxy[eo1 Fxy^-1[S2]/N]
 template <typename T, int N1, int N2, int N3, int PPC>
 __global__ void __launch_bounds__(256) k3c_inv_mid(const SweepField<T> *fields, PlaneGeom g, int t)
