@@ -106,6 +106,7 @@ struct Engine {
     bool no_fixed_kernels = false;   // force the run-time sized kernels (tests)
     bool cluster_step = false;       // one-launch cluster step for 32^3 (PSCFG_CLUSTER_STEP=1)
     bool smem_zconv = false;         // shared-memory z pass instead of register columns (PSCFG_SMEM_ZCONV=1)
+    bool smem_fft = false;           // shared-memory x-y column passes (PSCFG_SMEM_FFT=1)
     // optional CUDA-event timing of the phases (ms, accumulated)
     bool profiling = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -363,6 +364,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         E.cluster_step = c && c[0] && c[0] != '0';
         const char *z = std::getenv("PSCFG_SMEM_ZCONV");
         E.smem_zconv = z && z[0] && z[0] != '0';
+        const char *xy = std::getenv("PSCFG_SMEM_FFT");
+        E.smem_fft = xy && xy[0] && xy[0] != '0';
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
@@ -462,6 +465,30 @@ static void step3c(Engine &E, const SweepField<T> *dfl, int nf, int t)
     E.launched();
 }
 
+// One 3-D MDE step with register-column x-y kernels (natural y order) and
+// the register z pass: 128 threads and PPC planes per CTA.
+template <typename T, int N1, int N2, int N3, int PPC>
+static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
+{
+    constexpr int P = N2 * (N1 / 2 + 1);
+    const size_t sm = sizeof(cx<T>) * PPC * P;
+    CK(allow_dyn_smem((const void *)k3r_fwd_pair<T, N1, N2, N3, PPC>));
+    CK(allow_dyn_smem((const void *)k3r_inv_mid<T, N1, N2, N3, PPC>));
+    CK(allow_dyn_smem((const void *)k3r_inv_final<T, N1, N2, N3, PPC>));
+    const dim3 gp(N3 / PPC, nf);
+    const unsigned rtile = (unsigned)((P + 127) / 128);
+    k3r_fwd_pair<T, N1, N2, N3, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
+    E.launched();
+    k3r_zconv<T, N1, N2, N3, true><<<dim3(rtile, nf, 2), 128, 0, E.st>>>(dfl, t, 3);
+    E.launched();
+    k3r_inv_mid<T, N1, N2, N3, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
+    E.launched();
+    k3r_zconv<T, N1, N2, N3, true><<<dim3(rtile, nf, 1), 128, 0, E.st>>>(dfl, t, 2);
+    E.launched();
+    k3r_inv_final<T, N1, N2, N3, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
+    E.launched();
+}
+
 // Returns true if the grid has a compile-time-shaped step (and runs it).
 template <typename T>
 static bool step3_fixed(Engine &E, const SweepField<T> *dfl, int nf, int t)
@@ -476,10 +503,15 @@ static bool step3_fixed(Engine &E, const SweepField<T> *dfl, int nf, int t)
             E.launched();
             return true;
         }
-        step3c<T, 32, 32, 32, 8>(E, dfl, nf, t);
+        if (E.smem_fft) step3c<T, 32, 32, 32, 8>(E, dfl, nf, t);
+        else step3r<T, 32, 32, 32, 4>(E, dfl, nf, t);
         return true;
     }
-    if (a == 16 && b == 16 && c == 16) { step3c<T, 16, 16, 16, 8>(E, dfl, nf, t); return true; }
+    if (a == 16 && b == 16 && c == 16) {
+        if (E.smem_fft) step3c<T, 16, 16, 16, 8>(E, dfl, nf, t);
+        else step3r<T, 16, 16, 16, 8>(E, dfl, nf, t);
+        return true;
+    }
     if (a == 64 && b == 64 && c == 64) { step3c<T, 64, 64, 64, 1>(E, dfl, nf, t); return true; }
     return false;
 }

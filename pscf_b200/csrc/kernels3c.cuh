@@ -176,6 +176,162 @@ struct PlaneStack {
     }
 };
 
+// A stack of PPC x-y planes like PlaneStack, with the column (y)
+// transforms in registers: one thread per (plane, kx) column holds its N2
+// values, so a transform is one shared-memory pass for the rows and one
+// for the columns, and spectra are in natural y order.  The forward
+// transform writes the columns straight to global memory, the inverse
+// reads them from there.
+template <typename T, int N1, int N2, int PPC>
+struct PlaneStackR {
+    static constexpr int M = N1 / 2, NH = M + 1, PS = N2 * NH, NP = N1 * N2;
+    using Base = PlaneStack<T, N1, N2, PPC>;
+
+    template <typename F>
+    __device__ __forceinline__ static void pack(cx<T> *buf, F value) { Base::pack(buf, value); }
+    __device__ __forceinline__ static T real_at(const cx<T> *buf, int e) { return Base::real_at(buf, e); }
+
+    // natural packed rows in buf -> spectrum [plane][y][kx] in dst (global)
+    __device__ __forceinline__ static void forward_to(cx<T> *buf, cx<T> *__restrict__ dst)
+    {
+        __syncthreads();
+        for (int row = threadIdx.x; row < PPC * N2; row += blockDim.x) {
+            cx<T> *b = buf + row * NH;
+            cx<T> z[M];
+#pragma unroll
+            for (int m = 0; m < M; m++) z[m] = b[m];
+            RegDft<M, -1, T>::run(z);
+#pragma unroll
+            for (int k = 0; k <= M; k++) {
+                const cx<T> zk = z[k % M], zm = conjg(z[(M - k) % M]);
+                const cx<T> w = twc<T>(N1, k);
+                b[k] = scale((zk + zm) + mul_si<-1>(cmul(w, zk - zm)), (T)0.5);
+            }
+        }
+        __syncthreads();
+        for (int c = threadIdx.x; c < PPC * NH; c += blockDim.x) {
+            const int off = (c / NH) * PS + (c % NH);
+            cx<T> v[N2];
+#pragma unroll
+            for (int y = 0; y < N2; y++) v[y] = buf[off + y * NH];
+            RegDft<N2, -1, T>::run(v);
+#pragma unroll
+            for (int y = 0; y < N2; y++) dst[off + y * NH] = v[y];
+        }
+    }
+
+    // spectrum [plane][y][kx] in src (global) -> natural packed rows of the
+    // unnormalised c2r in buf
+    __device__ __forceinline__ static void inverse_from(const cx<T> *__restrict__ src, cx<T> *buf)
+    {
+        __syncthreads();
+        for (int c = threadIdx.x; c < PPC * NH; c += blockDim.x) {
+            const int off = (c / NH) * PS + (c % NH);
+            cx<T> v[N2];
+#pragma unroll
+            for (int y = 0; y < N2; y++) v[y] = src[off + y * NH];
+            RegDft<N2, 1, T>::run(v);
+#pragma unroll
+            for (int y = 0; y < N2; y++) buf[off + y * NH] = v[y];
+        }
+        __syncthreads();
+        for (int row = threadIdx.x; row < PPC * N2; row += blockDim.x) {
+            cx<T> *b = buf + row * NH;
+            cx<T> x[M + 1];
+#pragma unroll
+            for (int k = 0; k <= M; k++) x[k] = b[k];
+            cx<T> z[M];
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                const cx<T> xk = x[k], xm = conjg(x[M - k]);
+                const cx<T> w = conjg(twc<T>(N1, k));
+                z[k] = (xk + xm) + mul_si<1>(cmul(w, xk - xm));
+            }
+            RegDft<M, 1, T>::run(z);
+#pragma unroll
+            for (int m = 0; m < M; m++) b[m] = z[m];
+        }
+        __syncthreads();
+    }
+};
+
+// The five step kernels of the register-column variant (same algebra as
+// k3c_fwd_pair / k3c_inv_mid / k3c_inv_final; spectra in natural y order,
+// z pass k3r_zconv<..., true>).  128 threads, PPC planes per CTA.
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(128, 3) k3r_fwd_pair(const SweepField<T> *fields, int t)
+{
+    using PSk = PlaneStackR<T, N1, N2, PPC>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3;
+    const int z0 = blockIdx.x * PPC;
+    const T *q = src_slice(f, src, nr) + (long)z0 * PSk::NP;
+    const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP, *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
+    PSk::pack(buf, [&](int e) { return eo1[e] * q[e]; });
+    PSk::forward_to(buf, f.S1 + (long)z0 * PSk::PS);
+    __syncthreads();
+    PSk::pack(buf, [&](int e) { return eo2[e] * q[e]; });
+    PSk::forward_to(buf, f.S2 + (long)z0 * PSk::PS);
+}
+
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(128, 3) k3r_inv_mid(const SweepField<T> *fields, int t)
+{
+    using PSk = PlaneStackR<T, N1, N2, PPC>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const T rn = (T)((long)N1 * N2 * N3);
+    const int z0 = blockIdx.x * PPC;
+    const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP;
+    T *q1 = f.q1 + (long)z0 * PSk::NP;
+    PSk::inverse_from(f.S1 + (long)z0 * PSk::PS, buf);
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) q1[e] = eo1[e] * PSk::real_at(buf, e) / rn;
+    PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
+    T *hout = f.h_out ? f.h_out + (long)z0 * PSk::NP : nullptr;
+    for (int i = threadIdx.x; i < PPC * N2 * PSk::M; i += blockDim.x) {
+        const int p = i / (N2 * PSk::M), r = i % (N2 * PSk::M), y = r / PSk::M, m = r % PSk::M;
+        const int e = p * PSk::NP + y * N1 + 2 * m;
+        cx<T> &z = buf[p * PSk::PS + y * PSk::NH + m];
+        z = mk<T>(eo1[e] * z.x / rn, eo1[e + 1] * z.y / rn);
+        if (hout) {
+            hout[e] = z.x;
+            hout[e + 1] = z.y;
+        }
+    }
+    PSk::forward_to(buf, f.S2 + (long)z0 * PSk::PS);
+}
+
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(128, 3) k3r_inv_final(const SweepField<T> *fields, int t)
+{
+    using PSk = PlaneStackR<T, N1, N2, PPC>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3;
+    const T rn = (T)nr;
+    const int z0 = blockIdx.x * PPC;
+    const T *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
+    const T *q1 = f.q1 + (long)z0 * PSk::NP;
+    T *out = dst_slice(f, dst, nr) + (long)z0 * PSk::NP;
+    T *q2o = f.q2_out ? f.q2_out + (long)z0 * PSk::NP : nullptr;
+    PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
+        const T q2 = eo2[e] * PSk::real_at(buf, e) / rn;
+        out[e] = ((T)4 * q2 - q1[e]) / (T)3;
+        if (q2o) q2o[e] = q2;
+    }
+}
+
 // K1: S1 = Fxy[eo1 q], S2 = Fxy[eo2 q]   grid = (N3/PPC, nfields)
 template <typename T, int N1, int N2, int N3, int PPC>
 __global__ void __launch_bounds__(256) k3c_fwd_pair(const SweepField<T> *fields, PlaneGeom g, int t)
@@ -242,7 +398,7 @@ __global__ void __launch_bounds__(256) k3c_zconv(const SweepField<T> *fields, Pl
 // take consecutive columns), transforms it in registers in natural order,
 // multiplies by ek and transforms back.  No shared memory, no barriers.
 // grid = (ceil(P / 128), nfields, 1 or 2); which as in k3c_zconv.
-template <typename T, int N1, int N2, int N3>
+template <typename T, int N1, int N2, int N3, bool YNAT = false>
 __global__ void __launch_bounds__(128) k3r_zconv(const SweepField<T> *fields, int t, int which)
 {
     constexpr int NH = N1 / 2 + 1, P = N2 * NH;
@@ -253,7 +409,7 @@ __global__ void __launch_bounds__(128) k3r_zconv(const SweepField<T> *fields, in
     if (col >= P) return;
     const int sel = which == 3 ? (int)blockIdx.z + 1 : which;
     cx<T> *S = ((sel == 1) ? f.S1 : f.S2) + col;
-    const T *ek = ((sel == 1) ? f.ek1[blk] : f.ek2[blk]) + (col % NH) + NH * iperm<N2>(col / NH);
+    const T *ek = ((sel == 1) ? f.ek1[blk] : f.ek2[blk]) + (col % NH) + NH * (YNAT ? col / NH : iperm<N2>(col / NH));
     cx<T> v[N3];
 #pragma unroll
     for (int z = 0; z < N3; z++) v[z] = S[(long)z * P];
