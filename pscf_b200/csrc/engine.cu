@@ -815,13 +815,37 @@ static void stress3c(Engine &E, const StressJob<T> *dj, int s0, int cnt)
     E.launched();
 }
 
+// Stress slice sums with the register-column kernels (N3 <= 32).
+template <typename T, int N1, int N2, int N3, int PPC>
+static void stress3r(Engine &E, const StressJob<T> *dj, int s0, int cnt)
+{
+    constexpr int P = N2 * (N1 / 2 + 1);
+    const int ntile = (P + 127) / 128;
+    const size_t sm = sizeof(cx<T>) * PPC * P;
+    CK(allow_dyn_smem((const void *)k3r_stress_xy<T, N1, N2, N3, PPC>));
+    k3r_stress_xy<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, cnt, 2), 128, sm, E.st>>>(dj, s0, (cx<T> *)E.spec);
+    E.launched();
+    k3r_stress_z<T, N1, N2, N3><<<dim3(ntile, cnt), 128, 0, E.st>>>(dj, s0, (cx<T> *)E.spec, E.stress_part);
+    E.launched();
+    k3_stress_sum<T><<<cnt, 32, 0, E.st>>>(dj, s0, ntile, E.stress_part);
+    E.launched();
+}
+
 template <typename T>
 static bool stress3_fixed(Engine &E, const StressJob<T> *dj, int s0, int cnt)
 {
     if (E.no_fixed_kernels) return false;
     const int a = E.n[0], b = E.n[1], c = E.n[2];
-    if (a == 32 && b == 32 && c == 32) { stress3c<T, 32, 32, 32, 8>(E, dj, s0, cnt); return true; }
-    if (a == 16 && b == 16 && c == 16) { stress3c<T, 16, 16, 16, 8>(E, dj, s0, cnt); return true; }
+    if (a == 32 && b == 32 && c == 32) {
+        if (E.smem_fft) stress3c<T, 32, 32, 32, 8>(E, dj, s0, cnt);
+        else stress3r<T, 32, 32, 32, 4>(E, dj, s0, cnt);
+        return true;
+    }
+    if (a == 16 && b == 16 && c == 16) {
+        if (E.smem_fft) stress3c<T, 16, 16, 16, 8>(E, dj, s0, cnt);
+        else stress3r<T, 16, 16, 16, 8>(E, dj, s0, cnt);
+        return true;
+    }
     if (a == 64 && b == 64 && c == 64) { stress3c<T, 64, 64, 64, 1>(E, dj, s0, cnt); return true; }
     return false;
 }

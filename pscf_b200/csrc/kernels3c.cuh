@@ -513,6 +513,77 @@ __global__ void __launch_bounds__(256) k3c_stress_xy(const StressJob<T> *job, Pl
     PSk::store(spec + ((long)blockIdx.y * 2 + blockIdx.z) * nk + (long)z0 * PSk::PS, buf);
 }
 
+// Register-column variant of the stress pass.  Pass 1: x-y forward of PPC
+// planes of slice s (qf or qr) with PlaneStackR (natural y order), 128
+// threads.  grid = (N3/PPC, cs, 2).
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(128, 3) k3r_stress_xy(const StressJob<T> *job, int s0, cx<T> *spec)
+{
+    using PSk = PlaneStackR<T, N1, N2, PPC>;
+    const StressJob<T> &J = *job;
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3, nk = (long)PSk::PS * N3;
+    const int z0 = blockIdx.x * PPC;
+    const T *q = (blockIdx.z == 0 ? J.qf : J.qr) + (long)s * nr + (long)z0 * PSk::NP;
+    PSk::pack(buf, [&](int e) { return q[e]; });
+    PSk::forward_to(buf, spec + ((long)blockIdx.y * 2 + blockIdx.z) * nk + (long)z0 * PSk::PS);
+}
+
+// Pass 2: one thread per z column: z-forward of the qf spectrum in
+// registers (written back in place), then of the qr spectrum, and the
+// weighted products sum_k wdgsq_b(k) Re(F conj R) of its column; block
+// sums per tile of 128 columns.  grid = (ceil(P/128), cs).
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(128) k3r_stress_z(const StressJob<T> *job, int s0, cx<T> *spec, double *part)
+{
+    constexpr int NH = N1 / 2 + 1, P = N2 * NH;
+    const StressJob<T> &J = *job;
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    __shared__ double red[32];
+    const long nk = (long)P * N3;
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[PSCFG_MAXCP] = {0, 0, 0, 0, 0, 0};
+    if (col < P) {
+        cx<T> *sf = spec + ((long)blockIdx.y * 2) * nk + col;
+        const cx<T> *sr = sf + nk;
+        cx<T> v[N3];
+#pragma unroll
+        for (int z = 0; z < N3; z++) v[z] = sf[(long)z * P];
+        RegDft<N3, -1, T>::run(v);
+#pragma unroll
+        for (int k = 0; k < N3; k++) sf[(long)k * P] = v[k];
+        // re-read the stored spectrum below instead of keeping it live in
+        // registers next to the second column (which would spill)
+        asm volatile("" ::: "memory");
+#pragma unroll
+        for (int z = 0; z < N3; z++) v[z] = sr[(long)z * P];
+        RegDft<N3, -1, T>::run(v);
+        double d[N3];
+#pragma unroll
+        for (int k = 0; k < N3; k++) {
+            const cx<T> f = sf[(long)k * P];
+            d[k] = (double)f.x * (double)v[k].x + (double)f.y * (double)v[k].y;
+        }
+        const double *w = J.wdgsq + col;
+#pragma unroll 1
+        for (int b = 0; b < J.ncp; b++) {
+            double a = 0.0;
+#pragma unroll
+            for (int k = 0; k < N3; k++) a += __ldg(w + (long)b * nk + (long)k * P) * d[k];
+            acc[b] = a;
+        }
+    }
+    for (int b = 0; b < J.ncp; b++) {
+        const double tot = block_sum(acc[b], red);
+        if (threadIdx.x == 0) part[((long)blockIdx.y * gridDim.x + blockIdx.x) * PSCFG_MAXCP + b] = tot;
+        __syncthreads();
+    }
+}
+
 // Pass 2: z-forward of both spectra on TC columns and the weighted dot
 // products sum_k wdgsq_b(k) Re(F conj R).  grid = (ntiles, cs).
 template <typename T, int N1, int N2, int N3, int TC>

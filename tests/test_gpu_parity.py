@@ -154,6 +154,29 @@ def test_fixed_shape_kernels_match_generic(n, monkeypatch):
         assert rel_err(c, a) < tol
 
 
+@pytest.mark.parametrize("n", [16, 32])
+def test_fixed_shape_density_and_stress_paths_agree(n, monkeypatch):
+    """Register-column kernels (default), shared-memory kernels and the
+    run-time sized kernels give the same density, Q and stress."""
+    s = diblock(3, [n, n, n], "cubic", [1.95], fA=0.3, ds=0.05)
+    w = omega_guess(s, 11, 2.0)
+    out = []
+    for env in ({}, {"PSCFG_SMEM_FFT": "1"}, {"PSCFG_GENERIC_KERNELS": "1"}):
+        for k in ("PSCFG_SMEM_FFT", "PSCFG_GENERIC_KERNELS"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        e = Engine([s], FP64)
+        rho, q = e.density(w[None])
+        st = e.scf_stress()
+        out.append((rho, q[:, :1], st[:, :1]))
+        e.close()
+    for o in out[1:]:
+        assert rel_err(o[0], out[0][0]) < 1e-13
+        assert rel_err(o[1], out[0][1]) < 1e-13
+        assert abs(o[2][0, 0] - out[0][2][0, 0]) < 1e-11 * max(1.0, abs(out[0][2][0, 0]))
+
+
 def _blend(ensemble):
     """AB diblock + A homopolymer + B-selective solvent (three species)."""
     from pscf_b200.system import Chain, Solvent, System
