@@ -466,7 +466,7 @@ static void step3c(Engine &E, const SweepField<T> *dfl, int nf, int t)
 }
 
 // One 3-D MDE step with register-column x-y kernels (natural y order) and
-// the register z pass: 128 threads and PPC planes per CTA.
+// the split-column z pass: 128 threads and PPC planes per CTA.
 template <typename T, int N1, int N2, int N3, int PPC>
 static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
 {
@@ -476,14 +476,14 @@ static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
     CK(allow_dyn_smem((const void *)k3r_inv_mid<T, N1, N2, N3, PPC>));
     CK(allow_dyn_smem((const void *)k3r_inv_final<T, N1, N2, N3, PPC>));
     const dim3 gp(N3 / PPC, nf);
-    const unsigned rtile = (unsigned)((P + 127) / 128);
+    const unsigned rtile = (unsigned)((P + 63) / 64);
     k3r_fwd_pair<T, N1, N2, N3, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
     E.launched();
-    k3r_zconv<T, N1, N2, N3, true><<<dim3(rtile, nf, 2), 128, 0, E.st>>>(dfl, t, 3);
+    k3s_zconv<T, N1, N2, N3, true><<<dim3(rtile, nf, 2), 128, 0, E.st>>>(dfl, t, 3);
     E.launched();
     k3r_inv_mid<T, N1, N2, N3, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
     E.launched();
-    k3r_zconv<T, N1, N2, N3, true><<<dim3(rtile, nf, 1), 128, 0, E.st>>>(dfl, t, 2);
+    k3s_zconv<T, N1, N2, N3, true><<<dim3(rtile, nf, 1), 128, 0, E.st>>>(dfl, t, 2);
     E.launched();
     k3r_inv_final<T, N1, N2, N3, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
     E.launched();

@@ -176,12 +176,67 @@ struct PlaneStack {
     }
 };
 
+// K2/K4 with a z column shared by two threads (half the registers of
+// k3r_zconv): lanes c and c+16 of a warp own column col.  Forward by
+// decimation in time: lane half h transforms the samples z = 2j + h
+// (length N3/2, registers), the odd half applies W_N^k, the halves meet in
+// shared memory and each lane forms one half of the spectrum, X[k + h N3/2].
+// After the ek multiply the inverse runs by decimation in frequency: the
+// spectrum halves meet again, lane half h forms (A + B) or (A - B) w^k,
+// transforms it and owns the samples z = 2m + h.  Natural order in and out.
+// 128 threads = 4 warps x 16 columns; grid = (ceil(P/64), nfields, 1 or 2).
+template <typename T, int N1, int N2, int N3, bool YNAT>
+__global__ void __launch_bounds__(128) k3s_zconv(const SweepField<T> *fields, int t, int which)
+{
+    constexpr int NH = N1 / 2 + 1, P = N2 * NH, H = N3 / 2;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    __shared__ __align__(16) cx<T> X[4][N3][16];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4, c = lane & 15;
+    const int col = (blockIdx.x * 4 + w) * 16 + c;
+    const bool ok = col < P;
+    const int sel = which == 3 ? (int)blockIdx.z + 1 : which;
+    cx<T> *S = ((sel == 1) ? f.S1 : f.S2) + (ok ? col : 0);
+    cx<T> v[H];
+#pragma unroll
+    for (int j = 0; j < H; j++) v[j] = ok ? S[(long)(2 * j + h) * P] : mk<T>((T)0, (T)0);
+    RegDft<H, -1, T>::run(v);
+#pragma unroll
+    for (int k = 0; k < H; k++) X[w][h * H + k][c] = (h && k) ? cmul(v[k], twc<T>(N3, k)) : v[k];
+    __syncwarp();
+    const T *ek = ((sel == 1) ? f.ek1[blk] : f.ek2[blk]) + (ok ? (col % NH) + NH * (YNAT ? col / NH : iperm<N2>(col / NH)) : 0);
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        const cx<T> a = X[w][k][c], b = X[w][H + k][c];
+        const cx<T> x = h ? a - b : a + b;
+        const T e = ok ? __ldg(ek + (long)(k + h * H) * P) : (T)0;
+        v[k] = mk<T>(e * x.x, e * x.y);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < H; k++) X[w][h * H + k][c] = v[k];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < H; k++) {
+        const cx<T> a = X[w][k][c], b = X[w][H + k][c];
+        v[k] = h ? ((k == 0) ? a - b : cmul(a - b, conjg(twc<T>(N3, k)))) : a + b;
+    }
+    RegDft<H, 1, T>::run(v);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < H; m++) S[(long)(2 * m + h) * P] = v[m];
+    }
+}
+
 // A stack of PPC x-y planes like PlaneStack, with the column (y)
-// transforms in registers: one thread per (plane, kx) column holds its N2
-// values, so a transform is one shared-memory pass for the rows and one
-// for the columns, and spectra are in natural y order.  The forward
-// transform writes the columns straight to global memory, the inverse
-// reads them from there.
+// transforms in registers: two lanes of a warp share a (plane, kx) column
+// and hold half of its N2 values each (decimation in time forward, in
+// frequency inverse, the halves meeting in place in the plane buffer), so
+// a transform is one shared-memory pass for the rows and one for the
+// columns, and spectra are in natural y order.  The forward transform
+// writes the columns straight to global memory, the inverse reads them
+// from there.  blockDim must be a multiple of 32.
 template <typename T, int N1, int N2, int PPC>
 struct PlaneStackR {
     static constexpr int M = N1 / 2, NH = M + 1, PS = N2 * NH, NP = N1 * N2;
@@ -209,14 +264,31 @@ struct PlaneStackR {
             }
         }
         __syncthreads();
-        for (int c = threadIdx.x; c < PPC * NH; c += blockDim.x) {
-            const int off = (c / NH) * PS + (c % NH);
-            cx<T> v[N2];
+        // columns, two lanes per column (lanes c and c+16 of a warp):
+        // decimation in time, the halves meet in place in buf
+        constexpr int H = N2 / 2, NCB = (PPC * NH + 15) / 16;
+        const int h = (threadIdx.x >> 4) & 1, cl = threadIdx.x & 15;
+        for (int cb = threadIdx.x >> 5; cb < NCB; cb += blockDim.x >> 5) {
+            const int c = cb * 16 + cl;
+            const bool ok = c < PPC * NH;
+            const int off = ok ? (c / NH) * PS + (c % NH) : 0;
+            cx<T> v[H];
+            if (ok) {
 #pragma unroll
-            for (int y = 0; y < N2; y++) v[y] = buf[off + y * NH];
-            RegDft<N2, -1, T>::run(v);
+                for (int j = 0; j < H; j++) v[j] = buf[off + (2 * j + h) * NH];
+                RegDft<H, -1, T>::run(v);
 #pragma unroll
-            for (int y = 0; y < N2; y++) dst[off + y * NH] = v[y];
+                for (int k = 0; k < H; k++) buf[off + (2 * k + h) * NH] = (h && k) ? cmul(v[k], twc<T>(N2, k)) : v[k];
+            }
+            __syncwarp();
+            if (ok) {
+#pragma unroll
+                for (int k = 0; k < H; k++) {
+                    const cx<T> a = buf[off + 2 * k * NH], b = buf[off + (2 * k + 1) * NH];
+                    dst[off + (k + h * H) * NH] = h ? a - b : a + b;
+                }
+            }
+            __syncwarp();
         }
     }
 
@@ -225,25 +297,42 @@ struct PlaneStackR {
     __device__ __forceinline__ static void inverse_from(const cx<T> *__restrict__ src, cx<T> *buf)
     {
         __syncthreads();
-        for (int c = threadIdx.x; c < PPC * NH; c += blockDim.x) {
-            const int off = (c / NH) * PS + (c % NH);
-            cx<T> v[N2];
+        // columns, two lanes per column: each lane brings its spectrum half
+        // into buf, then decimation in frequency; lane half h ends with the
+        // samples y = 2m + h
+        constexpr int H = N2 / 2, NCB = (PPC * NH + 15) / 16;
+        const int h = (threadIdx.x >> 4) & 1, cl = threadIdx.x & 15;
+        for (int cb = threadIdx.x >> 5; cb < NCB; cb += blockDim.x >> 5) {
+            const int c = cb * 16 + cl;
+            const bool ok = c < PPC * NH;
+            const int off = ok ? (c / NH) * PS + (c % NH) : 0;
+            cx<T> v[H];
+            if (ok) {
 #pragma unroll
-            for (int y = 0; y < N2; y++) v[y] = src[off + y * NH];
-            RegDft<N2, 1, T>::run(v);
+                for (int k = 0; k < H; k++) buf[off + (k + h * H) * NH] = src[off + (k + h * H) * NH];
+            }
+            __syncwarp();
+            if (ok) {
 #pragma unroll
-            for (int y = 0; y < N2; y++) buf[off + y * NH] = v[y];
+                for (int k = 0; k < H; k++) {
+                    const cx<T> a = buf[off + k * NH], b = buf[off + (k + H) * NH];
+                    v[k] = h ? ((k == 0) ? a - b : cmul(a - b, conjg(twc<T>(N2, k)))) : a + b;
+                }
+            }
+            __syncwarp();
+            if (ok) {
+                RegDft<H, 1, T>::run(v);
+#pragma unroll
+                for (int m = 0; m < H; m++) buf[off + (2 * m + h) * NH] = v[m];
+            }
         }
         __syncthreads();
         for (int row = threadIdx.x; row < PPC * N2; row += blockDim.x) {
             cx<T> *b = buf + row * NH;
-            cx<T> x[M + 1];
-#pragma unroll
-            for (int k = 0; k <= M; k++) x[k] = b[k];
             cx<T> z[M];
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                const cx<T> xk = x[k], xm = conjg(x[M - k]);
+                const cx<T> xk = b[k], xm = conjg(b[M - k]);
                 const cx<T> w = conjg(twc<T>(N1, k));
                 z[k] = (xk + xm) + mul_si<1>(cmul(w, xk - xm));
             }
@@ -259,7 +348,7 @@ struct PlaneStackR {
 // k3c_fwd_pair / k3c_inv_mid / k3c_inv_final; spectra in natural y order,
 // z pass k3r_zconv<..., true>).  128 threads, PPC planes per CTA.
 template <typename T, int N1, int N2, int N3, int PPC>
-__global__ void __launch_bounds__(128, 3) k3r_fwd_pair(const SweepField<T> *fields, int t)
+__global__ void __launch_bounds__(128, 4) k3r_fwd_pair(const SweepField<T> *fields, int t)
 {
     using PSk = PlaneStackR<T, N1, N2, PPC>;
     const SweepField<T> &f = fields[blockIdx.y];
@@ -279,7 +368,7 @@ __global__ void __launch_bounds__(128, 3) k3r_fwd_pair(const SweepField<T> *fiel
 }
 
 template <typename T, int N1, int N2, int N3, int PPC>
-__global__ void __launch_bounds__(128, 3) k3r_inv_mid(const SweepField<T> *fields, int t)
+__global__ void __launch_bounds__(128, 4) k3r_inv_mid(const SweepField<T> *fields, int t)
 {
     using PSk = PlaneStackR<T, N1, N2, PPC>;
     const SweepField<T> &f = fields[blockIdx.y];
@@ -309,7 +398,7 @@ __global__ void __launch_bounds__(128, 3) k3r_inv_mid(const SweepField<T> *field
 }
 
 template <typename T, int N1, int N2, int N3, int PPC>
-__global__ void __launch_bounds__(128, 3) k3r_inv_final(const SweepField<T> *fields, int t)
+__global__ void __launch_bounds__(128, 4) k3r_inv_final(const SweepField<T> *fields, int t)
 {
     using PSk = PlaneStackR<T, N1, N2, PPC>;
     const SweepField<T> &f = fields[blockIdx.y];
@@ -517,7 +606,7 @@ __global__ void __launch_bounds__(256) k3c_stress_xy(const StressJob<T> *job, Pl
 // planes of slice s (qf or qr) with PlaneStackR (natural y order), 128
 // threads.  grid = (N3/PPC, cs, 2).
 template <typename T, int N1, int N2, int N3, int PPC>
-__global__ void __launch_bounds__(128, 3) k3r_stress_xy(const StressJob<T> *job, int s0, cx<T> *spec)
+__global__ void __launch_bounds__(128, 4) k3r_stress_xy(const StressJob<T> *job, int s0, cx<T> *spec)
 {
     using PSk = PlaneStackR<T, N1, N2, PPC>;
     const StressJob<T> &J = *job;

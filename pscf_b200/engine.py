@@ -21,7 +21,9 @@ from .system import (MAX_BLOCK, MAX_CELL_PARAM, MAX_CHAIN, MAX_MONOMER,
                      MAX_SOLVENT, System)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libpscfgpu.so")
+# PSCFG_LIB points the binding at another build of the same library (for
+# example one compiled with different flags); default: the in-tree build.
+LIB_PATH = os.environ.get("PSCFG_LIB") or os.path.join(_HERE, "_lib", "libpscfgpu.so")
 
 FP64 = 0
 FP32 = 1
