@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/pscf_gpu.h"
@@ -489,6 +490,47 @@ static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
     E.launched();
 }
 
+// A whole 3-D sweep with the register-column kernels, the last kernel of
+// every step fused with the first of the next.  Returns false where the
+// grid has no such kernels (or another path was requested).
+template <typename T>
+static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
+{
+    if (E.no_fixed_kernels || E.smem_fft || E.cluster_step) return false;
+    auto run = [&](auto n1c, auto ppcc) {
+        constexpr int N = decltype(n1c)::value, PPC = decltype(ppcc)::value;
+        constexpr int P = N * (N / 2 + 1);
+        const size_t sm = sizeof(cx<T>) * PPC * P;
+        CK(allow_dyn_smem((const void *)k3r_fwd_pair<T, N, N, N, PPC>));
+        CK(allow_dyn_smem((const void *)k3r_inv_mid<T, N, N, N, PPC>));
+        CK(allow_dyn_smem((const void *)k3r_final_fwd<T, N, N, N, PPC>));
+        const dim3 gp(N / PPC, nf);
+        const unsigned rtile = (unsigned)((P + 63) / 64);
+        k3r_fwd_pair<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, 0);
+        E.launched();
+        for (int t = 0; t < ns_max; t++) {
+            k3s_zconv<T, N, N, N, true><<<dim3(rtile, nf, 2), 128, 0, E.st>>>(dfl, t, 3);
+            E.launched();
+            k3r_inv_mid<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
+            E.launched();
+            k3s_zconv<T, N, N, N, true><<<dim3(rtile, nf, 1), 128, 0, E.st>>>(dfl, t, 2);
+            E.launched();
+            k3r_final_fwd<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
+            E.launched();
+        }
+    };
+    const int a = E.n[0], b = E.n[1], c = E.n[2];
+    if (a == 32 && b == 32 && c == 32) {
+        run(std::integral_constant<int, 32>(), std::integral_constant<int, 4>());
+        return true;
+    }
+    if (a == 16 && b == 16 && c == 16) {
+        run(std::integral_constant<int, 16>(), std::integral_constant<int, 8>());
+        return true;
+    }
+    return false;
+}
+
 // Returns true if the grid has a compile-time-shaped step (and runs it).
 template <typename T>
 static bool step3_fixed(Engine &E, const SweepField<T> *dfl, int nf, int t)
@@ -596,6 +638,7 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
         const long P = (long)g.n1h * g.n2;
         const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
         const int txy = 256, tz = 256;
+        if (sweep3r<T>(E, dfl, nf, ns_max)) return;
         for (int t = 0; t < ns_max; t++) {
             if (step3_fixed<T>(E, dfl, nf, t)) continue;
             k3_fwd_pair<T><<<dim3(g.n3, nf), txy, smxy, E.st>>>(dfl, g, t);
@@ -820,12 +863,12 @@ template <typename T, int N1, int N2, int N3, int PPC>
 static void stress3r(Engine &E, const StressJob<T> *dj, int s0, int cnt)
 {
     constexpr int P = N2 * (N1 / 2 + 1);
-    const int ntile = (P + 127) / 128;
+    const int ntile = (P + 63) / 64;
     const size_t sm = sizeof(cx<T>) * PPC * P;
     CK(allow_dyn_smem((const void *)k3r_stress_xy<T, N1, N2, N3, PPC>));
     k3r_stress_xy<T, N1, N2, N3, PPC><<<dim3(N3 / PPC, cnt, 2), 128, sm, E.st>>>(dj, s0, (cx<T> *)E.spec);
     E.launched();
-    k3r_stress_z<T, N1, N2, N3><<<dim3(ntile, cnt), 128, 0, E.st>>>(dj, s0, (cx<T> *)E.spec, E.stress_part);
+    k3s_stress_z<T, N1, N2, N3><<<dim3(ntile, cnt), 128, 0, E.st>>>(dj, s0, (const cx<T> *)E.spec, E.stress_part);
     E.launched();
     k3_stress_sum<T><<<cnt, 32, 0, E.st>>>(dj, s0, ntile, E.stress_part);
     E.launched();

@@ -245,6 +245,13 @@ struct PlaneStackR {
     template <typename F>
     __device__ __forceinline__ static void pack(cx<T> *buf, F value) { Base::pack(buf, value); }
     __device__ __forceinline__ static T real_at(const cx<T> *buf, int e) { return Base::real_at(buf, e); }
+    // the slot real_at reads, for writing a real value back in place
+    __device__ __forceinline__ static T &real_ref(cx<T> *buf, int e)
+    {
+        const int p = e / NP, r = e % NP, y = r / N1, x = r % N1;
+        cx<T> &z = buf[p * PS + y * NH + (x >> 1)];
+        return (x & 1) ? z.y : z.x;
+    }
 
     // natural packed rows in buf -> spectrum [plane][y][kx] in dst (global)
     __device__ __forceinline__ static void forward_to(cx<T> *buf, cx<T> *__restrict__ dst)
@@ -602,6 +609,48 @@ __global__ void __launch_bounds__(256) k3c_stress_xy(const StressJob<T> *job, Pl
     PSk::store(spec + ((long)blockIdx.y * 2 + blockIdx.z) * nk + (long)z0 * PSk::PS, buf);
 }
 
+// K5 of step t fused with K1 of step t+1 (sweeps only): q_out as in
+// k3r_inv_final, kept in the plane buffer, then, if the field has a step
+// t+1, its x-y forward transforms of exp(-w ds/2) q_out and
+// exp(-w ds/4) q_out with the tables of step t+1's block.
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(128, 4) k3r_final_fwd(const SweepField<T> *fields, int t)
+{
+    using PSk = PlaneStackR<T, N1, N2, PPC>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3;
+    const T rn = (T)nr;
+    const int z0 = blockIdx.x * PPC;
+    const T *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
+    const T *q1 = f.q1 + (long)z0 * PSk::NP;
+    T *out = dst_slice(f, dst, nr) + (long)z0 * PSk::NP;
+    PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
+        T &slot = PSk::real_ref(buf, e);
+        const T q2 = eo2[e] * slot / rn;
+        const T o = ((T)4 * q2 - q1[e]) / (T)3;
+        out[e] = o;
+        slot = o;
+    }
+    int blk2, src2, dst2;
+    if (!step_slices(f, t + 1, blk2, src2, dst2)) return;   // the same for the whole CTA
+    __syncthreads();
+    const T *n1 = f.eo1[blk2] + (long)z0 * PSk::NP, *n2 = f.eo2[blk2] + (long)z0 * PSk::NP;
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
+        T &slot = PSk::real_ref(buf, e);
+        slot = n1[e] * slot;
+    }
+    PSk::forward_to(buf, f.S1 + (long)z0 * PSk::PS);
+    __syncthreads();
+    const T *qn = out;   // written above by this CTA; visible after the barrier
+    PSk::pack(buf, [&](int e) { return n2[e] * qn[e]; });
+    PSk::forward_to(buf, f.S2 + (long)z0 * PSk::PS);
+}
+
 // Register-column variant of the stress pass.  Pass 1: x-y forward of PPC
 // planes of slice s (qf or qr) with PlaneStackR (natural y order), 128
 // threads.  grid = (N3/PPC, cs, 2).
@@ -663,6 +712,63 @@ __global__ void __launch_bounds__(128) k3r_stress_z(const StressJob<T> *job, int
             double a = 0.0;
 #pragma unroll
             for (int k = 0; k < N3; k++) a += __ldg(w + (long)b * nk + (long)k * P) * d[k];
+            acc[b] = a;
+        }
+    }
+    for (int b = 0; b < J.ncp; b++) {
+        const double tot = block_sum(acc[b], red);
+        if (threadIdx.x == 0) part[((long)blockIdx.y * gridDim.x + blockIdx.x) * PSCFG_MAXCP + b] = tot;
+        __syncthreads();
+    }
+}
+
+// Stress pass 2 with two lanes per z column (as k3s_zconv): each lane ends
+// with half of the qf spectrum and the same half of the qr spectrum in
+// registers and forms its products sum_k wdgsq_b(k) Re(F conj R) there;
+// block sums per tile of 64 columns.  grid = (ceil(P/64), cs).
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(128) k3s_stress_z(const StressJob<T> *job, int s0, const cx<T> *spec, double *part)
+{
+    constexpr int NH = N1 / 2 + 1, P = N2 * NH, H = N3 / 2;
+    const StressJob<T> &J = *job;
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    __shared__ __align__(16) cx<T> X[4][N3][16];
+    __shared__ double red[32];
+    const long nk = (long)P * N3;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4, c = lane & 15;
+    const int col = (blockIdx.x * 4 + w) * 16 + c;
+    const bool ok = col < P;
+    const cx<T> *sf = spec + ((long)blockIdx.y * 2) * nk + (ok ? col : 0), *sr = sf + nk;
+    // forward z transform of one column half (decimation in time); returns
+    // the spectrum entries k + h H, k < H, in v
+    auto ztrans = [&](const cx<T> *src, cx<T> *v) {
+#pragma unroll
+        for (int j = 0; j < H; j++) v[j] = ok ? src[(long)(2 * j + h) * P] : mk<T>((T)0, (T)0);
+        RegDft<H, -1, T>::run(v);
+#pragma unroll
+        for (int k = 0; k < H; k++) X[w][h * H + k][c] = (h && k) ? cmul(v[k], twc<T>(N3, k)) : v[k];
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < H; k++) {
+            const cx<T> a = X[w][k][c], b = X[w][H + k][c];
+            v[k] = h ? a - b : a + b;
+        }
+        __syncwarp();
+    };
+    cx<T> fv[H], rv[H];
+    ztrans(sf, fv);
+    ztrans(sr, rv);
+    double acc[PSCFG_MAXCP] = {0, 0, 0, 0, 0, 0};
+    if (ok) {
+        const double *wp = J.wdgsq + col + (long)h * H * P;
+#pragma unroll 1
+        for (int b = 0; b < J.ncp; b++) {
+            double a = 0.0;
+#pragma unroll
+            for (int k = 0; k < H; k++)
+                a += __ldg(wp + (long)b * nk + (long)k * P) *
+                     ((double)fv[k].x * (double)rv[k].x + (double)fv[k].y * (double)rv[k].y);
             acc[b] = a;
         }
     }
