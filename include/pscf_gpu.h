@@ -98,7 +98,7 @@ typedef struct pscfg_am_param {
     int domain;              /* 1: relax the unit cell (stress -> 0) */
     double error_max;
     double switch_error;     /* PSCFG_MIXED: FP32 -> FP64 below this error (0: 1e-3), on
-                                stagnation within 1000x of it, when the error rises to 1000x the
+                                stagnation within 1000x of it, when the error rises to 10x the
                                 best FP32 error, or after 500 FP32 iterations */
 } pscfg_am_param;
 

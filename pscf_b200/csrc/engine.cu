@@ -1401,15 +1401,16 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
             // instance moves to FP64 once its error is below the switch error,
             // or once it is within 1000x of it and has not improved by 10% for
             // 10 iterations (the FP32 noise floor), or as soon as its error
-            // rises to 1000x the best FP32 error or stops being finite (an FP32
-            // run blowing up; smaller rises are normal early in Anderson
-            // mixing), or after 500 FP32 iterations
+            // rises to 10x the best FP32 error or stops being finite, or after
+            // 500 FP32 iterations.  (Looser guards let FP32 runs that drift
+            // during a large cell change land in a different basin, from which
+            // the FP64 iteration may not converge.)
             const bool was32 = I.prec_now == PSCFG_FP32;
             if (was32) {
                 s.itr_fp32++;
                 const double sw = prm.switch_error > 0 ? prm.switch_error : 1e-3;
                 bool go = s.error < sw || s.error < prm.error_max || s.itr_fp32 >= 500 ||
-                          !(s.error <= 1.0e3 * s.best);
+                          !(s.error <= 10.0 * s.best);
                 if (s.error < 0.9 * s.best) {
                     s.best = s.error;
                     s.since_best = 0;
