@@ -179,6 +179,17 @@ int pscfg_density_adjoint(pscfg_engine *e, const double *grad_rho, const double 
 int pscfg_density_adjoint_device(pscfg_engine *e, const double *grad_rho_dev, const double *grad_lnq,
                                  double *grad_omega_dev);
 
+/* pscfg_density_adjoint plus the derivative with respect to the cell
+ * parameters: grad_cell [n_inst][PSCFG_MAXCP] (host) = dL/d cell_param.
+ * Exact derivative of the discrete algorithm (the k-space filters
+ * exp(-ds b^2 k^2/6), exp(-ds b^2 k^2/12) of step_exp depend on the cell
+ * through k^2 = G^T GG G, src/unit_cell_mod.f90:723-757); for
+ * L = -(phi/N) lnQ it is the continuum stress of scf_stress
+ * (src/scf_mod.fp.f90:451-550) up to the contour discretisation.  No
+ * counterpart routine in the reference. */
+int pscfg_density_adjoint_cell(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega,
+                               double *grad_cell);
+
 /* Ideal-gas linear response of instance `inst` to Bloch perturbations
  * (replaces drho_domega_id's loop over perturbations, calc_q0 / calc_delq /
  * calc_delrho, src/response_mod.f90:389-468, 697-1186, with the steps of

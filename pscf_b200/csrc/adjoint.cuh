@@ -109,4 +109,51 @@ __global__ void k_adj_overlap(const AdjOverlap *jobs, long nr, double *part)
     if (threadIdx.x == 0) part[(long)blockIdx.y * gridDim.x + blockIdx.x] = acc;
 }
 
+// Real-field pairs whose weighted spectral products give the cell
+// derivative of one adjoint step <lambda, P(cell) q>: with the symmetric
+// k-space filters C1 = C(ds), C2 = C(ds/2) and E1 = exp(-w ds/2),
+// E2 = exp(-w ds/4), h_x = E1 C2 E2 x,
+//   d<lambda, P1 q> = <E1 lambda, dC1 (E1 q)>,  C1 E1 q = P1 q / E1
+//   d<lambda, P2 q> = <E2 lambda, dC2 h_q> + <h_lambda, dC2 E2 q>,
+//                     C2 h_q = P2 q / E2,  C2 E2 q = h_q / E1
+// so the pairs (a, b) = (E1 lam, P1q/E1), (E2 lam, P2q/E2), (h_lam, h_q/E1)
+// carry the k-space filter in b.
+struct AdjCellPair {
+    const double *lam, *hl, *p1q, *hq, *p2q;
+    const double *eo1, *eo2;
+    double *a, *b;        // [3][nr] each
+};
+
+static __global__ void k_adj_cellpairs(const AdjCellPair *jobs, long nr)
+{
+    const AdjCellPair &J = jobs[blockIdx.y];
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += (long)gridDim.x * blockDim.x) {
+        const double e1 = J.eo1[r], e2 = J.eo2[r], l = J.lam[r];
+        J.a[r] = e1 * l;
+        J.b[r] = J.p1q[r] / e1;
+        J.a[nr + r] = e2 * l;
+        J.b[nr + r] = J.p2q[r] / e2;
+        J.a[2 * nr + r] = J.hl[r];
+        J.b[2 * nr + r] = J.hq[r] / e1;
+    }
+}
+
+// g[b] += sum over jobs and pairs of coef[pair] * inc[pair][b], fixed order
+struct AdjCellAcc {
+    const double *inc;    // [3][PSCFG_MAXCP]
+    double coef[3];
+    double *g;            // [PSCFG_MAXCP]
+    int ncp;
+};
+
+static __global__ void k_adj_cellacc(const AdjCellAcc *jobs, int n)
+{
+    const int b = threadIdx.x;
+    for (int k = 0; k < n; k++) {
+        const AdjCellAcc &J = jobs[k];
+        if (b < J.ncp)
+            for (int p = 0; p < 3; p++) J.g[b] += J.coef[p] * J.inc[p * PSCFG_MAXCP + b];
+    }
+}
+
 }  // namespace pscfg

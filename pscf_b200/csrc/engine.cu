@@ -57,6 +57,23 @@ struct Err {
 
 static const int Z_TILE = 16;
 
+// Device buffers owned by one call.
+struct CallScratch {
+    std::vector<void *> p;
+    void *get(size_t bytes)
+    {
+        void *d = nullptr;
+        cudaError_t e = cudaMalloc(&d, std::max(bytes, (size_t)16));
+        if (e != cudaSuccess) throw Err(PSCFG_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+        p.push_back(d);
+        return d;
+    }
+    ~CallScratch()
+    {
+        for (void *d : p) cudaFree(d);
+    }
+};
+
 struct Inst {
     pscfg_system sys;
     Cell cell;
@@ -91,6 +108,7 @@ struct Inst {
     int *d_orb_start = nullptr;
     int norb = 0;
     double *kweight = nullptr;    // [nk] star weights (nullptr: exact Parseval weights)
+    double *wdg0 = nullptr;       // [MAXCP][nk] stress weights without star weights (set with kweight)
 };
 
 struct Engine {
@@ -307,6 +325,8 @@ static void update_cells(Engine &E, const std::vector<int> &which)
         j.ksq = I.ksq;
         j.wdgsq = I.wdgsq;
         j.kweight = I.kweight;
+        if (I.kweight && !I.wdg0) I.wdg0 = (double *)E.dalloc(sizeof(double) * PSCFG_MAXCP * E.nk);
+        j.wdg0 = I.kweight ? I.wdg0 : nullptr;
         jobs.push_back(j);
         I.have_density = false;
     }
@@ -893,24 +913,12 @@ static bool stress3_fixed(Engine &E, const StressJob<T> *dj, int s0, int cnt)
     return false;
 }
 
+// Per slice s of every job: inc[s][b] = sum_k wdgsq_b(k) Re(F[qf_s] conj F[qr_s])
+// on the half spectrum (the stress slice sums; also the adjoint's cell pairs).
 template <typename T>
-static void stress_impl(Engine &E, const std::vector<int> &act)
+static void slice_dots(Engine &E, const std::vector<StressJob<T>> &jobs)
 {
     const PlaneGeom &g = E.geom();
-    std::vector<StressJob<T>> jobs;
-    for (int i : act) {
-        Inst &I = E.inst[i];
-        for (int c = 0; c < I.sys.n_chain; c++) {
-            StressJob<T> j;
-            j.qf = (const T *)I.qf[c];
-            j.qr = (const T *)I.qr[c];
-            j.wdgsq = I.wdgsq;
-            j.ncp = I.cell.ncp;
-            j.nslices = I.ns[c] + 1;
-            j.inc = I.inc[c];
-            jobs.push_back(j);
-        }
-    }
     if (jobs.empty()) return;
     StressJob<T> *dj = E.upload(jobs, 0);
     size_t off = ((jobs.size() * sizeof(StressJob<T>) + 255) / 256) * 256;
@@ -959,6 +967,29 @@ static void stress_impl(Engine &E, const std::vector<int> &act)
             }
         }
     }
+}
+
+template <typename T>
+static void stress_impl(Engine &E, const std::vector<int> &act)
+{
+    const PlaneGeom &g = E.geom();
+    std::vector<StressJob<T>> jobs;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            StressJob<T> j;
+            j.qf = (const T *)I.qf[c];
+            j.qr = (const T *)I.qr[c];
+            j.wdgsq = I.wdgsq;
+            j.ncp = I.cell.ncp;
+            j.nslices = I.ns[c] + 1;
+            j.inc = I.inc[c];
+            jobs.push_back(j);
+        }
+    }
+    if (jobs.empty()) return;
+    slice_dots<T>(E, jobs);
+    const size_t off = ((jobs.size() * sizeof(StressJob<T>) + 255) / 256) * 256;
     std::vector<StressFinal> fin;
     for (int i : act) {
         Inst &I = E.inst[i];
@@ -1602,7 +1633,8 @@ static void run_single_steps(Engine &E, const SweepField<T> *dfl, int nf)
 
 template <typename T>
 static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vector<const double *> &G,
-                         const std::vector<const double *> &gQ, const std::vector<double *> &grad)
+                         const std::vector<const double *> &gQ, const std::vector<double *> &grad,
+                         const std::vector<double *> &gcell)
 {
     const size_t ts = sizeof(T);
     const long nr = E.nr, nk = E.nk;
@@ -1671,6 +1703,18 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
         }
     }
     if (sw.empty()) return;
+    // cell derivative: pair slabs, slice sums and per-instance accumulators
+    bool want_cell = false;
+    for (double *p : gcell) want_cell = want_cell || p != nullptr;
+    CallScratch cscr;
+    double *cA = nullptr, *cB = nullptr, *cinc = nullptr, *cg = nullptr;
+    if (want_cell) {
+        cA = (double *)cscr.get(sizeof(double) * 3 * nr * sw.size());
+        cB = (double *)cscr.get(sizeof(double) * 3 * nr * sw.size());
+        cinc = (double *)cscr.get(sizeof(double) * 3 * PSCFG_MAXCP * sw.size());
+        cg = (double *)cscr.get(sizeof(double) * PSCFG_MAXCP * act.size());
+        CK(cudaMemsetAsync(cg, 0, sizeof(double) * PSCFG_MAXCP * act.size(), E.st));
+    }
     std::vector<double> Sc(ov.size());
     {
         AdjOverlap *dov = E.upload(ov, off);
@@ -1787,6 +1831,70 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
         run_single_steps<T>(E, dfl, (int)fl.size());
         k_adj_point<T><<<dim3((unsigned)std::min<long>((nr + 255) / 256, 256), (unsigned)pts.size()), 256, 0, E.st>>>(dpt, nr);
         E.launched();
+        if (want_cell) {
+            // the step's cell derivative (4/3) d<lam,P2 q> - (1/3) d<lam,P1 q>
+            // from three real-field pairs per sweep (adjoint.cuh)
+            std::vector<AdjCellPair> cp;
+            std::vector<StressJob<double>> cj;
+            std::vector<AdjCellAcc> ca;
+            int k = 0;
+            for (auto &S : sw) {
+                if (t >= S.ns) continue;
+                Inst &I = E.inst[S.inst];
+                size_t kin = 0;
+                while (act[kin] != S.inst) kin++;
+                const int cur = t & 1;
+                const int qslice = (S.d == 0) ? S.ns - 1 - t : t + 1;
+                const int blk = (S.d == 0) ? seg_block(I, S.c, qslice) : seg_block(I, S.c, qslice - 1);
+                AdjCellPair a;
+                a.lam = (const double *)S.lam[cur];
+                a.hl = (const double *)S.h[0];
+                a.p1q = (const double *)S.p1[1];
+                a.hq = (const double *)S.h[1];
+                a.p2q = (const double *)S.p2[1];
+                a.eo1 = (const double *)I.eo1[S.c][blk];
+                a.eo2 = (const double *)I.eo2[S.c][blk];
+                a.a = cA + (long)3 * k * nr;
+                a.b = cB + (long)3 * k * nr;
+                cp.push_back(a);
+                StressJob<double> j;
+                j.qf = a.a;
+                j.qr = a.b;
+                j.wdgsq = I.wdg0 ? I.wdg0 : I.wdgsq;
+                j.ncp = I.cell.ncp;
+                j.nslices = 3;
+                j.inc = cinc + (long)3 * k * PSCFG_MAXCP;
+                cj.push_back(j);
+                const double bb = I.sys.kuhn[I.sys.block_monomer[S.c][blk]];
+                const double f = I.bds[S.c][blk] * bb * bb / (double)nr;
+                AdjCellAcc acc;
+                acc.inc = j.inc;
+                acc.coef[0] = f / 18.0;
+                acc.coef[1] = -f / 9.0;
+                acc.coef[2] = -f / 9.0;
+                acc.g = cg + (long)kin * PSCFG_MAXCP;
+                acc.ncp = I.cell.ncp;
+                ca.push_back(acc);
+                k++;
+            }
+            if (k > 0) {
+                AdjCellPair *dcp = E.upload(cp, (size_t)8 << 20);
+                k_adj_cellpairs<<<dim3((unsigned)std::min<long>((nr + 255) / 256, 256), (unsigned)k), 256, 0, E.st>>>(dcp, nr);
+                E.launched();
+                slice_dots<double>(E, cj);
+                AdjCellAcc *dca = E.upload(ca, (size_t)9 << 20);
+                k_adj_cellacc<<<1, 32, 0, E.st>>>(dca, k);
+                E.launched();
+            }
+        }
+    }
+    if (want_cell) {
+        std::vector<double> h(PSCFG_MAXCP * act.size());
+        CK(cudaMemcpyAsync(h.data(), cg, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, E.st));
+        CK(cudaStreamSynchronize(E.st));
+        for (size_t k = 0; k < act.size(); k++)
+            if (k < gcell.size() && gcell[k])
+                for (int b = 0; b < PSCFG_MAXCP; b++) gcell[k][b] = b < E.inst[act[k]].cell.ncp ? h[k * PSCFG_MAXCP + b] : 0.0;
     }
     // grad = sum over sweeps of the instance, fixed order
     for (size_t k = 0; k < act.size(); k++) {
@@ -1802,7 +1910,8 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
 }
 
 static void adjoint_all(Engine &E, const std::vector<int> &act, const std::vector<const double *> &G,
-                        const std::vector<const double *> &gQ, const std::vector<double *> &grad)
+                        const std::vector<const double *> &gQ, const std::vector<double *> &grad,
+                        const std::vector<double *> &gcell = {})
 {
     for (int i : act)
         if (!E.inst[i].have_density) throw Err(PSCFG_ESTATE, "the adjoint requires a preceding density call");
@@ -1810,28 +1919,12 @@ static void adjoint_all(Engine &E, const std::vector<int> &act, const std::vecto
     split_prec(E, act, a64, a32);
     if (!a32.empty()) throw Err(PSCFG_EINVAL, "the adjoint runs on FP64 propagators (use PSCFG_FP64 or PSCFG_MIXED)");
     E.cur = PSCFG_FP64;
-    adjoint_impl<double>(E, act, G, gQ, grad);
+    adjoint_impl<double>(E, act, G, gQ, grad, gcell);
 }
 
 // ---------------------------------------------------------------------
 // Linear response of a periodic state (RESPONSE, src/response_mod.f90)
 // ---------------------------------------------------------------------
-// Device buffers owned by one call.
-struct CallScratch {
-    std::vector<void *> p;
-    void *get(size_t bytes)
-    {
-        void *d = nullptr;
-        cudaError_t e = cudaMalloc(&d, std::max(bytes, (size_t)16));
-        if (e != cudaSuccess) throw Err(PSCFG_ENOMEM, std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
-        p.push_back(d);
-        return d;
-    }
-    ~CallScratch()
-    {
-        for (void *d : p) cudaFree(d);
-    }
-};
 
 // Line passes of one complex transform of every job (k_cline).  step: the
 // fftc_step E IFFT[K FFT[E x]]; otherwise the forward transform / N.
@@ -2594,7 +2687,8 @@ int pscfg_set_symmetry(pscfg_engine *e, int inst, int nops, const int *ops)
 
 void *pscfg_stream(const pscfg_engine *e) { return e ? (void *)e->E.st : nullptr; }
 
-static int adjoint_common(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega, bool device)
+static int adjoint_common(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega, bool device,
+                          double *grad_cell = nullptr)
 {
     if (!e || !grad_rho || !grad_omega) return PSCFG_EINVAL;
     ABI_BEGIN
@@ -2622,7 +2716,10 @@ static int adjoint_common(pscfg_engine *e, const double *grad_rho, const double 
         gQ[i] = grad_lnq ? grad_lnq + (long)i * PSCFG_MAXC : nullptr;
     }
     try {
-        adjoint_all(E, all, G, gQ, out);
+        std::vector<double *> gc;
+        if (grad_cell)
+            for (int i = 0; i < ni; i++) gc.push_back(grad_cell + (long)i * PSCFG_MAXCP);
+        adjoint_all(E, all, G, gQ, out, gc);
         if (!device) {
             for (int i = 0; i < ni; i++)
                 CK(cudaMemcpyAsync(grad_omega + (long)i * fl, out[i], sizeof(double) * fl, cudaMemcpyDeviceToHost, E.st));
@@ -2645,6 +2742,13 @@ int pscfg_density_adjoint_device(pscfg_engine *e, const double *grad_rho_dev, co
                                  double *grad_omega_dev)
 {
     return adjoint_common(e, grad_rho_dev, grad_lnq, grad_omega_dev, true);
+}
+
+int pscfg_density_adjoint_cell(pscfg_engine *e, const double *grad_rho, const double *grad_lnq, double *grad_omega,
+                               double *grad_cell)
+{
+    if (!grad_cell) return PSCFG_EINVAL;
+    return adjoint_common(e, grad_rho, grad_lnq, grad_omega, false, grad_cell);
 }
 
 int pscfg_response(pscfg_engine *e, int inst, const double *kvec, double ktrans_sq, int n_pert,

@@ -402,6 +402,7 @@ struct GeomJob {
     double *ksq;     // [nk]
     double *wdgsq;   // [PSCFG_MAXCP][nk]
     const double *kweight;   // [nk] star weights or nullptr (all 1)
+    double *wdg0;            // [PSCFG_MAXCP][nk] w(kx) G^T dGG_b G without star weights, or nullptr
 };
 
 __device__ __forceinline__ double gnorm_dev(int dim, const int Gt[3], const double G[3][3])
@@ -449,14 +450,15 @@ static __global__ void k_make_geom(const GeomJob *jobs, int dim, int n1, int n2,
             }
         }
         J.ksq[idx] = gnorm_dev(dim, Gmin, J.G);
-        double w = (i1 == 0 || (n1 % 2 == 0 && i1 == n1 / 2)) ? 1.0 : 2.0;
-        if (J.kweight) w *= J.kweight[idx];
+        const double w0 = (i1 == 0 || (n1 % 2 == 0 && i1 == n1 / 2)) ? 1.0 : 2.0;
+        const double w = J.kweight ? w0 * J.kweight[idx] : w0;
         for (int b = 0; b < PSCFG_MAXCP; b++) {
             double v = 0;
             if (b < J.ncp)
                 for (int j = 0; j < dim; j++)
                     for (int l = 0; l < dim; l++) v += (double)Gmin[j] * (double)Gmin[l] * J.dGG[b][j][l];
             J.wdgsq[(long)b * nk + idx] = w * v;
+            if (J.wdg0) J.wdg0[(long)b * nk + idx] = w0 * v;
         }
     }
 }

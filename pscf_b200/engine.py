@@ -108,6 +108,7 @@ SIGNATURES = {
     "pscfg_propagate_noalloc": (C.c_int, [C.c_int, C.POINTER(C.c_int), _vp, _vp, C.c_double, C.c_double,
                                           _vp, _vp, C.c_int, _vp]),
     "pscfg_density_adjoint": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "pscfg_density_adjoint_cell": (C.c_int, [_vp, _dp, _dp, _dp, _dp]),
     "pscfg_response": (C.c_int, [_vp, C.c_int, _dp, C.c_double, C.c_int, C.POINTER(C.c_int), _dp, C.c_int,
                                  C.POINTER(C.c_int), _dp, _dp]),
     "pscfg_density_adjoint_device": (C.c_int, [_vp, _vp, _dp, _vp]),
@@ -240,8 +241,10 @@ class Engine:
         self._check(self.lib.pscfg_density_device(self._h, _vp(omega_dev_ptr), _vp(rho_dev_ptr), _ptr(q), None))
         return q
 
-    def density_adjoint(self, grad_rho, grad_lnq=None) -> np.ndarray:
-        """dL/domega for upstream dL/drho [n_inst][M][nr] and dL/dlnQ [n_inst][n_chain]."""
+    def density_adjoint(self, grad_rho, grad_lnq=None, want_cell=False):
+        """dL/domega for upstream dL/drho [n_inst][M][nr] and dL/dlnQ
+        [n_inst][n_chain]; with want_cell also dL/dcell_param
+        [n_inst][n_cell_param] (returns the pair)."""
         G = np.ascontiguousarray(grad_rho, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
         gq = None
         if grad_lnq is not None:
@@ -249,8 +252,14 @@ class Engine:
             a = np.asarray(grad_lnq, dtype=np.float64).reshape(self.n_inst, -1)
             gq[:, : a.shape[1]] = a
         out = np.zeros_like(G)
-        self._check(self.lib.pscfg_density_adjoint(self._h, _ptr(G), None if gq is None else _ptr(gq), _ptr(out)))
-        return out
+        if not want_cell:
+            self._check(self.lib.pscfg_density_adjoint(self._h, _ptr(G), None if gq is None else _ptr(gq), _ptr(out)))
+            return out
+        gc = np.zeros((self.n_inst, MAX_CELL_PARAM))
+        self._check(self.lib.pscfg_density_adjoint_cell(self._h, _ptr(G), None if gq is None else _ptr(gq), _ptr(out),
+                                                        _ptr(gc)))
+        ncp = len(self.systems[0].cell_param)
+        return out, gc[:, :ncp].copy()
 
     def response_raw(self, inst: int, kvec, ktrans_sq: float, pert_monomer, pert_field, read_index, read_coef):
         """pscfg_response: density response of instance `inst` to the Bloch
