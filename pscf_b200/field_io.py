@@ -1,0 +1,221 @@
+"""Field files in the reference's formats (src/field_io_mod.f90).
+
+Basis format (input_field / output_field, :55-135): a header
+  format 1 0 / dim / crystal_system / N_cell_param / cell_param /
+  group_name / N_monomer / N_star
+then one line per star: the N_monomer coefficients (ES20.12), the star's
+first wave G (I4 each, in first-Brillouin-zone form) and the number of
+waves in the star (I6).  A reader finds the star by its wave, so the line
+order does not matter (input_field :71-79).  The reference's basis
+function of a star is sum_G c_G exp(iG.r) with the coefficient of its first
+wave real and positive, 1/sqrt(N) with sqrt taken in single precision
+(src/basis_mod.f90:916-936), and the first wave is the largest in the
+ordering of G_lt (components compared in turn, :1576-1620).  Only stars
+closed under inversion are handled (the centrosymmetric groups); for
+other groups use the grid format.
+
+Grid format (output_field_grid :151-200, read back by RGRID_TO_FIELD,
+src/pscf.fp.f90:890-980): the same header up to N_monomer, then ngrid and
+the values at every grid point, x fastest, N_monomer values (F18.9) per
+line.
+
+Fields are handled here as grid arrays [n_monomer][nr] (x fastest), the
+engine's representation; the star coefficients are computed from them by
+FFT.
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
+
+from .basis import StarBasis
+from .system import make_unit_cell
+
+
+def _fl32_sqrt(n: int) -> float:
+    return float(np.sqrt(np.float32(n)))
+
+
+def _label(name: str) -> str:
+    return f"{name:<20}"
+
+
+def _header(cell: Dict, group_name: str, n_monomer: int) -> List[str]:
+    cp = list(cell["cell_param"])
+    return [" format  1  0",
+            _label("dim"), f"{cell['dim']:>20d}",
+            _label("crystal_system"), f"{chr(39) + cell['crystal_system'] + chr(39):>20}",
+            _label("N_cell_param"), f"{len(cp):>20d}",
+            _label("cell_param"), "".join(f"{v:20.10E}" for v in cp),
+            _label("group_name"), f"{chr(39) + group_name + chr(39):>20}",
+            _label("N_monomer"), f"{n_monomer:>20d}"]
+
+
+def _read_header(lines: List[str]) -> Tuple[Dict, int]:
+    """Parse 'name / value' pairs after the version line; returns the
+    header and the index of the first unread line."""
+    h: Dict = {}
+    i = 1
+    keys = ("dim", "crystal_system", "N_cell_param", "cell_param", "group_name", "N_monomer")
+    for k in keys:
+        assert lines[i].split()[0] == k, f"expected {k!r} in field file header, got {lines[i]!r}"
+        val = lines[i + 1].split()
+        i += 2
+        if k in ("dim", "N_cell_param", "N_monomer"):
+            h[k] = int(val[0])
+        elif k == "cell_param":
+            h[k] = [float(v.replace("D", "E")) for v in val]
+        else:
+            h[k] = " ".join(val).strip("'\"")
+    return h, i
+
+
+def _g_to_bz(G: np.ndarray, n: Sequence[int], Gb: np.ndarray, dim: int) -> np.ndarray:
+    """Minimum image of integer waves, images +1, 0, -1 per dimension in
+    that order, a later one winning only if shorter by more than 1e-8
+    (G_to_bz, src/grid_mod.f90:225-283).  G: [k, 3]."""
+    best = np.zeros_like(G)
+    gmin = np.full(len(G), 1.0e10)
+    rng = [(1, 0, -1) if a < dim else (0,) for a in range(3)]
+    for s1 in rng[0]:
+        for s2 in rng[1]:
+            for s3 in rng[2]:
+                t = G + np.array([s1 * n[0], s2 * n[1], s3 * n[2]])
+                v = t[:, :dim] @ Gb[:dim, :dim]
+                q = (v * v).sum(axis=1)
+                win = q < gmin - 1.0e-8
+                best[win] = t[win]
+                gmin[win] = q[win]
+    return best
+
+
+def _grid_waves(idx: np.ndarray, n: Sequence[int]) -> np.ndarray:
+    return np.stack([idx % n[0], (idx // n[0]) % n[1], idx // (n[0] * n[1])], axis=1)
+
+
+def _spectrum(field: np.ndarray, n: Sequence[int]) -> np.ndarray:
+    """F(G) = (1/N) sum_r f(r) exp(-iG.r), flat x fastest."""
+    nr = int(np.prod(n))
+    return (np.fft.fftn(field.reshape(n[2], n[1], n[0])) / nr).ravel()
+
+
+def _centrosymmetric_star(idx: np.ndarray, n: Sequence[int]) -> bool:
+    g = _grid_waves(idx, n)
+    neg = (-g) % np.array(n)
+    key = lambda w: set(map(tuple, w.tolist()))
+    return key(neg) == key(g)
+
+
+class FieldBasis:
+    """Star basis of a group on a grid with the reference's file
+    conventions (first wave, coefficient normalisation)."""
+
+    def __init__(self, group_name: str, system):
+        self.group = group_name
+        self.dim = system.dim
+        self.n = list(system.n)
+        self.nr = system.nr
+        self.basis = StarBasis(group_name, system.ngrid)
+        Gb = make_unit_cell(system.dim, system.crystal_system, system.cell_param)[0]
+        self.first = []        # flat grid index of the reference's first wave
+        self.first_bz = []     # its first-zone form
+        self.count = []
+        self.star_of = {}
+        for s, idx in enumerate(self.basis.star_idx):
+            if not _centrosymmetric_star(idx, self.n):
+                raise ValueError(f"group {group_name!r}: stars not closed under inversion are not "
+                                 "supported in the basis format (use the grid format)")
+            bz = _g_to_bz(_grid_waves(np.asarray(idx), self.n), self.n, Gb, self.dim)
+            order = sorted(range(len(idx)), key=lambda j: tuple(bz[j][:self.dim]), reverse=True)
+            j0 = order[0]
+            self.first.append(int(idx[j0]))
+            self.first_bz.append(bz[j0][:self.dim].astype(int))
+            self.count.append(len(idx))
+            for i in idx:
+                self.star_of[int(i)] = s
+
+    def to_coeffs(self, field: np.ndarray) -> np.ndarray:
+        """Reference basis coefficients [n_star] of a grid field."""
+        F = _spectrum(np.asarray(field, dtype=np.float64), self.n)
+        return np.array([float(np.real(F[i])) * _fl32_sqrt(c) for i, c in zip(self.first, self.count)])
+
+    def to_grid(self, coeffs: Sequence[float]) -> np.ndarray:
+        """Grid field sum_s a_s f_s with the reference's basis functions."""
+        F = np.zeros(self.nr, dtype=complex)
+        for s, a in enumerate(coeffs):
+            idx = np.asarray(self.basis.star_idx[s])
+            c = np.asarray(self.basis.star_coef[s])
+            j0 = int(np.nonzero(idx == self.first[s])[0][0])
+            F[idx] += a * c / c[j0] / _fl32_sqrt(self.count[s])
+        n = self.n
+        f = np.fft.ifftn(F.reshape(n[2], n[1], n[0])) * self.nr
+        return np.real(f).ravel()
+
+
+def write_field(path: str, fields: np.ndarray, system, group_name: str) -> None:
+    """Basis-format file of grid fields [n_monomer][nr] (output_field)."""
+    fb = FieldBasis(group_name, system)
+    fields = np.asarray(fields, dtype=np.float64).reshape(-1, system.nr)
+    coeffs = np.stack([fb.to_coeffs(f) for f in fields])          # [M][n_star]
+    cell = {"dim": system.dim, "crystal_system": system.crystal_system, "cell_param": system.cell_param}
+    out = _header(cell, group_name, len(fields))
+    out += [_label("N_star"), f"{fb.basis.n_star:>20d}"]
+    for s in range(fb.basis.n_star):
+        line = "".join(f"{a:20.12E}" for a in coeffs[:, s]) + "    "
+        line += "".join(f"{g:4d}" for g in fb.first_bz[s]) + f"{fb.count[s]:6d}"
+        out.append(line)
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+
+
+def read_field(path: str, system, group_name: str = None) -> Tuple[Dict, np.ndarray]:
+    """(header, grid fields [n_monomer][nr]) of a basis-format file
+    (input_field).  `system` gives the grid; the group is the file's unless
+    given.  A star count in the file that differs from the basis rescales
+    its coefficient by sqrt(N_file / N_basis), as input_field does."""
+    lines = open(path).read().splitlines()
+    h, i = _read_header(lines)
+    assert lines[i].split()[0] == "N_star"
+    nstar = int(lines[i + 1].split()[0])
+    M = h["N_monomer"]
+    fb = FieldBasis(group_name or h["group_name"], system)
+    coeffs = np.zeros((M, fb.basis.n_star))
+    n = np.array(system.n)
+    for line in lines[i + 2:i + 2 + nstar]:
+        v = line.split()
+        a = np.array([float(x.replace("D", "E")) for x in v[:M]])
+        g = np.zeros(3, dtype=int)
+        g[:system.dim] = [int(x) for x in v[M:M + system.dim]]
+        n_arm = int(v[M + system.dim])
+        gi = g % n
+        flat = int(gi[0] + n[0] * (gi[1] + n[1] * gi[2]))
+        s = fb.star_of.get(flat)
+        if s is None:
+            continue                      # a wave with no star on this grid (valid_wave false)
+        coeffs[:, s] = a * np.sqrt(n_arm / fb.count[s])
+    fields = np.stack([fb.to_grid(coeffs[m]) for m in range(M)])
+    return h, fields
+
+
+def write_rgrid(path: str, fields: np.ndarray, system, group_name: str) -> None:
+    """Grid-format file (output_field_grid)."""
+    fields = np.asarray(fields, dtype=np.float64).reshape(-1, system.nr)
+    cell = {"dim": system.dim, "crystal_system": system.crystal_system, "cell_param": system.cell_param}
+    out = _header(cell, group_name, len(fields))
+    out += [_label("ngrid"), "".join(f"{g:20d}" for g in system.ngrid)]
+    for r in range(system.nr):
+        out.append("".join(f"{fields[m, r]:18.9f}" for m in range(len(fields))) + "    ")
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+
+
+def read_rgrid(path: str) -> Tuple[Dict, List[int], np.ndarray]:
+    """(header, ngrid, grid fields [n_monomer][nr]) of a grid-format file."""
+    lines = open(path).read().splitlines()
+    h, i = _read_header(lines)
+    assert lines[i].split()[0] == "ngrid"
+    ngrid = [int(x) for x in lines[i + 1].split()]
+    nr = int(np.prod(ngrid))
+    vals = np.array([[float(x) for x in ln.split()] for ln in lines[i + 2:i + 2 + nr]])
+    return h, ngrid, vals.T.copy()
