@@ -242,8 +242,20 @@ struct PlaneStackR {
     static constexpr int M = N1 / 2, NH = M + 1, PS = N2 * NH, NP = N1 * N2;
     using Base = PlaneStack<T, N1, N2, PPC>;
 
+    static constexpr int KT = 128;   // threads per CTA of the kernels using this stack
+
+    // packed rows z[m] = f(2m) + i f(2m+1); compile-time stride so that the
+    // loads of several iterations are in flight together
     template <typename F>
-    __device__ __forceinline__ static void pack(cx<T> *buf, F value) { Base::pack(buf, value); }
+    __device__ __forceinline__ static void pack(cx<T> *buf, F value)
+    {
+#pragma unroll 4
+        for (int i = threadIdx.x; i < PPC * N2 * M; i += KT) {
+            const int p = i / (N2 * M), r = i % (N2 * M), y = r / M, m = r % M;
+            const int e = p * NP + y * N1 + 2 * m;
+            buf[p * PS + y * NH + m] = mk<T>(value(e), value(e + 1));
+        }
+    }
     __device__ __forceinline__ static T real_at(const cx<T> *buf, int e) { return Base::real_at(buf, e); }
     // the slot real_at reads, for writing a real value back in place
     __device__ __forceinline__ static T &real_ref(cx<T> *buf, int e)
@@ -388,10 +400,13 @@ __global__ void __launch_bounds__(128, 4) k3r_inv_mid(const SweepField<T> *field
     const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP;
     T *q1 = f.q1 + (long)z0 * PSk::NP;
     PSk::inverse_from(f.S1 + (long)z0 * PSk::PS, buf);
-    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) q1[e] = eo1[e] * PSk::real_at(buf, e) / rn;
+#pragma unroll 4
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) q1[e] = eo1[e] * PSk::real_at(buf, e) / rn;
     PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
     T *hout = f.h_out ? f.h_out + (long)z0 * PSk::NP : nullptr;
-    for (int i = threadIdx.x; i < PPC * N2 * PSk::M; i += blockDim.x) {
+
+#pragma unroll 4
+    for (int i = threadIdx.x; i < PPC * N2 * PSk::M; i += PSk::KT) {
         const int p = i / (N2 * PSk::M), r = i % (N2 * PSk::M), y = r / PSk::M, m = r % PSk::M;
         const int e = p * PSk::NP + y * N1 + 2 * m;
         cx<T> &z = buf[p * PSk::PS + y * PSk::NH + m];
@@ -421,7 +436,9 @@ __global__ void __launch_bounds__(128, 4) k3r_inv_final(const SweepField<T> *fie
     T *out = dst_slice(f, dst, nr) + (long)z0 * PSk::NP;
     T *q2o = f.q2_out ? f.q2_out + (long)z0 * PSk::NP : nullptr;
     PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
-    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
+
+#pragma unroll 4
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) {
         const T q2 = eo2[e] * PSk::real_at(buf, e) / rn;
         out[e] = ((T)4 * q2 - q1[e]) / (T)3;
         if (q2o) q2o[e] = q2;
@@ -629,7 +646,9 @@ __global__ void __launch_bounds__(128, 4) k3r_final_fwd(const SweepField<T> *fie
     const T *q1 = f.q1 + (long)z0 * PSk::NP;
     T *out = dst_slice(f, dst, nr) + (long)z0 * PSk::NP;
     PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
-    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
+
+#pragma unroll 4
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) {
         T &slot = PSk::real_ref(buf, e);
         const T q2 = eo2[e] * slot / rn;
         const T o = ((T)4 * q2 - q1[e]) / (T)3;
@@ -640,7 +659,9 @@ __global__ void __launch_bounds__(128, 4) k3r_final_fwd(const SweepField<T> *fie
     if (!step_slices(f, t + 1, blk2, src2, dst2)) return;   // the same for the whole CTA
     __syncthreads();
     const T *n1 = f.eo1[blk2] + (long)z0 * PSk::NP, *n2 = f.eo2[blk2] + (long)z0 * PSk::NP;
-    for (int e = threadIdx.x; e < PPC * PSk::NP; e += blockDim.x) {
+
+#pragma unroll 4
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) {
         T &slot = PSk::real_ref(buf, e);
         slot = n1[e] * slot;
     }
