@@ -163,3 +163,54 @@ def test_torch_autograd_cell_input():
     g_ref, gc_ref = e.density_adjoint(G[None], np.array([[1.0]]), want_cell=True)
     np.testing.assert_allclose(w.grad.numpy()[0], g_ref[0], rtol=1e-12, atol=1e-14)
     np.testing.assert_allclose(cell.grad.numpy(), gc_ref, rtol=1e-12)
+
+
+def test_gyroid_64_loss_gradients():
+    """The gyroid workload (I a -3 d, 64^3, a = 3.7, f_A = 0.40, chi N = 16,
+    ds = 0.005, FP64 forward): L = sum_r (phi_A - phi_target)^2 with a seeded
+    smooth target (+-0.1 around f_A); dL/domega at sampled points and dL/da
+    through torch.autograd agree with central differences (h = 1e-6
+    relative for a; 1e-4 for omega, whose single-point effect on the summed
+    loss is below roundoff at 1e-6).  chi does not enter density(omega):
+    dL/dchi = 0."""
+    import torch
+    from pscf_b200.autograd import density
+    s = diblock(3, [64, 64, 64], "cubic", [3.7], fA=0.40, chiN=16.0, ds=0.005)
+    n = 64
+    x = 2 * np.pi * np.arange(n) / n
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    Gy = (np.sin(X) * np.cos(Y) + np.sin(Y) * np.cos(Z) + np.sin(Z) * np.cos(X)).ravel()
+    delta = -(np.abs(Gy) - np.abs(Gy).mean())
+    w0 = s.omega_uniform()
+    rng = np.random.default_rng(20261203 + 3)
+    w = np.stack([w0[0] + delta, w0[1] - delta]) + rng.normal(0, 0.01, (2, s.nr))
+    # target: Gaussian-filtered N(0,1) (sigma = 2 cells), scaled to +-0.1 around f_A
+    k = np.fft.fftfreq(n) * n
+    KZ, KY, KX = np.meshgrid(k, k, k, indexing="ij")
+    filt = np.exp(-0.5 * (2.0 * 2 * np.pi / n) ** 2 * (KX ** 2 + KY ** 2 + KZ ** 2))
+    t = np.real(np.fft.ifftn(np.fft.fftn(rng.normal(size=(n, n, n))) * filt)).ravel()
+    target = 0.40 + 0.1 * t / np.max(np.abs(t))
+    e = Engine([s], FP64)
+
+    def loss_np(wv, a):
+        e.set_cell_param(0, [a])
+        rho, _ = e.density(wv[None])
+        return float(((rho[0, 0] - target) ** 2).sum())
+
+    wt = torch.tensor(w[None], dtype=torch.float64, requires_grad=True)
+    cell = torch.tensor([[3.7]], dtype=torch.float64, requires_grad=True)
+    rho, _ = density(wt, e, cell)
+    L = ((rho[0, 0] - torch.from_numpy(target)) ** 2).sum()
+    L.backward()
+    gw = wt.grad.numpy()[0]
+    h = 1e-6 * 3.7
+    fd_a = (loss_np(w, 3.7 + h) - loss_np(w, 3.7 - h)) / (2 * h)
+    assert abs(fd_a - cell.grad.item()) < 1e-5 * max(1.0, abs(fd_a)), (fd_a, cell.grad.item())
+    for m, r in [(0, 0), (1, 12345), (0, 200000), (1, 77777)]:
+        hw = 1e-4 * max(1.0, abs(w[m, r]))    # a smaller step is below the roundoff of L
+        wp, wm = w.copy(), w.copy()
+        wp[m, r] += hw
+        wm[m, r] -= hw
+        fd = (loss_np(wp, 3.7) - loss_np(wm, 3.7)) / (2 * hw)
+        assert abs(fd - gw[m, r]) < 1e-6 * max(1e-3, abs(fd)) + 1e-10, (m, r, fd, gw[m, r])
+    e.close()
