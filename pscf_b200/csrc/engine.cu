@@ -126,6 +126,15 @@ struct Engine {
     bool cluster_step = false;       // one-launch cluster step for 32^3 (PSCFG_CLUSTER_STEP=1)
     bool smem_zconv = false;         // shared-memory z pass instead of register columns (PSCFG_SMEM_ZCONV=1)
     bool smem_fft = false;           // shared-memory x-y column passes (PSCFG_SMEM_FFT=1)
+    bool no_graphs = false;          // launch the 3-D sweeps directly (PSCFG_NO_GRAPHS=1)
+    // CUDA graphs of 3-D sweeps, keyed by descriptor address, field and step count
+    struct SweepGraph {
+        const void *dfl;
+        int nf, ns, tsize;
+        cudaGraphExec_t exec;
+        long launches;
+    };
+    std::vector<SweepGraph> graphs;
     // optional CUDA-event timing of the phases (ms, accumulated)
     bool profiling = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -162,6 +171,7 @@ struct Engine {
         if (stress_part) cudaFree(stress_part);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -387,6 +397,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         E.smem_zconv = z && z[0] && z[0] != '0';
         const char *xy = std::getenv("PSCFG_SMEM_FFT");
         E.smem_fft = xy && xy[0] && xy[0] != '0';
+        const char *ng = std::getenv("PSCFG_NO_GRAPHS");
+        E.no_graphs = ng && ng[0] && ng[0] != '0';
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
@@ -517,6 +529,9 @@ template <typename T>
 static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
 {
     if (E.no_fixed_kernels || E.smem_fft || E.cluster_step) return false;
+    // The sweep is a fixed sequence of 1 + 4 ns_max launches whose jobs are
+    // read from the descriptors at dfl, so it is captured once into a CUDA
+    // graph per (dfl, nf, ns_max) and replayed after each descriptor upload.
     auto run = [&](auto n1c, auto ppcc) {
         constexpr int N = decltype(n1c)::value, PPC = decltype(ppcc)::value;
         constexpr int P = N * (N / 2 + 1);
@@ -526,18 +541,56 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
         CK(allow_dyn_smem((const void *)k3r_final_fwd<T, N, N, N, PPC>));
         const dim3 gp(N / PPC, nf);
         const unsigned rtile = (unsigned)((P + 63) / 64);
-        k3r_fwd_pair<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, 0);
-        E.launched();
-        for (int t = 0; t < ns_max; t++) {
-            k3s_zconv<T, N, N, N, true><<<dim3(rtile, nf, 2), 128, 0, E.st>>>(dfl, t, 3);
+        auto emit = [&]() {
+            k3r_fwd_pair<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, 0);
             E.launched();
-            k3r_inv_mid<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
-            E.launched();
-            k3s_zconv<T, N, N, N, true><<<dim3(rtile, nf, 1), 128, 0, E.st>>>(dfl, t, 2);
-            E.launched();
-            k3r_final_fwd<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
-            E.launched();
+            for (int t = 0; t < ns_max; t++) {
+                k3s_zconv<T, N, N, N, true><<<dim3(rtile, nf, 2), 128, 0, E.st>>>(dfl, t, 3);
+                E.launched();
+                k3r_inv_mid<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
+                E.launched();
+                k3s_zconv<T, N, N, N, true><<<dim3(rtile, nf, 1), 128, 0, E.st>>>(dfl, t, 2);
+                E.launched();
+                k3r_final_fwd<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
+                E.launched();
+            }
+        };
+        if (E.no_graphs) {
+            emit();
+            return;
         }
+        for (auto &g : E.graphs)
+            if (g.dfl == (const void *)dfl && g.nf == nf && g.ns == ns_max && g.tsize == (int)sizeof(T)) {
+                CK(cudaGraphLaunch(g.exec, E.st));
+                E.launches += g.launches;
+                return;
+            }
+        Engine::SweepGraph sg;
+        sg.dfl = dfl;
+        sg.nf = nf;
+        sg.ns = ns_max;
+        sg.tsize = (int)sizeof(T);
+        const long l0 = E.launches;
+        CK(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t graph = nullptr;
+        try {
+            emit();
+        } catch (...) {
+            cudaStreamEndCapture(E.st, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        CK(cudaStreamEndCapture(E.st, &graph));
+        cudaError_t ie = cudaGraphInstantiate(&sg.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(ie);
+        sg.launches = E.launches - l0;
+        if (E.graphs.size() >= 16) {
+            cudaGraphExecDestroy(E.graphs.front().exec);
+            E.graphs.erase(E.graphs.begin());
+        }
+        E.graphs.push_back(sg);
+        CK(cudaGraphLaunch(sg.exec, E.st));
     };
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 32 && b == 32 && c == 32) {
