@@ -153,6 +153,16 @@ struct Engine {
     double *d_part = nullptr;
     size_t d_part_len = 0;
     double *d_small = nullptr;   // scalars [n_inst][64]
+    // pinned host staging of per-instance scalars read back each Anderson
+    // iteration (one synchronisation per iteration): [n_inst][16] Q and
+    // Q_solvent, [n_inst][8] stress, [n_inst] free-energy terms, from
+    // n_inst*32 the Anderson sums
+    double *hpin = nullptr;
+    int hpin_inst = 0;
+    double *hq(int i) { return hpin + (size_t)i * 16; }
+    double *hst(int i) { return hpin + (size_t)hpin_inst * 16 + (size_t)i * 8; }
+    double *hfe() { return hpin + (size_t)hpin_inst * 24; }
+    double *hsm() { return hpin + (size_t)hpin_inst * 32; }
     void *spec = nullptr;        // 3-D stress spectra scratch
     void *fe_spec = nullptr;     // spectra for the star-weighted free energy
     size_t fe_spec_bytes = 0;
@@ -172,6 +182,7 @@ struct Engine {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+        if (hpin) cudaFreeHost(hpin);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -452,6 +463,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     }
     E.d_small = nullptr;
     CK(cudaMalloc(&E.d_small, sizeof(double) * 64 * n_inst));
+    CK(cudaMallocHost(&E.hpin, sizeof(double) * 128 * n_inst));
+    E.hpin_inst = n_inst;
     E.part((size_t)64 * n_inst * (PSCFG_MAXH + 2 * PSCFG_MAXM + 8) + 1024);
 }
 
@@ -876,7 +889,9 @@ static void split_prec(Engine &E, const std::vector<int> &act, std::vector<int> 
     for (int i : act) (E.inst[i].prec_now == PSCFG_FP32 ? a32 : a64).push_back(i);
 }
 
-static void density_all(Engine &E, const std::vector<int> &act)
+static void density_finish(Engine &E, const std::vector<int> &act);
+
+static void density_all(Engine &E, const std::vector<int> &act, bool finish = true)
 {
     std::vector<int> a64, a32;
     split_prec(E, act, a64, a32);
@@ -888,17 +903,29 @@ static void density_all(Engine &E, const std::vector<int> &act)
         E.cur = PSCFG_FP32;
         density_impl<float>(E, a32);
     }
-    // pull Q to the host (needed for mu and for the caller)
+    // pull Q to the host (needed for mu and for the caller), through the
+    // pinned staging buffer; finish = false leaves the synchronisation and
+    // density_finish to the caller
     for (int i : act) {
         Inst &I = E.inst[i];
-        CK(cudaMemcpyAsync(I.Q, I.Qdev, sizeof(double) * PSCFG_MAXC, cudaMemcpyDeviceToHost, E.st));
-        CK(cudaMemcpyAsync(I.Qs, I.Qsolv, sizeof(double) * PSCFG_MAXS, cudaMemcpyDeviceToHost, E.st));
-    }
-    CK(cudaStreamSynchronize(E.st));
-    for (int i : act) {
-        Inst &I = E.inst[i];
+        CK(cudaMemcpyAsync(E.hq(i), I.Qdev, sizeof(double) * PSCFG_MAXC, cudaMemcpyDeviceToHost, E.st));
+        CK(cudaMemcpyAsync(E.hq(i) + 8, I.Qsolv, sizeof(double) * PSCFG_MAXS, cudaMemcpyDeviceToHost, E.st));
         I.have_density = true;
         I.dens_prec = I.prec_now;
+    }
+    if (finish) {
+        CK(cudaStreamSynchronize(E.st));
+        density_finish(E, act);
+    }
+}
+
+// Q, Q_solvent from the staging buffer, then mu_phi_chain / mu_phi_solvent.
+static void density_finish(Engine &E, const std::vector<int> &act)
+{
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        std::memcpy(I.Q, E.hq(i), sizeof(double) * PSCFG_MAXC);
+        std::memcpy(I.Qs, E.hq(i) + 8, sizeof(double) * PSCFG_MAXS);
         // mu_phi_chain / mu_phi_solvent (src/scf_mod.fp.f90:768-820)
         for (int c = 0; c < I.sys.n_chain; c++) {
             if (I.sys.ensemble == 0) I.sys.mu_chain[c] = std::log(I.sys.phi_chain[c] / I.Q[c]);
@@ -1095,7 +1122,7 @@ static void stress_all(Engine &E, const std::vector<int> &act)
 // ---------------------------------------------------------------------
 // Field term sum_k w r [..] / nr^2 for instances with star weights, from
 // the spectra of rho and omega (FP64 forward FFTs).
-static void fe_spectral(Engine &E, const std::vector<int> &which, std::vector<double> &terms)
+static void fe_spectral(Engine &E, const std::vector<int> &which, double *hout)
 {
     const PlaneGeom &g = E.g64;
     const int M = E.M;
@@ -1107,7 +1134,6 @@ static void fe_spectral(Engine &E, const std::vector<int> &which, std::vector<do
         CK(cudaMalloc(&E.fe_spec, per * chunk));
         E.fe_spec_bytes = per * chunk;
     }
-    terms.assign(which.size(), 0.0);
     const int nct = red_ctas(E.nk);
     for (size_t c0 = 0; c0 < which.size(); c0 += chunk) {
         const int cn = (int)std::min<size_t>(chunk, which.size() - c0);
@@ -1164,24 +1190,32 @@ static void fe_spectral(Engine &E, const std::vector<int> &which, std::vector<do
         const double rn2 = (double)E.nr * (double)E.nr;
         k_final_sum<<<(unsigned)((cn + 127) / 128), 128, 0, E.st>>>(part, nct, rn2, E.d_small, cn);
         E.launched();
-        CK(cudaMemcpyAsync(terms.data() + c0, E.d_small, sizeof(double) * cn, cudaMemcpyDeviceToHost, E.st));
-        CK(cudaStreamSynchronize(E.st));
+        CK(cudaMemcpyAsync(hout + c0, E.d_small, sizeof(double) * cn, cudaMemcpyDeviceToHost, E.st));
     }
 }
 
-static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p)
+// Instances without star weights first (real-space field terms), then
+// those with star weights (spectral), in act order within each group.
+static void fe_partition(Engine &E, const std::vector<int> &act, std::vector<size_t> &pos_plain,
+                         std::vector<size_t> &pos_w)
 {
-    std::vector<int> plain, weighted;
+    for (size_t k = 0; k < act.size(); k++) (E.inst[act[k]].kweight ? pos_w : pos_plain).push_back(k);
+}
+
+static void fe_finish(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p);
+
+// Field terms of the free energy into the staging buffer; with finish, the
+// synchronisation and the assembly (fe_finish) follow.
+static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p,
+                            bool finish = true)
+{
     std::vector<size_t> pos_plain, pos_w;
-    for (size_t k = 0; k < act.size(); k++) {
-        if (E.inst[act[k]].kweight) { weighted.push_back(act[k]); pos_w.push_back(k); }
-        else { plain.push_back(act[k]); pos_plain.push_back(k); }
-    }
-    std::vector<double> terms(act.size(), 0.0);
-    if (!plain.empty()) {
+    fe_partition(E, act, pos_plain, pos_w);
+    double *hfe = E.hfe();
+    if (!pos_plain.empty()) {
         std::vector<FieldJob> fj;
-        for (int i : plain) {
-            Inst &I = E.inst[i];
+        for (size_t k : pos_plain) {
+            Inst &I = E.inst[act[k]];
             FieldJob j;
             std::memset(&j, 0, sizeof(j));
             j.omega = I.omega;
@@ -1198,16 +1232,29 @@ static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<
         E.launched();
         k_final_sum<<<(unsigned)((fj.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small, (int)fj.size());
         E.launched();
-        std::vector<double> t(fj.size());
-        CK(cudaMemcpyAsync(t.data(), E.d_small, sizeof(double) * fj.size(), cudaMemcpyDeviceToHost, E.st));
+        CK(cudaMemcpyAsync(hfe, E.d_small, sizeof(double) * fj.size(), cudaMemcpyDeviceToHost, E.st));
+    }
+    if (!pos_w.empty()) {
+        std::vector<int> weighted;
+        for (size_t k : pos_w) weighted.push_back(act[k]);
+        fe_spectral(E, weighted, hfe + pos_plain.size());
+    }
+    if (finish) {
         CK(cudaStreamSynchronize(E.st));
-        for (size_t k = 0; k < plain.size(); k++) terms[pos_plain[k]] = t[k];
+        fe_finish(E, act, f, p);
     }
-    if (!weighted.empty()) {
-        std::vector<double> t;
-        fe_spectral(E, weighted, t);
-        for (size_t k = 0; k < weighted.size(); k++) terms[pos_w[k]] = t[k];
-    }
+}
+
+// f_Helmholtz and pressure (src/scf_mod.fp.f90:834-886) from the staged
+// field terms and the host mu / phi.
+static void fe_finish(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p)
+{
+    std::vector<size_t> pos_plain, pos_w;
+    fe_partition(E, act, pos_plain, pos_w);
+    std::vector<double> terms(act.size(), 0.0);
+    const double *hfe = E.hfe();
+    for (size_t k = 0; k < pos_plain.size(); k++) terms[pos_plain[k]] = hfe[k];
+    for (size_t k = 0; k < pos_w.size(); k++) terms[pos_w[k]] = hfe[pos_plain.size() + k];
     f.assign(act.size(), 0.0);
     p.assign(act.size(), 0.0);
     for (size_t k = 0; k < act.size(); k++) {
@@ -1382,14 +1429,16 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
         const int na = (int)act.size();
         for (int i : act) st[i].itr++;
 
-        density_all(E, act);
+        // density, stress, free-energy terms and the Anderson sums are all
+        // enqueued first; their scalars come back through the pinned staging
+        // buffer with one synchronisation (below)
+        density_all(E, act, false);
         if (prm.domain) stress_all(E, act);
         std::vector<double> fe, pe;
-        free_energy_all(E, act, fe, pe);
-        std::vector<double> sh((size_t)na * PSCFG_MAXCP, 0.0);
+        free_energy_all(E, act, fe, pe, false);
         if (prm.domain) {
             for (int k = 0; k < na; k++)
-                CK(cudaMemcpyAsync(&sh[(size_t)k * PSCFG_MAXCP], E.inst[act[k]].stress_dev, sizeof(double) * PSCFG_MAXCP,
+                CK(cudaMemcpyAsync(E.hst(k), E.inst[act[k]].stress_dev, sizeof(double) * PSCFG_MAXCP,
                                    cudaMemcpyDeviceToHost, E.st));
         }
         // deviations into the ring slot of the current omega
@@ -1454,9 +1503,15 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
         k_final_sum<<<(unsigned)((na * (PSCFG_MAXH + 1) + 127) / 128), 128, 0, E.st>>>(dpart, nct, 1.0, dres,
                                                                                        na * (PSCFG_MAXH + 1));
         E.launched();
-        hsmall.resize((size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1));
-        CK(cudaMemcpyAsync(hsmall.data(), E.d_small, sizeof(double) * hsmall.size(), cudaMemcpyDeviceToHost, E.st));
+        const size_t nsm = (size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1);
+        CK(cudaMemcpyAsync(E.hsm(), E.d_small, sizeof(double) * nsm, cudaMemcpyDeviceToHost, E.st));
         CK(cudaStreamSynchronize(E.st));
+        density_finish(E, act);
+        fe_finish(E, act, fe, pe);
+        hsmall.assign(E.hsm(), E.hsm() + nsm);
+        std::vector<double> sh((size_t)na * PSCFG_MAXCP, 0.0);
+        if (prm.domain)
+            for (int k = 0; k < na; k++) std::memcpy(&sh[(size_t)k * PSCFG_MAXCP], E.hst(k), sizeof(double) * PSCFG_MAXCP);
 
         std::vector<AmMix> mixes;
         std::vector<int> mix_inst;
