@@ -363,9 +363,11 @@ struct PlaneStackR {
     }
 };
 
-// The five step kernels of the register-column variant (same algebra as
+// The step kernels of the register-column variant (same algebra as
 // k3c_fwd_pair / k3c_inv_mid / k3c_inv_final; spectra in natural y order,
-// z pass k3r_zconv<..., true>).  128 threads, PPC planes per CTA.
+// z pass k3s_zconv<..., true>).  128 threads, PPC planes per CTA.  They read
+// only exp(-w ds/4) and square it for exp(-w ds/2) (one table load less
+// per grid point; within an ulp of the tabulated value).
 template <typename T, int N1, int N2, int N3, int PPC>
 __global__ void __launch_bounds__(128, 4) k3r_fwd_pair(const SweepField<T> *fields, int t)
 {
@@ -378,8 +380,8 @@ __global__ void __launch_bounds__(128, 4) k3r_fwd_pair(const SweepField<T> *fiel
     const long nr = (long)N1 * N2 * N3;
     const int z0 = blockIdx.x * PPC;
     const T *q = src_slice(f, src, nr) + (long)z0 * PSk::NP;
-    const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP, *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
-    PSk::pack(buf, [&](int e) { return eo1[e] * q[e]; });
+    const T *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
+    PSk::pack(buf, [&](int e) { const T a = eo2[e]; return a * (a * q[e]); });
     PSk::forward_to(buf, f.S1 + (long)z0 * PSk::PS);
     __syncthreads();
     PSk::pack(buf, [&](int e) { return eo2[e] * q[e]; });
@@ -397,11 +399,11 @@ __global__ void __launch_bounds__(128, 4) k3r_inv_mid(const SweepField<T> *field
     cx<T> *buf = (cx<T> *)smem_raw;
     const T rn = (T)((long)N1 * N2 * N3);
     const int z0 = blockIdx.x * PPC;
-    const T *eo1 = f.eo1[blk] + (long)z0 * PSk::NP;
+    const T *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
     T *q1 = f.q1 + (long)z0 * PSk::NP;
     PSk::inverse_from(f.S1 + (long)z0 * PSk::PS, buf);
 #pragma unroll 4
-    for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) q1[e] = eo1[e] * PSk::real_at(buf, e) / rn;
+    for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) { const T a = eo2[e]; q1[e] = (a * a) * PSk::real_at(buf, e) / rn; }
     PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
     T *hout = f.h_out ? f.h_out + (long)z0 * PSk::NP : nullptr;
 
@@ -410,7 +412,7 @@ __global__ void __launch_bounds__(128, 4) k3r_inv_mid(const SweepField<T> *field
         const int p = i / (N2 * PSk::M), r = i % (N2 * PSk::M), y = r / PSk::M, m = r % PSk::M;
         const int e = p * PSk::NP + y * N1 + 2 * m;
         cx<T> &z = buf[p * PSk::PS + y * PSk::NH + m];
-        z = mk<T>(eo1[e] * z.x / rn, eo1[e + 1] * z.y / rn);
+        { const T a = eo2[e], c = eo2[e + 1]; z = mk<T>((a * a) * z.x / rn, (c * c) * z.y / rn); }
         if (hout) {
             hout[e] = z.x;
             hout[e + 1] = z.y;
@@ -658,12 +660,12 @@ __global__ void __launch_bounds__(128, 4) k3r_final_fwd(const SweepField<T> *fie
     int blk2, src2, dst2;
     if (!step_slices(f, t + 1, blk2, src2, dst2)) return;   // the same for the whole CTA
     __syncthreads();
-    const T *n1 = f.eo1[blk2] + (long)z0 * PSk::NP, *n2 = f.eo2[blk2] + (long)z0 * PSk::NP;
+    const T *n2 = f.eo2[blk2] + (long)z0 * PSk::NP;
 
 #pragma unroll 4
     for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) {
         T &slot = PSk::real_ref(buf, e);
-        slot = n1[e] * slot;
+        { const T a = n2[e]; slot = (a * a) * slot; }
     }
     PSk::forward_to(buf, f.S1 + (long)z0 * PSk::PS);
     __syncthreads();
