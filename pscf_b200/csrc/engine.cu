@@ -33,6 +33,7 @@
 #include "adjoint.cuh"
 #include "kernels3x.cuh"
 #include "response.cuh"
+#include "kernels3l.cuh"
 
 namespace pscfg {
 
@@ -127,6 +128,7 @@ struct Engine {
     bool smem_zconv = false;         // shared-memory z pass instead of register columns (PSCFG_SMEM_ZCONV=1)
     bool smem_fft = false;           // shared-memory x-y column passes (PSCFG_SMEM_FFT=1)
     bool no_graphs = false;          // launch the 3-D sweeps directly (PSCFG_NO_GRAPHS=1)
+    bool line_step = false;          // line-pass 3-D step even where the plane kernels fit (PSCFG_LINE_STEP=1)
     // CUDA graphs of 3-D sweeps, keyed by descriptor address, field and step count
     struct SweepGraph {
         const void *dfl;
@@ -410,6 +412,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         E.smem_fft = xy && xy[0] && xy[0] != '0';
         const char *ng = std::getenv("PSCFG_NO_GRAPHS");
         E.no_graphs = ng && ng[0] && ng[0] != '0';
+        const char *ls = std::getenv("PSCFG_LINE_STEP");
+        E.line_step = ls && ls[0] && ls[0] != '0';
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
@@ -617,6 +621,54 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
     return false;
 }
 
+// One 3-D MDE step as line passes (kernels3l.cuh), for grids with an even
+// n1 whose x-y plane (or z tile) does not fit the shared memory of the
+// whole-plane kernels (or with PSCFG_LINE_STEP=1).  Returns false if not
+// applicable.  (Where both fit, the whole-plane kernels measured as fast or
+// faster: C5-size 64 x 128 x 224 FP64 2.5k vs 2.7k steps/s, FP32 4.3k vs
+// 2.8k.)
+template <typename T>
+static bool step3l(Engine &E, const SweepField<T> *dfl, int nf, int t)
+{
+    if (E.n[0] % 2 != 0) return false;
+    const PlaneGeom &g = E.geom();
+    const size_t smxy_plane = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
+    const size_t smz_plane = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
+    const bool plane_fits = smxy_plane <= 227 * 1024 && smz_plane <= 227 * 1024;
+    if (plane_fits && !E.line_step) return false;
+    const int M = g.n1 / 2, NH = M + 1;
+    const long nrow = (long)g.n2 * g.n3;
+    const int TLr = l3_rows_per_cta<T>(M);
+    const unsigned gr = (unsigned)((nrow + TLr - 1) / TLr);
+    const size_t smr = 2 * (size_t)TLr * NH * sizeof(cx<T>);
+    auto lines_tl = [&](int L) { return std::max(1, std::min(32, (int)(65536 / (2 * L * (int)sizeof(cx<T>))))); };
+    const int TLy = lines_tl(g.n2), TLz = lines_tl(g.n3);
+    const unsigned gy = (unsigned)(((long)NH * g.n3 + TLy - 1) / TLy);
+    const unsigned gz = (unsigned)(((long)NH * g.n2 + TLz - 1) / TLz);
+    const size_t smy = 2 * (size_t)TLy * g.n2 * sizeof(cx<T>), smz = 2 * (size_t)TLz * g.n3 * sizeof(cx<T>);
+    CK(allow_dyn_smem((const void *)k3l_rows<T, 0>));
+    CK(allow_dyn_smem((const void *)k3l_rows<T, 1>));
+    CK(allow_dyn_smem((const void *)k3l_rows<T, 2>));
+    CK(allow_dyn_smem((const void *)k3l_lines<T>));
+    auto yz = [&](int which, int nz) {
+        k3l_lines<T><<<dim3(gy, nf, nz), L3_THREADS, smy, E.st>>>(dfl, g, t, 1, 0, which, TLy);
+        E.launched();
+        k3l_lines<T><<<dim3(gz, nf, nz), L3_THREADS, smz, E.st>>>(dfl, g, t, 2, 2, which, TLz);
+        E.launched();
+        k3l_lines<T><<<dim3(gy, nf, nz), L3_THREADS, smy, E.st>>>(dfl, g, t, 1, 1, which, TLy);
+        E.launched();
+    };
+    k3l_rows<T, 0><<<dim3(gr, nf, 2), L3_THREADS, smr, E.st>>>(dfl, g, t, TLr);
+    E.launched();
+    yz(3, 2);
+    k3l_rows<T, 1><<<dim3(gr, nf, 2), L3_THREADS, smr, E.st>>>(dfl, g, t, TLr);
+    E.launched();
+    yz(2, 1);
+    k3l_rows<T, 2><<<dim3(gr, nf, 1), L3_THREADS, smr, E.st>>>(dfl, g, t, TLr);
+    E.launched();
+    return true;
+}
+
 // Returns true if the grid has a compile-time-shaped step (and runs it).
 template <typename T>
 static bool step3_fixed(Engine &E, const SweepField<T> *dfl, int nf, int t)
@@ -716,7 +768,8 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
     } else {
         size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
         size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
-        if (smxy > 227 * 1024 || smz > 227 * 1024) throw Err(PSCFG_EINVAL, "grid plane too large");
+        if ((smxy > 227 * 1024 || smz > 227 * 1024) && E.n[0] % 2 != 0)
+            throw Err(PSCFG_EINVAL, "grid plane too large for the whole-plane kernels (odd n1)");
         CK(allow_dyn_smem((const void *)k3_fwd_pair<T>));
         CK(allow_dyn_smem((const void *)k3_inv_mid<T>));
         CK(allow_dyn_smem((const void *)k3_inv_final<T>));
@@ -727,6 +780,7 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
         if (sweep3r<T>(E, dfl, nf, ns_max)) return;
         for (int t = 0; t < ns_max; t++) {
             if (step3_fixed<T>(E, dfl, nf, t)) continue;
+            if (step3l<T>(E, dfl, nf, t)) continue;
             k3_fwd_pair<T><<<dim3(g.n3, nf), txy, smxy, E.st>>>(dfl, g, t);
             E.launched();
             k3_zconv<T, Z_TILE><<<dim3(ntile, nf, 2), tz, smz, E.st>>>(dfl, g, t, 3);
@@ -1717,7 +1771,7 @@ static void run_single_steps(Engine &E, const SweepField<T> *dfl, int nf)
         int threads = (int)std::min<long>(256, std::max<long>(32, ((nr / 2 + 31) / 32) * 32));
         k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, 1);
         E.launched();
-    } else if (!step3_fixed<T>(E, dfl, nf, 0)) {
+    } else if (!step3_fixed<T>(E, dfl, nf, 0) && !step3l<T>(E, dfl, nf, 0)) {
         size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
         size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<T>);
         CK(allow_dyn_smem((const void *)k3_fwd_pair<T>));

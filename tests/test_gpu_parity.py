@@ -256,3 +256,51 @@ def test_sweep_graph_replay_matches_direct_launches(monkeypatch):
     for x, y in zip(a[:4], b[:4]):
         assert np.array_equal(x, y)
     assert a[4] == b[4] and a[5] == b[5]
+
+
+@pytest.mark.parametrize("ngrid,crystal,cell", [([12, 20, 28], "orthorhombic", [1.5, 2.0, 2.5]),
+                                                ([16, 30, 14], "orthorhombic", [1.6, 2.4, 1.4]),
+                                                ([24, 24, 24], "cubic", [2.0])])
+def test_line_pass_step_matches_plane_step(ngrid, crystal, cell, monkeypatch):
+    """The line-pass 3-D step (any even n1 with 2,3,5,7-smooth extents; used
+    where the x-y plane does not fit shared memory) agrees with the
+    whole-plane kernels: propagation, density, stress, and the FP32 path."""
+    s = diblock(3, ngrid, crystal, cell, fA=0.3, ds=0.05)
+    w = omega_guess(s, 12, 2.0)
+    wf = 7.0 + smooth_field(s, 13, 2.0)
+    q0 = 1.0 + 0.3 * smooth_field(s, 14, 1.0)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("PSCFG_LINE_STEP", flag)
+        e = Engine([s], FP64)
+        p = e.propagate(0, wf, 1.0, 0.01, q0, 3)
+        rho, q = e.density(w[None])
+        st = e.scf_stress()[0, :len(cell)]
+        e.close()
+        e32 = Engine([s], FP32)
+        rho32, _ = e32.density(w[None])
+        e32.close()
+        out[flag] = (p, rho, q[:, :1], st, rho32)
+    a, b = out["0"], out["1"]
+    assert rel_err(a[0], b[0]) < 1e-13
+    assert rel_err(a[1], b[1]) < 1e-13 and rel_err(a[2], b[2]) < 1e-13
+    assert np.max(np.abs(a[3] - b[3])) < 1e-11 * max(1.0, np.max(np.abs(b[3])))
+    assert rel_err(a[4], b[4]) < 1e-5
+
+
+def test_large_plane_density_uses_line_passes():
+    """A grid whose x-y plane does not fit the shared memory of the
+    whole-plane kernels (256 x 128 spectral plane, 528 KB) runs on the line
+    passes and matches the oracle's propagators and density."""
+    s = diblock(3, [256, 128, 4], "orthorhombic", [4.0, 3.0, 0.5], fA=0.4, chiN=12.0, ds=0.1)
+    w = omega_guess(s, 15, 2.0)
+    o = O.Oracle(s)
+    rho_ref, q_ref = o.density(w)
+    e = Engine([s], FP64)
+    rho, q = e.density(w[None])
+    assert rel_err(q[0, :1], q_ref) < 1e-12
+    assert rel_err(rho[0], rho_ref) < 1e-12
+    qf_ref, _ = o.propagators(0)
+    qf, _ = e.propagators(0, 0)
+    assert rel_err(qf, qf_ref) < 1e-12
+    e.close()
