@@ -1049,12 +1049,68 @@ static bool stress3_fixed(Engine &E, const StressJob<T> *dj, int s0, int cnt)
 
 // Per slice s of every job: inc[s][b] = sum_k wdgsq_b(k) Re(F[qf_s] conj F[qr_s])
 // on the half spectrum (the stress slice sums; also the adjoint's cell pairs).
+// All jobs of slice_dots in batched launches with the register-column
+// kernels (16^3, 32^3).  Returns false where they do not apply.
+template <typename T>
+static bool slice_dots_r(Engine &E, const StressJob<T> *dj, int njobs, int maxs)
+{
+    if (E.no_fixed_kernels || E.smem_fft || E.dim != 3) return false;
+    auto run = [&](auto n1c, auto ppcc) {
+        constexpr int N = decltype(n1c)::value, PPC = decltype(ppcc)::value;
+        constexpr int P = N * (N / 2 + 1);
+        const int ntile = (P + 63) / 64;
+        const size_t per_slice = 2 * (size_t)E.nk * sizeof(cx<T>);
+        const int cs = (int)std::max<size_t>(1, std::min<size_t>((size_t)maxs, ((size_t)1 << 30) / (per_slice * njobs)));
+        if (E.spec_bytes < per_slice * cs * njobs) {
+            if (E.spec) cudaFree(E.spec);
+            E.spec = nullptr;
+            CK(cudaMalloc(&E.spec, per_slice * cs * njobs));
+            E.spec_bytes = per_slice * cs * njobs;
+        }
+        const size_t plen = (size_t)cs * njobs * ntile * PSCFG_MAXCP;
+        if (E.stress_part_len < plen) {
+            if (E.stress_part) cudaFree(E.stress_part);
+            E.stress_part = nullptr;
+            CK(cudaMalloc(&E.stress_part, plen * sizeof(double)));
+            E.stress_part_len = plen;
+        }
+        const size_t sm = sizeof(cx<T>) * PPC * P;
+        CK(allow_dyn_smem((const void *)k3r_stress_xy_b<T, N, N, N, PPC>));
+        for (int s0 = 0; s0 < maxs; s0 += cs) {
+            const int cnt = std::min(cs, maxs - s0);
+            k3r_stress_xy_b<T, N, N, N, PPC><<<dim3(N / PPC, cnt, 2 * njobs), 128, sm, E.st>>>(dj, s0, cs, (cx<T> *)E.spec);
+            E.launched();
+            k3s_stress_z_b<T, N, N, N><<<dim3(ntile, cnt, njobs), 128, 0, E.st>>>(dj, s0, cs, (const cx<T> *)E.spec,
+                                                                                   E.stress_part);
+            E.launched();
+            k3_stress_sum_b<T><<<dim3(cnt, njobs), 32, 0, E.st>>>(dj, s0, cs, ntile, E.stress_part);
+            E.launched();
+        }
+    };
+    const int a = E.n[0], b = E.n[1], c = E.n[2];
+    if (2 * njobs > 65535) return false;
+    if (a == 32 && b == 32 && c == 32) {
+        run(std::integral_constant<int, 32>(), std::integral_constant<int, 4>());
+        return true;
+    }
+    if (a == 16 && b == 16 && c == 16) {
+        run(std::integral_constant<int, 16>(), std::integral_constant<int, 8>());
+        return true;
+    }
+    return false;
+}
+
 template <typename T>
 static void slice_dots(Engine &E, const std::vector<StressJob<T>> &jobs)
 {
     const PlaneGeom &g = E.geom();
     if (jobs.empty()) return;
     StressJob<T> *dj = E.upload(jobs, 0);
+    {
+        int maxs = 0;
+        for (auto &j : jobs) maxs = std::max(maxs, j.nslices);
+        if (slice_dots_r<T>(E, dj, (int)jobs.size(), maxs)) return;
+    }
     size_t off = ((jobs.size() * sizeof(StressJob<T>) + 255) / 256) * 256;
     if (E.dim <= 2) {
         int maxs = 0;

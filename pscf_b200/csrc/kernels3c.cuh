@@ -802,6 +802,94 @@ __global__ void __launch_bounds__(128) k3s_stress_z(const StressJob<T> *job, int
     }
 }
 
+// Batched forms of the register-column stress pass: all jobs of a call in
+// one launch per pass (job = blockIdx.z [/ 2]), cs slices from s0 each;
+// spectra at ((job cs + slice) 2 + which) nk, partial sums at
+// ((job cs + slice) ntiles + tile) PSCFG_MAXCP.
+template <typename T, int N1, int N2, int N3, int PPC>
+__global__ void __launch_bounds__(128, 4) k3r_stress_xy_b(const StressJob<T> *jobs, int s0, int cs, cx<T> *spec)
+{
+    using PSk = PlaneStackR<T, N1, N2, PPC>;
+    const int job = blockIdx.z >> 1, which = blockIdx.z & 1;
+    const StressJob<T> &J = jobs[job];
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3, nk = (long)PSk::PS * N3;
+    const int z0 = blockIdx.x * PPC;
+    const T *q = (which == 0 ? J.qf : J.qr) + (long)s * nr + (long)z0 * PSk::NP;
+    PSk::pack(buf, [&](int e) { return q[e]; });
+    PSk::forward_to(buf, spec + (((long)job * cs + blockIdx.y) * 2 + which) * nk + (long)z0 * PSk::PS);
+}
+
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(128) k3s_stress_z_b(const StressJob<T> *jobs, int s0, int cs, const cx<T> *spec,
+                                                      double *part)
+{
+    constexpr int NH = N1 / 2 + 1, P = N2 * NH, H = N3 / 2;
+    const int job = blockIdx.z;
+    const StressJob<T> &J = jobs[job];
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    __shared__ __align__(16) cx<T> X[4][N3][16];
+    __shared__ double red[32];
+    const long nk = (long)P * N3;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, h = lane >> 4, c = lane & 15;
+    const int col = (blockIdx.x * 4 + w) * 16 + c;
+    const bool ok = col < P;
+    const cx<T> *sf = spec + (((long)job * cs + blockIdx.y) * 2) * nk + (ok ? col : 0), *sr = sf + nk;
+    auto ztrans = [&](const cx<T> *src, cx<T> *v) {
+#pragma unroll
+        for (int j = 0; j < H; j++) v[j] = ok ? src[(long)(2 * j + h) * P] : mk<T>((T)0, (T)0);
+        RegDft<H, -1, T>::run(v);
+#pragma unroll
+        for (int k = 0; k < H; k++) X[w][h * H + k][c] = (h && k) ? cmul(v[k], twc<T>(N3, k)) : v[k];
+        __syncwarp();
+#pragma unroll
+        for (int k = 0; k < H; k++) {
+            const cx<T> a = X[w][k][c], b = X[w][H + k][c];
+            v[k] = h ? a - b : a + b;
+        }
+        __syncwarp();
+    };
+    cx<T> fv[H], rv[H];
+    ztrans(sf, fv);
+    ztrans(sr, rv);
+    double acc[PSCFG_MAXCP] = {0, 0, 0, 0, 0, 0};
+    if (ok) {
+        const double *wp = J.wdgsq + col + (long)h * H * P;
+#pragma unroll 1
+        for (int b = 0; b < J.ncp; b++) {
+            double a = 0.0;
+#pragma unroll
+            for (int k = 0; k < H; k++)
+                a += __ldg(wp + (long)b * nk + (long)k * P) *
+                     ((double)fv[k].x * (double)rv[k].x + (double)fv[k].y * (double)rv[k].y);
+            acc[b] = a;
+        }
+    }
+    for (int b = 0; b < J.ncp; b++) {
+        const double tot = block_sum(acc[b], red);
+        if (threadIdx.x == 0)
+            part[(((long)job * cs + blockIdx.y) * gridDim.x + blockIdx.x) * PSCFG_MAXCP + b] = tot;
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void k3_stress_sum_b(const StressJob<T> *jobs, int s0, int cs, int ntiles, const double *part)
+{
+    const int job = blockIdx.y;
+    const StressJob<T> &J = jobs[job];
+    const int s = s0 + blockIdx.x;
+    if (s >= J.nslices || threadIdx.x >= J.ncp) return;
+    const int b = threadIdx.x;
+    double acc = 0.0;
+    for (int t = 0; t < ntiles; t++) acc += part[(((long)job * cs + blockIdx.x) * ntiles + t) * PSCFG_MAXCP + b];
+    J.inc[(long)s * PSCFG_MAXCP + b] = acc;
+}
+
 // Pass 2: z-forward of both spectra on TC columns and the weighted dot
 // products sum_k wdgsq_b(k) Re(F conj R).  grid = (ntiles, cs).
 template <typename T, int N1, int N2, int N3, int TC>
