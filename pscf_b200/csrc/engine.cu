@@ -176,6 +176,7 @@ struct Engine {
     {
         for (void *p : allocs) cudaFree(p);
         if (d_desc) cudaFree(d_desc);
+        for (void *p : desc_retired) cudaFree(p);
         if (d_part) cudaFree(d_part);
         if (d_small) cudaFree(d_small);
         if (spec) cudaFree(spec);
@@ -202,10 +203,14 @@ struct Engine {
     size_t tsize() const { return prec == PSCFG_FP32 ? sizeof(float) : sizeof(double); }
     const PlaneGeom &geom() const { return cur == PSCFG_FP32 ? g32 : g64; }
 
+    // Growing the descriptor scratch retires the old buffer instead of
+    // freeing it: descriptors uploaded earlier in the same host sequence may
+    // still be waiting for their launches.  Retired buffers (a geometric
+    // series, so at most about the final size) are freed with the engine.
     void *desc(size_t bytes)
     {
         if (bytes > d_desc_bytes) {
-            if (d_desc) cudaFree(d_desc);
+            if (d_desc) desc_retired.push_back(d_desc);
             d_desc = nullptr;
             size_t nb = std::max(bytes + bytes / 2, (size_t)16 << 20);
             CK(cudaMalloc(&d_desc, nb));
@@ -213,6 +218,7 @@ struct Engine {
         }
         return d_desc;
     }
+    std::vector<void *> desc_retired;
     // upload host descriptors into a sub-range of the descriptor scratch
     template <typename D>
     D *upload(const std::vector<D> &v, size_t offset_bytes)
