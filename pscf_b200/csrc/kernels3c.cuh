@@ -249,7 +249,7 @@ struct PlaneStackR {
     template <typename F>
     __device__ __forceinline__ static void pack(cx<T> *buf, F value)
     {
-#pragma unroll 4
+#pragma unroll 16
         for (int i = threadIdx.x; i < PPC * N2 * M; i += KT) {
             const int p = i / (N2 * M), r = i % (N2 * M), y = r / M, m = r % M;
             const int e = p * NP + y * N1 + 2 * m;
@@ -402,12 +402,12 @@ __global__ void __launch_bounds__(128, 4) k3r_inv_mid(const SweepField<T> *field
     const T *eo2 = f.eo2[blk] + (long)z0 * PSk::NP;
     T *q1 = f.q1 + (long)z0 * PSk::NP;
     PSk::inverse_from(f.S1 + (long)z0 * PSk::PS, buf);
-#pragma unroll 4
+#pragma unroll 16
     for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) { const T a = eo2[e]; q1[e] = (a * a) * PSk::real_at(buf, e) / rn; }
     PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
     T *hout = f.h_out ? f.h_out + (long)z0 * PSk::NP : nullptr;
 
-#pragma unroll 4
+#pragma unroll 16
     for (int i = threadIdx.x; i < PPC * N2 * PSk::M; i += PSk::KT) {
         const int p = i / (N2 * PSk::M), r = i % (N2 * PSk::M), y = r / PSk::M, m = r % PSk::M;
         const int e = p * PSk::NP + y * N1 + 2 * m;
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(128, 4) k3r_inv_final(const SweepField<T> *fie
     T *q2o = f.q2_out ? f.q2_out + (long)z0 * PSk::NP : nullptr;
     PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
 
-#pragma unroll 4
+#pragma unroll 16
     for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) {
         const T q2 = eo2[e] * PSk::real_at(buf, e) / rn;
         out[e] = ((T)4 * q2 - q1[e]) / (T)3;
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(128, 4) k3r_final_fwd(const SweepField<T> *fie
     T *out = dst_slice(f, dst, nr) + (long)z0 * PSk::NP;
     PSk::inverse_from(f.S2 + (long)z0 * PSk::PS, buf);
 
-#pragma unroll 4
+#pragma unroll 16
     for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) {
         T &slot = PSk::real_ref(buf, e);
         const T q2 = eo2[e] * slot / rn;
@@ -662,7 +662,7 @@ __global__ void __launch_bounds__(128, 4) k3r_final_fwd(const SweepField<T> *fie
     __syncthreads();
     const T *n2 = f.eo2[blk2] + (long)z0 * PSk::NP;
 
-#pragma unroll 4
+#pragma unroll 16
     for (int e = threadIdx.x; e < PPC * PSk::NP; e += PSk::KT) {
         T &slot = PSk::real_ref(buf, e);
         { const T a = n2[e]; slot = (a * a) * slot; }
