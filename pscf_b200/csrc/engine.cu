@@ -129,6 +129,7 @@ struct Engine {
     bool smem_fft = false;           // shared-memory x-y column passes (PSCFG_SMEM_FFT=1)
     bool no_graphs = false;          // launch the 3-D sweeps directly (PSCFG_NO_GRAPHS=1)
     bool line_step = false;          // line-pass 3-D step even where the plane kernels fit (PSCFG_LINE_STEP=1)
+    int planes = 0;                  // planes per CTA of the register sweep, 0 = by launch size (PSCFG_PLANES)
     // CUDA graphs of 3-D sweeps, keyed by descriptor address, field and step count
     struct SweepGraph {
         const void *dfl;
@@ -420,6 +421,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         E.no_graphs = ng && ng[0] && ng[0] != '0';
         const char *ls = std::getenv("PSCFG_LINE_STEP");
         E.line_step = ls && ls[0] && ls[0] != '0';
+        const char *pl = std::getenv("PSCFG_PLANES");
+        E.planes = pl ? std::atoi(pl) : 0;
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
@@ -545,6 +548,24 @@ static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
     E.launched();
 }
 
+// Planes per CTA of the register sweep for nf fields of an n3-plane grid: the
+// largest power of two up to pmax whose x-y launches still have 512 CTAs or
+// more (the register limit allows 4 CTAs on each of the 148 SMs, 592 slots).
+// Few fields (one or a few instances) take fewer planes per CTA so that more
+// SMs share the work: at 32^3, 20 Anderson iterations of one BCC instance
+// sweep in 61 ms with one plane per CTA against 107 ms with four, while 64
+// instances are fastest with four (465 ms against 473 with two).
+static int sweep_planes(const Engine &E, int nf, int n3, int pmax)
+{
+    if (E.planes > 0) {
+        for (int p = pmax; p >= 1; p /= 2)
+            if (E.planes == p) return p;
+    }
+    int p = pmax;
+    while (p > 1 && (long)nf * (n3 / p) < 512) p /= 2;
+    return p;
+}
+
 // A whole 3-D sweep with the register-column kernels, the last kernel of
 // every step fused with the first of the next.  Returns false where the
 // grid has no such kernels (or another path was requested).
@@ -617,11 +638,22 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
     };
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 32 && b == 32 && c == 32) {
-        run(std::integral_constant<int, 32>(), std::integral_constant<int, 4>());
+        using N = std::integral_constant<int, 32>;
+        switch (sweep_planes(E, nf, 32, 4)) {
+        case 4: run(N(), std::integral_constant<int, 4>()); break;
+        case 2: run(N(), std::integral_constant<int, 2>()); break;
+        default: run(N(), std::integral_constant<int, 1>()); break;
+        }
         return true;
     }
     if (a == 16 && b == 16 && c == 16) {
-        run(std::integral_constant<int, 16>(), std::integral_constant<int, 8>());
+        using N = std::integral_constant<int, 16>;
+        switch (sweep_planes(E, nf, 16, 8)) {
+        case 8: run(N(), std::integral_constant<int, 8>()); break;
+        case 4: run(N(), std::integral_constant<int, 4>()); break;
+        case 2: run(N(), std::integral_constant<int, 2>()); break;
+        default: run(N(), std::integral_constant<int, 1>()); break;
+        }
         return true;
     }
     return false;

@@ -258,6 +258,29 @@ def test_sweep_graph_replay_matches_direct_launches(monkeypatch):
     assert a[4] == b[4] and a[5] == b[5]
 
 
+@pytest.mark.parametrize("n,choices", [(32, ("4", "2", "1")), (16, ("8", "4", "2", "1"))])
+def test_sweep_planes_per_cta_agree(n, choices, monkeypatch):
+    """The register sweep with any number of x-y planes per CTA (chosen by
+    launch size: fewer planes for few instances) gives bit-identical
+    propagators and densities; every field, row and column is transformed by
+    the same arithmetic whatever CTA holds it."""
+    s = diblock(3, [n, n, n], "cubic", [1.95 * n / 32], fA=0.3, ds=0.02)
+    ws = np.stack([omega_guess(s, 30 + i, 2.0) for i in range(2)])
+    out = {}
+    for p in choices:
+        monkeypatch.setenv("PSCFG_PLANES", p)
+        e = Engine([s, s], FP64)
+        rho, q = e.density(ws)
+        st = e.scf_stress()
+        fh, fp, _ = e.free_energy()
+        out[p] = (rho, q, st, fh, fp)
+        e.close()
+    ref = out[choices[0]]
+    for p in choices[1:]:
+        for x, y in zip(out[p], ref):
+            assert np.array_equal(x, y), p
+
+
 @pytest.mark.parametrize("ngrid,crystal,cell", [([12, 20, 28], "orthorhombic", [1.5, 2.0, 2.5]),
                                                 ([16, 30, 14], "orthorhombic", [1.6, 2.4, 1.4]),
                                                 ([24, 24, 24], "cubic", [2.0])])
