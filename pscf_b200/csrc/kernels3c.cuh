@@ -243,6 +243,16 @@ struct PlaneStackR {
     using Base = PlaneStack<T, N1, N2, PPC>;
 
     static constexpr int KT = 128;   // threads per CTA of the kernels using this stack
+    // column passes: 16 columns per warp (two lanes each).  Columns kx = 0
+    // and kx = M are real after the row pass and can be transformed together
+    // as one complex column; that is done where it saves a round of the
+    // warps (4 planes of 32 x 32: 68 -> 64 columns), not where it only
+    // adds the separation step.
+    static constexpr int WARPS = KT / 32;
+    static constexpr bool PACK =
+        ((PPC * NH + 15) / 16 + WARPS - 1) / WARPS > ((PPC * M + 15) / 16 + WARPS - 1) / WARPS;
+    static constexpr int CW = PACK ? M : NH;   // column tasks per plane
+    static_assert(!PACK || 16 % M == 0, "packed column tasks must tile the 16-task warp blocks");
 
     // packed rows z[m] = f(2m) + i f(2m+1); compile-time stride so that the
     // loads of several iterations are in flight together
@@ -284,27 +294,56 @@ struct PlaneStackR {
         }
         __syncthreads();
         // columns, two lanes per column (lanes c and c+16 of a warp):
-        // decimation in time, the halves meet in place in buf
-        constexpr int H = N2 / 2, NCB = (PPC * NH + 15) / 16;
+        // decimation in time, the halves meet in place in buf.  With PACK,
+        // task kx = 0 transforms x0 + i xM and separates the two columns
+        // afterwards by Hermitian symmetry.
+        constexpr int H = N2 / 2, NC = PPC * CW, NCB = (NC + 15) / 16;
         const int h = (threadIdx.x >> 4) & 1, cl = threadIdx.x & 15;
-        for (int cb = threadIdx.x >> 5; cb < NCB; cb += blockDim.x >> 5) {
+        for (int cb = threadIdx.x >> 5; cb < NCB; cb += KT >> 5) {
             const int c = cb * 16 + cl;
-            const bool ok = c < PPC * NH;
-            const int off = ok ? (c / NH) * PS + (c % NH) : 0;
+            const bool ok = c < NC;
+            const int kx = ok ? c % CW : 1;
+            const int off = ok ? (c / CW) * PS + kx : 0;
+            const bool pk = PACK && ok && kx == 0;
             cx<T> v[H];
             if (ok) {
 #pragma unroll
-                for (int j = 0; j < H; j++) v[j] = buf[off + (2 * j + h) * NH];
+                for (int j = 0; j < H; j++) {
+                    v[j] = buf[off + (2 * j + h) * NH];
+                    if (pk) v[j] = mk<T>(v[j].x, buf[off + M + (2 * j + h) * NH].x);
+                }
                 RegDft<H, -1, T>::run(v);
 #pragma unroll
                 for (int k = 0; k < H; k++) buf[off + (2 * k + h) * NH] = (h && k) ? cmul(v[k], twc<T>(N2, k)) : v[k];
             }
             __syncwarp();
             if (ok) {
+                // the packed task parks its transform in column M (read by
+                // both of its lanes before the previous __syncwarp)
 #pragma unroll
                 for (int k = 0; k < H; k++) {
                     const cx<T> a = buf[off + 2 * k * NH], b = buf[off + (2 * k + 1) * NH];
-                    dst[off + (k + h * H) * NH] = h ? a - b : a + b;
+                    const cx<T> r = h ? a - b : a + b;
+                    if (pk)
+                        buf[off + M + (k + h * H) * NH] = r;
+                    else
+                        dst[off + (k + h * H) * NH] = r;
+                }
+            }
+            __syncwarp();
+            if (PACK) {
+                // separation of the block's packed columns, one (column, ky)
+                // per lane: X0[ky] = (Z[ky] + conj Z[-ky]) / 2,
+                // XM[ky] = (Z[ky] - conj Z[-ky]) / 2i
+                constexpr int PB = 16 / M;   // packed columns per block of 16 tasks
+                for (int l = threadIdx.x & 31; l < PB * N2; l += 32) {
+                    const int p = (cb * 16) / M + l / N2, ky = l % N2;
+                    if (p < PPC) {
+                        const int o = p * PS;
+                        const cx<T> z = buf[o + M + ky * NH], zm = conjg(buf[o + M + ((N2 - ky) % N2) * NH]);
+                        dst[o + ky * NH] = scale(z + zm, (T)0.5);
+                        dst[o + M + ky * NH] = scale(mul_si<-1>(z - zm), (T)0.5);
+                    }
                 }
             }
             __syncwarp();
@@ -319,16 +358,23 @@ struct PlaneStackR {
         // columns, two lanes per column: each lane brings its spectrum half
         // into buf, then decimation in frequency; lane half h ends with the
         // samples y = 2m + h
-        constexpr int H = N2 / 2, NCB = (PPC * NH + 15) / 16;
+        // (with PACK, columns kx = 0 and M, Hermitian in ky, go together as
+        // one complex column X0 + i XM whose transform is x0 + i xM)
+        constexpr int H = N2 / 2, NC = PPC * CW, NCB = (NC + 15) / 16;
         const int h = (threadIdx.x >> 4) & 1, cl = threadIdx.x & 15;
-        for (int cb = threadIdx.x >> 5; cb < NCB; cb += blockDim.x >> 5) {
+        for (int cb = threadIdx.x >> 5; cb < NCB; cb += KT >> 5) {
             const int c = cb * 16 + cl;
-            const bool ok = c < PPC * NH;
-            const int off = ok ? (c / NH) * PS + (c % NH) : 0;
+            const bool ok = c < NC;
+            const int kx = ok ? c % CW : 1;
+            const int off = ok ? (c / CW) * PS + kx : 0;
+            const bool pk = PACK && ok && kx == 0;
             cx<T> v[H];
             if (ok) {
 #pragma unroll
-                for (int k = 0; k < H; k++) buf[off + (k + h * H) * NH] = src[off + (k + h * H) * NH];
+                for (int k = 0; k < H; k++) {
+                    const int e = off + (k + h * H) * NH;
+                    buf[e] = pk ? src[e] + mul_si<1>(src[e + M]) : src[e];
+                }
             }
             __syncwarp();
             if (ok) {
@@ -342,7 +388,14 @@ struct PlaneStackR {
             if (ok) {
                 RegDft<H, 1, T>::run(v);
 #pragma unroll
-                for (int m = 0; m < H; m++) buf[off + (2 * m + h) * NH] = v[m];
+                for (int m = 0; m < H; m++) {
+                    if (pk) {
+                        buf[off + (2 * m + h) * NH] = mk<T>(v[m].x, (T)0);
+                        buf[off + M + (2 * m + h) * NH] = mk<T>(v[m].y, (T)0);
+                    } else {
+                        buf[off + (2 * m + h) * NH] = v[m];
+                    }
+                }
             }
         }
         __syncthreads();
