@@ -156,6 +156,7 @@ struct Engine {
     double *d_part = nullptr;
     size_t d_part_len = 0;
     double *d_small = nullptr;   // scalars [n_inst][64]
+    double *dstage = nullptr;    // device twin of hpin: per-instance scalars gathered for one copy
     // pinned host staging of per-instance scalars read back each Anderson
     // iteration (one synchronisation per iteration): [n_inst][16] Q and
     // Q_solvent, [n_inst][8] stress, [n_inst] free-energy terms, from
@@ -180,6 +181,7 @@ struct Engine {
         for (void *p : desc_retired) cudaFree(p);
         if (d_part) cudaFree(d_part);
         if (d_small) cudaFree(d_small);
+        if (dstage) cudaFree(dstage);
         if (spec) cudaFree(spec);
         if (fe_spec) cudaFree(fe_spec);
         if (stress_part) cudaFree(stress_part);
@@ -477,6 +479,7 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     E.d_small = nullptr;
     CK(cudaMalloc(&E.d_small, sizeof(double) * 64 * n_inst));
     CK(cudaMallocHost(&E.hpin, sizeof(double) * 128 * n_inst));
+    CK(cudaMalloc(&E.dstage, sizeof(double) * 128 * n_inst));
     E.hpin_inst = n_inst;
     E.part((size_t)64 * n_inst * (PSCFG_MAXH + 2 * PSCFG_MAXM + 8) + 1024);
 }
@@ -983,6 +986,20 @@ static void split_prec(Engine &E, const std::vector<int> &act, std::vector<int> 
 
 static void density_finish(Engine &E, const std::vector<int> &act);
 
+// One launch for a list of device copies (descriptors in their own
+// region of the descriptor scratch).
+static void copy_list(Engine &E, const std::vector<CopyJob> &jobs, long maxn)
+{
+    const unsigned gx = (unsigned)std::max<long>(1, std::min<long>((maxn + 255) / 256, 64));
+    for (size_t j0 = 0; j0 < jobs.size(); j0 += 65535) {
+        const size_t cnt = std::min<size_t>(65535, jobs.size() - j0);
+        std::vector<CopyJob> part(jobs.begin() + j0, jobs.begin() + j0 + cnt);
+        CopyJob *dj = E.upload(part, E.geom_off + ((size_t)2 << 20));
+        k_copy_list<<<dim3(gx, (unsigned)cnt), 256, 0, E.st>>>(dj);
+        E.launched();
+    }
+}
+
 static void density_all(Engine &E, const std::vector<int> &act, bool finish = true)
 {
     std::vector<int> a64, a32;
@@ -995,16 +1012,19 @@ static void density_all(Engine &E, const std::vector<int> &act, bool finish = tr
         E.cur = PSCFG_FP32;
         density_impl<float>(E, a32);
     }
-    // pull Q to the host (needed for mu and for the caller), through the
-    // pinned staging buffer; finish = false leaves the synchronisation and
-    // density_finish to the caller
+    // pull Q to the host (needed for mu and for the caller): gathered on the
+    // device, one copy into the pinned staging buffer; finish = false leaves
+    // the synchronisation and density_finish to the caller
+    std::vector<CopyJob> cj;
     for (int i : act) {
         Inst &I = E.inst[i];
-        CK(cudaMemcpyAsync(E.hq(i), I.Qdev, sizeof(double) * PSCFG_MAXC, cudaMemcpyDeviceToHost, E.st));
-        CK(cudaMemcpyAsync(E.hq(i) + 8, I.Qsolv, sizeof(double) * PSCFG_MAXS, cudaMemcpyDeviceToHost, E.st));
+        cj.push_back(CopyJob{I.Qdev, E.dstage + (size_t)i * 16, PSCFG_MAXC});
+        cj.push_back(CopyJob{I.Qsolv, E.dstage + (size_t)i * 16 + 8, PSCFG_MAXS});
         I.have_density = true;
         I.dens_prec = I.prec_now;
     }
+    copy_list(E, cj, 8);
+    CK(cudaMemcpyAsync(E.hq(0), E.dstage, sizeof(double) * 16 * E.hpin_inst, cudaMemcpyDeviceToHost, E.st));
     if (finish) {
         CK(cudaStreamSynchronize(E.st));
         density_finish(E, act);
@@ -1585,9 +1605,11 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
         std::vector<double> fe, pe;
         free_energy_all(E, act, fe, pe, false);
         if (prm.domain) {
-            for (int k = 0; k < na; k++)
-                CK(cudaMemcpyAsync(E.hst(k), E.inst[act[k]].stress_dev, sizeof(double) * PSCFG_MAXCP,
-                                   cudaMemcpyDeviceToHost, E.st));
+            std::vector<CopyJob> sj;
+            double *dst = E.dstage + (size_t)E.hpin_inst * 16;
+            for (int k = 0; k < na; k++) sj.push_back(CopyJob{E.inst[act[k]].stress_dev, dst + (size_t)k * 8, PSCFG_MAXCP});
+            copy_list(E, sj, 8);
+            CK(cudaMemcpyAsync(E.hst(0), dst, sizeof(double) * 8 * na, cudaMemcpyDeviceToHost, E.st));
         }
         // deviations into the ring slot of the current omega
         std::vector<AmJob> aj;
@@ -1778,9 +1800,9 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
             }
             // symmetric omega (the reference's star basis), recorded in the history
             symmetrize_omega(E, mix_inst);
-            for (size_t k = 0; k < mix_inst.size(); k++)
-                CK(cudaMemcpyAsync(slots[k], E.inst[mix_inst[k]].omega, sizeof(double) * fl,
-                                   cudaMemcpyDeviceToDevice, E.st));
+            std::vector<CopyJob> hj;
+            for (size_t k = 0; k < mix_inst.size(); k++) hj.push_back(CopyJob{E.inst[mix_inst[k]].omega, slots[k], fl});
+            copy_list(E, hj, fl);
             if (prm.domain) update_cells(E, mix_inst);
         }
         remaining = 0;

@@ -4,6 +4,23 @@
 
 namespace pscfg {
 
+// Batched copies of double arrays, job j = blockIdx.y: the per-instance
+// scalars (Q, stress) gathered into one staging block before a single
+// device-to-host copy, and the per-instance field copies of an Anderson
+// step, as one launch instead of one copy per instance.
+struct CopyJob {
+    const double *src;
+    double *dst;
+    long n;
+};
+
+static __global__ void k_copy_list(const CopyJob *jobs)
+{
+    const CopyJob j = jobs[blockIdx.y];
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < j.n; i += (long)gridDim.x * blockDim.x)
+        j.dst[i] = j.src[i];
+}
+
 // ---------------------------------------------------------------------
 // Stress (scf_stress, src/scf_mod.fp.f90:451-550).  Per contour slice i:
 //   inc_b(i) = sum_k w(k) dGsq_b(k) Re(qf^_i(k) conj(qr^_i(k)))
