@@ -247,9 +247,11 @@ struct PlaneStackR {
     // and kx = M are real after the row pass and can be transformed together
     // as one complex column; that is done where it saves a round of the
     // warps (4 planes of 32 x 32: 68 -> 64 columns), not where it only
-    // adds the separation step.
+    // adds the separation step.  FP64 only: the FP32 transforms keep the
+    // plain layout, whose rounding the mixed-precision switch was tuned on
+    // (with packed FP32 columns one of 64 BCC solves left its basin).
     static constexpr int WARPS = KT / 32;
-    static constexpr bool PACK =
+    static constexpr bool PACK = sizeof(T) == 8 &&
         ((PPC * NH + 15) / 16 + WARPS - 1) / WARPS > ((PPC * M + 15) / 16 + WARPS - 1) / WARPS;
     static constexpr int CW = PACK ? M : NH;   // column tasks per plane
     static_assert(!PACK || 16 % M == 0, "packed column tasks must tile the 16-task warp blocks");
