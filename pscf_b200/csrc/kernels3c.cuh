@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(128) k3s_zconv(const SweepField<T> *fields, in
 // a transform is one shared-memory pass for the rows and one for the
 // columns, and spectra are in natural y order.  The forward transform
 // writes the columns straight to global memory, the inverse reads them
-// from there.  blockDim must be a multiple of 32.
+// from there.  Kernels using it run blockDim = KT (128) threads.
 template <typename T, int N1, int N2, int PPC>
 struct PlaneStackR {
     static constexpr int M = N1 / 2, NH = M + 1, PS = N2 * NH, NP = N1 * N2;
