@@ -115,6 +115,7 @@ def lib():
         L.orc_set_symmetry.argtypes = [vp, C.c_int, ip, ip]
         L.orc_symmetrize.argtypes = [vp, dp]
         L.orc_density_batch.argtypes = [C.POINTER(OrcSystem), C.c_int, dp, vp, C.c_int]
+        L.orc_set_fft_threads.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -187,6 +188,11 @@ def fft_c2r(spec: np.ndarray, n1: int) -> np.ndarray:
     inter = np.ascontiguousarray(np.stack([s.real, s.imag], axis=-1))
     lib().orc_fft_c2r(np.array([n1, n2, n3], np.int32), inter.reshape(-1), out.reshape(-1))
     return out
+
+
+def set_fft_threads(n: int) -> None:
+    """Threads of the oracle's 3-D transforms (1 = serial; results identical)."""
+    lib().orc_set_fft_threads(int(n))
 
 
 def make_ksq(dim, n, G):

@@ -170,30 +170,74 @@ static void fft3d_free(fft3d *f)
     free(f->full); free(f->lin); free(f->lout);
 }
 
+/* Threads of the 3-D transforms (POSIX threads over independent lines; 1 =
+ * serial).  The lines are independent, so the result does not depend on it. */
+static int g_fft_threads = 1;
+
+int orc_set_fft_threads(int n)
+{
+    g_fft_threads = n < 1 ? 1 : (n > 64 ? 64 : n);
+    return 0;
+}
+
+typedef struct {
+    fft3d *f;
+    cplx *a;
+    int sign, axis;
+    long l0, l1;   /* line range */
+} lines_job;
+
+/* Lines [l0, l1) along one axis: x lines are numbered l = j + n2 k, y lines
+ * l = i + n1 k, z lines l = i + n1 j. */
+static void *lines_run(void *arg)
+{
+    lines_job *J = (lines_job *)arg;
+    fft3d *f = J->f;
+    const int n1 = f->n[0], n2 = f->n[1];
+    const int ax = J->axis, n = f->n[ax];
+    cplx *lin = (cplx *)malloc(sizeof(cplx) * n), *lout = (cplx *)malloc(sizeof(cplx) * n);
+    for (long l = J->l0; l < J->l1; l++) {
+        long base, es;
+        if (ax == 0) { base = l * n1; es = 1; }
+        else if (ax == 1) { base = (l % n1) + (long)n1 * n2 * (l / n1); es = n1; }
+        else { base = l; es = (long)n1 * n2; }
+        for (int e = 0; e < n; e++) lin[e] = J->a[base + e * es];
+        fft1d_exec(&f->p[ax], lin, lout, J->sign);
+        for (int e = 0; e < n; e++) J->a[base + e * es] = lout[e];
+    }
+    free(lin);
+    free(lout);
+    return NULL;
+}
+
+static void fft3d_lines(fft3d *f, cplx *a, int sign, int axis)
+{
+    const long nl = f->nr / f->n[axis];
+    int nt = g_fft_threads;
+    if (nt > nl) nt = (int)nl;
+    lines_job jobs[64];
+    pthread_t th[64];
+    for (int t = 0; t < nt; t++) {
+        jobs[t].f = f;
+        jobs[t].a = a;
+        jobs[t].sign = sign;
+        jobs[t].axis = axis;
+        jobs[t].l0 = nl * t / nt;
+        jobs[t].l1 = nl * (t + 1) / nt;
+    }
+    if (nt <= 1) {
+        lines_run(&jobs[0]);
+        return;
+    }
+    for (int t = 1; t < nt; t++) pthread_create(&th[t], NULL, lines_run, &jobs[t]);
+    lines_run(&jobs[0]);
+    for (int t = 1; t < nt; t++) pthread_join(th[t], NULL);
+}
+
 static void fft3d_c2c_inplace(fft3d *f, cplx *a, int sign)
 {
-    const int n1 = f->n[0], n2 = f->n[1], n3 = f->n[2];
-    /* x lines */
-    if (n1 > 1)
-        for (long l = 0; l < (long)n2 * n3; l++) {
-            cplx *row = a + l * n1;
-            memcpy(f->lin, row, sizeof(cplx) * n1);
-            fft1d_exec(&f->p[0], f->lin, row, sign);
-        }
-    if (n2 > 1)
-        for (int k = 0; k < n3; k++)
-            for (int i = 0; i < n1; i++) {
-                for (int j = 0; j < n2; j++) f->lin[j] = a[i + (long)n1 * (j + (long)n2 * k)];
-                fft1d_exec(&f->p[1], f->lin, f->lout, sign);
-                for (int j = 0; j < n2; j++) a[i + (long)n1 * (j + (long)n2 * k)] = f->lout[j];
-            }
-    if (n3 > 1)
-        for (int j = 0; j < n2; j++)
-            for (int i = 0; i < n1; i++) {
-                for (int k = 0; k < n3; k++) f->lin[k] = a[i + (long)n1 * (j + (long)n2 * k)];
-                fft1d_exec(&f->p[2], f->lin, f->lout, sign);
-                for (int k = 0; k < n3; k++) a[i + (long)n1 * (j + (long)n2 * k)] = f->lout[k];
-            }
+    for (int ax = 0; ax < 3; ax++)
+        if (f->n[ax] > 1) fft3d_lines(f, a, sign, ax);
 }
 
 /* r2c forward, unnormalised (FFTW dfftw_plan_dft_r2c_3d, src/fft3_mod.f90:85-94) */

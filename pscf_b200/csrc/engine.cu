@@ -34,6 +34,7 @@
 #include "kernels3x.cuh"
 #include "response.cuh"
 #include "kernels3l.cuh"
+#include "kernels3p.cuh"
 
 namespace pscfg {
 
@@ -129,6 +130,7 @@ struct Engine {
     bool smem_fft = false;           // shared-memory x-y column passes (PSCFG_SMEM_FFT=1)
     bool no_graphs = false;          // launch the 3-D sweeps directly (PSCFG_NO_GRAPHS=1)
     bool line_step = false;          // line-pass 3-D step even where the plane kernels fit (PSCFG_LINE_STEP=1)
+    int plane_p = -1;                // shared-memory plane kernels (kernels3p.cuh): -1 default shapes, 0 off, 1 also 64^3 (PSCFG_PLANE_P)
     int planes = 0;                  // planes per CTA of the register sweep, 0 = by launch size (PSCFG_PLANES)
     // CUDA graphs of 3-D sweeps, keyed by descriptor address, field and step count
     struct SweepGraph {
@@ -425,6 +427,8 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         E.line_step = ls && ls[0] && ls[0] != '0';
         const char *pl = std::getenv("PSCFG_PLANES");
         E.planes = pl ? std::atoi(pl) : 0;
+        const char *pp = std::getenv("PSCFG_PLANE_P");
+        if (pp && pp[0]) E.plane_p = std::atoi(pp);
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     upload_dft_constants();
@@ -569,6 +573,51 @@ static int sweep_planes(const Engine &E, int nf, int n3, int pmax)
     return p;
 }
 
+// Runs emit() -- a fixed sequence of sweep launches whose jobs are read from
+// the descriptors at dfl -- through a CUDA graph captured once per (dfl,
+// field count, step count, precision) and replayed after each descriptor
+// upload (PSCFG_NO_GRAPHS=1 launches directly).
+template <typename Emit>
+static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsize, Emit emit)
+{
+    if (E.no_graphs) {
+        emit();
+        return;
+    }
+    for (auto &g : E.graphs)
+        if (g.dfl == dfl && g.nf == nf && g.ns == ns_max && g.tsize == tsize) {
+            CK(cudaGraphLaunch(g.exec, E.st));
+            E.launches += g.launches;
+            return;
+        }
+    Engine::SweepGraph sg;
+    sg.dfl = dfl;
+    sg.nf = nf;
+    sg.ns = ns_max;
+    sg.tsize = tsize;
+    const long l0 = E.launches;
+    CK(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    try {
+        emit();
+    } catch (...) {
+        cudaStreamEndCapture(E.st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    CK(cudaStreamEndCapture(E.st, &graph));
+    cudaError_t ie = cudaGraphInstantiate(&sg.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(ie);
+    sg.launches = E.launches - l0;
+    if (E.graphs.size() >= 16) {
+        cudaGraphExecDestroy(E.graphs.front().exec);
+        E.graphs.erase(E.graphs.begin());
+    }
+    E.graphs.push_back(sg);
+    CK(cudaGraphLaunch(sg.exec, E.st));
+}
+
 // A whole 3-D sweep with the register-column kernels, the last kernel of
 // every step fused with the first of the next.  Returns false where the
 // grid has no such kernels (or another path was requested).
@@ -602,42 +651,7 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
                 E.launched();
             }
         };
-        if (E.no_graphs) {
-            emit();
-            return;
-        }
-        for (auto &g : E.graphs)
-            if (g.dfl == (const void *)dfl && g.nf == nf && g.ns == ns_max && g.tsize == (int)sizeof(T)) {
-                CK(cudaGraphLaunch(g.exec, E.st));
-                E.launches += g.launches;
-                return;
-            }
-        Engine::SweepGraph sg;
-        sg.dfl = dfl;
-        sg.nf = nf;
-        sg.ns = ns_max;
-        sg.tsize = (int)sizeof(T);
-        const long l0 = E.launches;
-        CK(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
-        cudaGraph_t graph = nullptr;
-        try {
-            emit();
-        } catch (...) {
-            cudaStreamEndCapture(E.st, &graph);
-            if (graph) cudaGraphDestroy(graph);
-            throw;
-        }
-        CK(cudaStreamEndCapture(E.st, &graph));
-        cudaError_t ie = cudaGraphInstantiate(&sg.exec, graph, 0);
-        cudaGraphDestroy(graph);
-        CK(ie);
-        sg.launches = E.launches - l0;
-        if (E.graphs.size() >= 16) {
-            cudaGraphExecDestroy(E.graphs.front().exec);
-            E.graphs.erase(E.graphs.begin());
-        }
-        E.graphs.push_back(sg);
-        CK(cudaGraphLaunch(sg.exec, E.st));
+        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), emit);
     };
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 32 && b == 32 && c == 32) {
@@ -657,6 +671,54 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
         case 2: run(N(), std::integral_constant<int, 2>()); break;
         default: run(N(), std::integral_constant<int, 1>()); break;
         }
+        return true;
+    }
+    return false;
+}
+
+// A whole 3-D sweep with the shared-memory plane kernels of kernels3p.cuh:
+// 64 x 128 x 224 by default, 64^3 with PSCFG_PLANE_P=1 (otherwise the k3c
+// kernels), none with PSCFG_PLANE_P=0.  Returns false where not applicable.
+template <typename T>
+static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
+{
+    if (E.no_fixed_kernels || E.smem_fft || E.cluster_step || E.line_step || E.plane_p == 0) return false;
+    auto run = [&](auto n1c, auto n2c, auto n3c, auto tcc) {
+        constexpr int N1 = decltype(n1c)::value, N2 = decltype(n2c)::value, N3 = decltype(n3c)::value;
+        constexpr int TC = decltype(tcc)::value;
+        using PL = PlaneP<T, N1, N2>;
+        const size_t smp = sizeof(cx<T>) * PL::PS, smz = sizeof(cx<T>) * N3 * TC;
+        CK(allow_dyn_smem((const void *)k3p_fwd_pair<T, N1, N2, N3>));
+        CK(allow_dyn_smem((const void *)k3p_mid<T, N1, N2, N3>));
+        CK(allow_dyn_smem((const void *)k3p_final_fwd<T, N1, N2, N3>));
+        CK(allow_dyn_smem((const void *)k3p_zconv<T, N1, N2, N3, TC>));
+        const PlaneGeom g = E.geom();
+        const unsigned ztiles = (unsigned)(PL::PS / TC);
+        auto emit = [&]() {
+            k3p_fwd_pair<T, N1, N2, N3><<<dim3(N3, nf), 256, smp, E.st>>>(dfl, g, 0);
+            E.launched();
+            for (int t = 0; t < ns_max; t++) {
+                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 2), 256, smz, E.st>>>(dfl, g, t, 3);
+                E.launched();
+                k3p_mid<T, N1, N2, N3><<<dim3(N3, nf, 2), 256, smp, E.st>>>(dfl, g, t);
+                E.launched();
+                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 1), 256, smz, E.st>>>(dfl, g, t, 2);
+                E.launched();
+                k3p_final_fwd<T, N1, N2, N3><<<dim3(N3, nf), 256, smp, E.st>>>(dfl, g, t);
+                E.launched();
+            }
+        };
+        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), emit);
+    };
+    const int a = E.n[0], b = E.n[1], c = E.n[2];
+    if (a == 64 && b == 128 && c == 224) {
+        run(std::integral_constant<int, 64>(), std::integral_constant<int, 128>(), std::integral_constant<int, 224>(),
+            std::integral_constant<int, 16>());
+        return true;
+    }
+    if (a == 64 && b == 64 && c == 64 && E.plane_p == 1) {
+        run(std::integral_constant<int, 64>(), std::integral_constant<int, 64>(), std::integral_constant<int, 64>(),
+            std::integral_constant<int, 32>());
         return true;
     }
     return false;
@@ -819,6 +881,7 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
         const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
         const int txy = 256, tz = 256;
         if (sweep3r<T>(E, dfl, nf, ns_max)) return;
+        if (sweep3p<T>(E, dfl, nf, ns_max)) return;
         for (int t = 0; t < ns_max; t++) {
             if (step3_fixed<T>(E, dfl, nf, t)) continue;
             if (step3l<T>(E, dfl, nf, t)) continue;

@@ -134,7 +134,65 @@ template <int R, int S, typename T> struct DftGeneric {
     }
 };
 template <int S, typename T> struct Dft<5, S, T> : DftGeneric<5, S, T> {};
-template <int S, typename T> struct Dft<7, S, T> : DftGeneric<7, S, T> {};
+
+// Length-7 DFT from the symmetric pairs t_j = x_j + x_{7-j}, d_j = x_j - x_{7-j}:
+// X_k = x_0 + sum_j cos(2 pi jk/7) t_j + S i sum_j sin(2 pi jk/7) d_j and
+// X_{7-k} the same with -S (k = 1, 2, 3): 66 real operations.
+template <int S, typename T> struct Dft<7, S, T> {
+    __device__ __forceinline__ static void run(cx<T> *v)
+    {
+        const T c1 = (T)0.623489801858733530525004884004239811;    // cos(2 pi/7)
+        const T c2 = (T)-0.222520933956314404288902564496794759;   // cos(4 pi/7)
+        const T c3 = (T)-0.900968867902419126236102319507445051;   // cos(6 pi/7)
+        const T s1 = (T)0.78183148246802980870844452667405775;     // sin(2 pi/7)
+        const T s2 = (T)0.974927912181823607018131682993931217;    // sin(4 pi/7)
+        const T s3 = (T)0.433883739117558120475768332848358755;    // sin(6 pi/7)
+        const cx<T> x0 = v[0];
+        const cx<T> t1 = v[1] + v[6], t2 = v[2] + v[5], t3 = v[3] + v[4];
+        const cx<T> d1 = v[1] - v[6], d2 = v[2] - v[5], d3 = v[3] - v[4];
+        v[0] = x0 + t1 + t2 + t3;
+        const cx<T> a1 = mk<T>(x0.x + c1 * t1.x + c2 * t2.x + c3 * t3.x, x0.y + c1 * t1.y + c2 * t2.y + c3 * t3.y);
+        const cx<T> a2 = mk<T>(x0.x + c2 * t1.x + c3 * t2.x + c1 * t3.x, x0.y + c2 * t1.y + c3 * t2.y + c1 * t3.y);
+        const cx<T> a3 = mk<T>(x0.x + c3 * t1.x + c1 * t2.x + c2 * t3.x, x0.y + c3 * t1.y + c1 * t2.y + c2 * t3.y);
+        const cx<T> b1 = mul_si<S>(mk<T>(s1 * d1.x + s2 * d2.x + s3 * d3.x, s1 * d1.y + s2 * d2.y + s3 * d3.y));
+        const cx<T> b2 = mul_si<S>(mk<T>(s2 * d1.x - s3 * d2.x - s1 * d3.x, s2 * d1.y - s3 * d2.y - s1 * d3.y));
+        const cx<T> b3 = mul_si<S>(mk<T>(s3 * d1.x - s1 * d2.x + s2 * d3.x, s3 * d1.y - s1 * d2.y + s2 * d3.y));
+        v[1] = a1 + b1;
+        v[6] = a1 - b1;
+        v[2] = a2 + b2;
+        v[5] = a2 - b2;
+        v[3] = a3 + b3;
+        v[4] = a3 - b3;
+    }
+};
+
+// Length-14 DFT as 2 x 7: n = 7 n1 + n2, k = k1 + 2 k2.
+template <int S, typename T> struct Dft<14, S, T> {
+    __device__ __forceinline__ static void run(cx<T> *v)
+    {
+        // W_14^m = cos(pi m/7) + S i sin(pi m/7), m = 1..6
+        const T c[7] = {(T)1, (T)0.900968867902419126236102319507445051, (T)0.623489801858733530525004884004239811,
+                        (T)0.222520933956314404288902564496794759, (T)-0.222520933956314404288902564496794759,
+                        (T)-0.623489801858733530525004884004239811, (T)-0.900968867902419126236102319507445051};
+        const T s[7] = {(T)0, (T)0.433883739117558120475768332848358755, (T)0.78183148246802980870844452667405775,
+                        (T)0.974927912181823607018131682993931217, (T)0.974927912181823607018131682993931217,
+                        (T)0.78183148246802980870844452667405775, (T)0.433883739117558120475768332848358755};
+        cx<T> a[7], b[7];
+#pragma unroll
+        for (int n2 = 0; n2 < 7; n2++) {
+            a[n2] = v[n2] + v[7 + n2];
+            const cx<T> d = v[n2] - v[7 + n2];
+            b[n2] = (n2 == 0) ? d : cmul(d, mk<T>(c[n2], (T)S * s[n2]));
+        }
+        Dft<7, S, T>::run(a);
+        Dft<7, S, T>::run(b);
+#pragma unroll
+        for (int k2 = 0; k2 < 7; k2++) {
+            v[2 * k2] = a[k2];
+            v[2 * k2 + 1] = b[k2];
+        }
+    }
+};
 
 // ---------------------------------------------------------------------
 // Line plan: length n = prod(rad[0..nst)), twiddle table tw[m] = W_n^m

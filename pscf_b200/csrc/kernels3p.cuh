@@ -1,0 +1,425 @@
+// kernels3p.cuh -- 3-D MDE step kernels for large grids of compile-time
+// shape (64 x 128 x 224, 64 x 64 x 64).
+//
+// Same four launches per step as the register-column kernels (kernels3c.cuh:
+// x-y forward pair, z pass on both spectra, x-y inverse + h + forward, z
+// pass, x-y inverse + Richardson fused with the next step's forward pair),
+// built for planes and z lines too long for registers:
+//   * a CTA of 256 threads holds one x-y plane spectrum (N2 rows of
+//     NH = N1/2 + 1 complex values) in shared memory, or a tile of TC z
+//     columns;
+//   * every 1-D transform is an in-place two-pass (four-step) transform
+//     N = P x Q (Split<N>) whose work items are numbered line-fastest, so
+//     that consecutive threads touch consecutive lines: with NH odd (row
+//     stride) or unit line stride every shared-memory pass is free of bank
+//     conflicts, and no radix above 16 is held in registers;
+//   * the row (x) transform of a real plane is a half-length complex
+//     transform of packed rows z[m] = f(2m) + i f(2m+1) untangled in place
+//     at the positions the forward transform leaves its outputs at, and the
+//     two real columns kx = 0 and kx = N1/2 are transformed as one complex
+//     column and separated by Hermitian symmetry (32 complex column lines
+//     per plane, every column pass an exact number of thread rounds).
+//
+// Spectrum layout ("positions").  Row y' of a plane spectrum holds ky =
+// iperm<N2>(y'); entry x' < M (M = N1/2) holds kx = iperm<M>(x'), entry M
+// holds kx = M.  A z column is forward transformed in natural z order,
+// multiplied by exp(-ds b^2 k^2/6 or /12) in the permuted order z' its
+// forward leaves, and inverse transformed back to natural order, so no
+// transform ever reorders data.  The k-space tables stay in the natural
+// order of make_propg (src/step_mod.f90:109-129).
+//
+// The algebra is step_exp (src/step_mod.f90:146-176), as in kernels.cuh.
+#pragma once
+#include "kernels3c.cuh"
+
+namespace pscfg {
+
+template <> struct Split<224> { static constexpr int P = 16, Q = 14; };
+
+// Pass A of a forward (S < 0) or the second pass of an inverse (S > 0)
+// transform of NL lines of length N: element e of line l at
+// buf[l * LSTR + e * ESTR]; tw = W_N^m (forward sign), m < N.
+template <int N, int S, typename T, int NL, int LSTR, int ESTR>
+__device__ __forceinline__ void lf_passA(cx<T> *buf, const cx<T> *__restrict__ tw)
+{
+    constexpr int P = Split<N>::P, Q = Split<N>::Q;
+    for (int w = threadIdx.x; w < NL * Q; w += blockDim.x) {
+        const int l = w % NL, n2 = w / NL;
+        cx<T> *b = buf + l * LSTR;
+        cx<T> v[P];
+        if (S < 0) {
+#pragma unroll
+            for (int n1 = 0; n1 < P; n1++) v[n1] = b[(Q * n1 + n2) * ESTR];
+            Dft<P, S, T>::run(v);
+            if (Q > 1) {
+#pragma unroll
+                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], __ldg_cx(tw + n2 * k1));
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < P; k1++) b[(Q * k1 + n2) * ESTR] = v[k1];
+        } else {
+#pragma unroll
+            for (int k1 = 0; k1 < P; k1++) v[k1] = b[(Q * k1 + n2) * ESTR];
+            if (Q > 1) {
+#pragma unroll
+                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], conjg(__ldg_cx(tw + n2 * k1)));
+            }
+            Dft<P, S, T>::run(v);
+#pragma unroll
+            for (int n1 = 0; n1 < P; n1++) b[(Q * n1 + n2) * ESTR] = v[n1];
+        }
+    }
+}
+
+// Pass B: length-Q transforms of the Q contiguous (stride ESTR) values at
+// Q k1 of each line.
+template <int N, int S, typename T, int NL, int LSTR, int ESTR>
+__device__ __forceinline__ void lf_passB(cx<T> *buf)
+{
+    constexpr int P = Split<N>::P, Q = Split<N>::Q;
+    if (Q == 1) return;
+    for (int w = threadIdx.x; w < NL * P; w += blockDim.x) {
+        const int l = w % NL, k1 = w / NL;
+        cx<T> *b = buf + l * LSTR + Q * k1 * ESTR;
+        cx<T> v[Q];
+#pragma unroll
+        for (int j = 0; j < Q; j++) v[j] = b[j * ESTR];
+        Dft<Q, S, T>::run(v);
+#pragma unroll
+        for (int j = 0; j < Q; j++) b[j * ESTR] = v[j];
+    }
+}
+
+// Forward (natural in, permuted out) or inverse (permuted in, natural out)
+// of NL lines; begins and ends with __syncthreads.
+template <int N, int S, typename T, int NL, int LSTR, int ESTR>
+__device__ __forceinline__ void lf_fft(cx<T> *buf, const cx<T> *__restrict__ tw)
+{
+    __syncthreads();
+    if (S < 0) {
+        lf_passA<N, S, T, NL, LSTR, ESTR>(buf, tw);
+        if (Split<N>::Q > 1) {
+            __syncthreads();
+            lf_passB<N, S, T, NL, LSTR, ESTR>(buf);
+        }
+    } else {
+        if (Split<N>::Q > 1) {
+            lf_passB<N, S, T, NL, LSTR, ESTR>(buf);
+            __syncthreads();
+        }
+        lf_passA<N, S, T, NL, LSTR, ESTR>(buf, tw);
+    }
+    __syncthreads();
+}
+
+template <typename T> struct Pair;
+template <> struct Pair<double> { using V = double2; };
+template <> struct Pair<float> { using V = float2; };
+
+// two consecutive reals at an even offset (16- or 8-byte aligned)
+template <typename T>
+__device__ __forceinline__ cx<T> ld_pair(const T *p)
+{
+    const typename Pair<T>::V v = *(const typename Pair<T>::V *)p;
+    return mk<T>(v.x, v.y);
+}
+template <typename T>
+__device__ __forceinline__ void st_pair(T *p, T a, T b)
+{
+    typename Pair<T>::V v;
+    v.x = a;
+    v.y = b;
+    *(typename Pair<T>::V *)p = v;
+}
+
+// Twiddle tables of one grid shape (device, precision T, forward sign):
+// W_M (rows), W_N1 (untangling), W_N2 (columns), W_N3 (z).
+template <typename T>
+struct Tw {
+    const cx<T> *M, *N1, *N2, *N3;
+};
+
+template <typename T>
+__host__ __device__ inline Tw<T> twiddles(const PlaneGeom &g)
+{
+    Tw<T> t;
+    t.M = (const cx<T> *)g.row.tw;
+    t.N1 = (const cx<T> *)g.rtw;
+    t.N2 = (const cx<T> *)g.col.tw;
+    t.N3 = (const cx<T> *)g.zp.tw;
+    return t;
+}
+
+// One x-y plane (N1 even, M = N1/2 a power of two >= 8, N2 a power of two).
+template <typename T, int N1, int N2>
+struct PlaneP {
+    static constexpr int M = N1 / 2, NH = M + 1, PS = N2 * NH, NP = N1 * N2, H = M / 2;
+
+    // kx of row position x'
+    __device__ __forceinline__ static int kx_of(int xp) { return xp < M ? iperm<M>(xp) : M; }
+
+    // packed natural rows: buf[y*NH + m] = pair(e) with pair(e) = (f(e), f(e+1)), e = y N1 + 2m
+    template <typename F>
+    __device__ __forceinline__ static void pack(cx<T> *buf, F pair)
+    {
+#pragma unroll 4
+        for (int i = threadIdx.x; i < N2 * M; i += blockDim.x) {
+            const int y = i / M, m = i % M;
+            buf[y * NH + m] = pair(y * N1 + 2 * m);
+        }
+    }
+
+    // element loop over the packed rows in the same thread mapping as pack():
+    // fn(slot, e) with slot = packed pair of reals e, e+1
+    template <typename F>
+    __device__ __forceinline__ static void each_pair(cx<T> *buf, F fn)
+    {
+#pragma unroll 4
+        for (int i = threadIdx.x; i < N2 * M; i += blockDim.x) {
+            const int y = i / M, m = i % M;
+            fn(buf[y * NH + m], y * N1 + 2 * m);
+        }
+    }
+
+    __device__ __forceinline__ static void load(cx<T> *buf, const cx<T> *src)
+    {
+#pragma unroll 4
+        for (int i = threadIdx.x; i < PS; i += blockDim.x) buf[i] = src[i];
+    }
+    __device__ __forceinline__ static void store(cx<T> *dst, const cx<T> *buf)
+    {
+#pragma unroll 4
+        for (int i = threadIdx.x; i < PS; i += blockDim.x) dst[i] = buf[i];
+    }
+
+    // packed natural rows -> plane spectrum (positions).  Ends synchronised.
+    __device__ static void forward(cx<T> *buf, const Tw<T> &tw)
+    {
+        lf_fft<M, -1, T, N2, NH, 1>(buf, tw.M);   // rows: permuted kx out
+        // untangle in place (each item reads and writes only the positions
+        // of kx = k and M - k); X[0] and X[M] are real and share position 0
+        for (int i = threadIdx.x; i < N2 * (H + 1); i += blockDim.x) {
+            const int y = i / (H + 1), k = i % (H + 1);
+            cx<T> *b = buf + y * NH;
+            if (k == 0) {
+                const cx<T> z0 = b[0];
+                b[0] = mk<T>(z0.x + z0.y, z0.x - z0.y);
+            } else if (k == H) {
+                const int p = perm<M>(H);
+                b[p] = conjg(b[p]);
+            } else {
+                const int p = perm<M>(k), pm = perm<M>(M - k);
+                const cx<T> zk = b[p], zm = b[pm];
+                const cx<T> wk = __ldg_cx(tw.N1 + k), wm = __ldg_cx(tw.N1 + (M - k));
+                const cx<T> ak = zk + conjg(zm), dk = zk - conjg(zm);
+                const cx<T> am = zm + conjg(zk), dm = zm - conjg(zk);
+                b[p] = scale(ak + mul_si<-1>(cmul(wk, dk)), (T)0.5);
+                b[pm] = scale(am + mul_si<-1>(cmul(wm, dm)), (T)0.5);
+            }
+        }
+        lf_fft<N2, -1, T, M, 1, NH>(buf, tw.N2);  // columns x' < M: permuted ky out
+        // separate column 0 = X0 + i XM into kx = 0 (position 0) and kx = M
+        for (int ky = threadIdx.x; ky <= N2 / 2; ky += blockDim.x) {
+            const int p = perm<N2>(ky);
+            if (ky == 0 || ky == N2 / 2) {
+                const cx<T> c = buf[p * NH];
+                buf[p * NH] = mk<T>(c.x, (T)0);
+                buf[p * NH + M] = mk<T>(c.y, (T)0);
+            } else {
+                const int pm = perm<N2>(N2 - ky);
+                const cx<T> ck = buf[p * NH], cm = conjg(buf[pm * NH]);
+                const cx<T> a = scale(ck + cm, (T)0.5);
+                const cx<T> b = scale(mul_si<-1>(ck - cm), (T)0.5);
+                buf[p * NH] = a;
+                buf[pm * NH] = conjg(a);
+                buf[p * NH + M] = b;
+                buf[pm * NH + M] = conjg(b);
+            }
+        }
+        __syncthreads();
+    }
+
+    // plane spectrum (positions) -> packed natural rows of the unnormalised
+    // c2r.  Ends synchronised.
+    __device__ static void inverse(cx<T> *buf, const Tw<T> &tw)
+    {
+        __syncthreads();
+        for (int r = threadIdx.x; r < N2; r += blockDim.x) {
+            const cx<T> a = buf[r * NH], b = buf[r * NH + M];
+            buf[r * NH] = mk<T>(a.x - b.y, a.y + b.x);   // a + i b
+        }
+        lf_fft<N2, 1, T, M, 1, NH>(buf, tw.N2);   // columns: natural y out
+        for (int i = threadIdx.x; i < N2 * (H + 1); i += blockDim.x) {
+            const int y = i / (H + 1), k = i % (H + 1);
+            cx<T> *b = buf + y * NH;
+            if (k == 0) {
+                const cx<T> c = b[0];   // (X0, XM), both real
+                b[0] = mk<T>(c.x + c.y, c.x - c.y);
+            } else if (k == H) {
+                const int p = perm<M>(H);
+                b[p] = scale(conjg(b[p]), (T)2);
+            } else {
+                const int p = perm<M>(k), pm = perm<M>(M - k);
+                const cx<T> xk = b[p], xm = b[pm];
+                const cx<T> wk = conjg(__ldg_cx(tw.N1 + k)), wm = conjg(__ldg_cx(tw.N1 + (M - k)));
+                b[p] = (xk + conjg(xm)) + mul_si<1>(cmul(wk, xk - conjg(xm)));
+                b[pm] = (xm + conjg(xk)) + mul_si<1>(cmul(wm, xm - conjg(xk)));
+            }
+        }
+        lf_fft<M, 1, T, N2, NH, 1>(buf, tw.M);    // rows: natural packed out
+    }
+};
+
+// K1 (first step of a sweep): S1 = Fxy[eo1 q], S2 = Fxy[eo2 q], with
+// eo1 = eo2^2.  grid = (N3, nfields), 256 threads.
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(256, 2) k3p_fwd_pair(const SweepField<T> *fields, PlaneGeom g, int t)
+{
+    using PL = PlaneP<T, N1, N2>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const Tw<T> tw = twiddles<T>(g);
+    const long nr = (long)N1 * N2 * N3;
+    const int z = blockIdx.x;
+    const T *q = src_slice(f, src, nr) + (long)z * PL::NP;
+    const T *eo2 = f.eo2[blk] + (long)z * PL::NP;
+    PL::pack(buf, [&](int e) {
+        const cx<T> a = ld_pair(eo2 + e), v = ld_pair(q + e);
+        return mk<T>(a.x * (a.x * v.x), a.y * (a.y * v.y));
+    });
+    PL::forward(buf, tw);
+    PL::store(f.S1 + (long)z * PL::PS, buf);
+    __syncthreads();
+    PL::pack(buf, [&](int e) {
+        const cx<T> a = ld_pair(eo2 + e), v = ld_pair(q + e);
+        return mk<T>(a.x * v.x, a.y * v.y);
+    });
+    PL::forward(buf, tw);
+    PL::store(f.S2 + (long)z * PL::PS, buf);
+}
+
+// K2/K4: S <- Fz^-1[ek . Fz[S]] on a tile of TC columns (positions c =
+// y' NH + x').  which: 1 = S1/ek1, 2 = S2/ek2, 3 = both (grid.z selects).
+// grid = (N2 NH / TC, nfields, 1 or 2), 256 threads.
+template <typename T, int N1, int N2, int N3, int TC>
+__global__ void __launch_bounds__(256, 2) k3p_zconv(const SweepField<T> *fields, PlaneGeom g, int t, int which)
+{
+    using PL = PlaneP<T, N1, N2>;
+    constexpr int NH = PL::NH, P = PL::PS;
+    static_assert(P % TC == 0, "column tiles must divide the plane");
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    const int sel = which == 3 ? (int)blockIdx.z + 1 : which;
+    cx<T> *S = (sel == 1) ? f.S1 : f.S2;
+    const T *ek = (sel == 1) ? f.ek1[blk] : f.ek2[blk];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const cx<T> *twz = (const cx<T> *)g.zp.tw;
+    const int c0 = blockIdx.x * TC;
+#pragma unroll 7
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int z = i / TC, c = i % TC;
+        buf[i] = S[(long)z * P + c0 + c];
+    }
+    lf_fft<N3, -1, T, TC, 1, TC>(buf, twz);
+#pragma unroll 7
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int pz = i / TC, c = c0 + i % TC;
+        const int yp = c / NH, xp = c % NH;
+        const long kidx = PL::kx_of(xp) + (long)NH * (iperm<N2>(yp) + (long)N2 * iperm<N3>(pz));
+        buf[i] = scale(buf[i], __ldg(ek + kidx));
+    }
+    lf_fft<N3, 1, T, TC, 1, TC>(buf, twz);
+#pragma unroll 7
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int z = i / TC, c = i % TC;
+        S[(long)z * P + c0 + c] = buf[i];
+    }
+}
+
+// K3: role 0 (grid.z = 0): q1 = eo1 . Fxy^-1[S1] / N.  Role 1: S2 <-
+// Fxy[eo2 . (eo2 . Fxy^-1[S2] / N)], the second half step's input.
+// grid = (N3, nfields, 2).
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(256, 2) k3p_mid(const SweepField<T> *fields, PlaneGeom g, int t)
+{
+    using PL = PlaneP<T, N1, N2>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const Tw<T> tw = twiddles<T>(g);
+    const T rn = (T)((long)N1 * N2 * N3);
+    const int z = blockIdx.x;
+    const T *eo2 = f.eo2[blk] + (long)z * PL::NP;
+    if (blockIdx.z == 0) {
+        T *q1 = f.q1 + (long)z * PL::NP;
+        PL::load(buf, f.S1 + (long)z * PL::PS);
+        PL::inverse(buf, tw);
+        PL::each_pair(buf, [&](cx<T> &s, int e) {
+            const cx<T> a = ld_pair(eo2 + e);
+            st_pair(q1 + e, (a.x * a.x) * s.x / rn, (a.y * a.y) * s.y / rn);
+        });
+    } else {
+        PL::load(buf, f.S2 + (long)z * PL::PS);
+        PL::inverse(buf, tw);
+        PL::each_pair(buf, [&](cx<T> &s, int e) {
+            const cx<T> a = ld_pair(eo2 + e);
+            s = mk<T>((a.x * a.x) * s.x / rn, (a.y * a.y) * s.y / rn);
+        });
+        PL::forward(buf, tw);
+        PL::store(f.S2 + (long)z * PL::PS, buf);
+    }
+}
+
+// K5 fused with the next step's K1: q_out = (4 eo2 . Fxy^-1[S2]/N - q1)/3,
+// then (if step t + 1 exists) S1 = Fxy[eo1' q_out], S2 = Fxy[eo2' q_out]
+// with the tables of step t + 1's block.  grid = (N3, nfields).
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(256, 2) k3p_final_fwd(const SweepField<T> *fields, PlaneGeom g, int t)
+{
+    using PL = PlaneP<T, N1, N2>;
+    const SweepField<T> &f = fields[blockIdx.y];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const Tw<T> tw = twiddles<T>(g);
+    const long nr = (long)N1 * N2 * N3;
+    const T rn = (T)nr;
+    const int z = blockIdx.x;
+    const T *eo2 = f.eo2[blk] + (long)z * PL::NP;
+    const T *q1 = f.q1 + (long)z * PL::NP;
+    T *out = dst_slice(f, dst, nr) + (long)z * PL::NP;
+    int blk2, src2, dst2;
+    const bool next = step_slices(f, t + 1, blk2, src2, dst2);   // the same for the whole CTA
+    const T *n2 = f.eo2[next ? blk2 : blk] + (long)z * PL::NP;
+    PL::load(buf, f.S2 + (long)z * PL::PS);
+    PL::inverse(buf, tw);
+    PL::each_pair(buf, [&](cx<T> &s, int e) {
+        const cx<T> a = ld_pair(eo2 + e), p = ld_pair(q1 + e);
+        const T o0 = ((T)4 * (a.x * s.x / rn) - p.x) / (T)3;
+        const T o1 = ((T)4 * (a.y * s.y / rn) - p.y) / (T)3;
+        st_pair(out + e, o0, o1);
+        const cx<T> b = ld_pair(n2 + e);
+        s = mk<T>((b.x * b.x) * o0, (b.y * b.y) * o1);
+    });
+    if (!next) return;
+    PL::forward(buf, tw);
+    PL::store(f.S1 + (long)z * PL::PS, buf);
+    __syncthreads();
+    // out was written above by the same threads in the same element mapping
+    PL::pack(buf, [&](int e) {
+        const cx<T> b = ld_pair(n2 + e), o = ld_pair((const T *)out + e);
+        return mk<T>(b.x * o.x, b.y * o.y);
+    });
+    PL::forward(buf, tw);
+    PL::store(f.S2 + (long)z * PL::PS, buf);
+}
+
+}  // namespace pscfg
