@@ -130,7 +130,7 @@ struct Engine {
     bool smem_fft = false;           // shared-memory x-y column passes (PSCFG_SMEM_FFT=1)
     bool no_graphs = false;          // launch the 3-D sweeps directly (PSCFG_NO_GRAPHS=1)
     bool line_step = false;          // line-pass 3-D step even where the plane kernels fit (PSCFG_LINE_STEP=1)
-    int plane_p = -1;                // shared-memory plane kernels (kernels3p.cuh): -1 default shapes, 0 off, 1 also 64^3 (PSCFG_PLANE_P)
+    int plane_p = 1;                 // shared-memory plane kernels (kernels3p.cuh) for 64x128x224 and 64^3; 0: off (PSCFG_PLANE_P)
     int planes = 0;                  // planes per CTA of the register sweep, 0 = by launch size (PSCFG_PLANES)
     // CUDA graphs of 3-D sweeps, keyed by descriptor address, field and step count
     struct SweepGraph {
@@ -291,6 +291,31 @@ static void make_geom(Engine &E, PlaneGeom &g)
     g.rtw = twiddle_table<T>(E, g.n1);
 }
 
+// W_N^m tables of the plane kernels (kernels3p.cuh), FP64 and FP32.
+template <int N>
+static void upload_ptw(const void *sym_d, const void *sym_f)
+{
+    double d[2][N];
+    float f[2][N];
+    for (int m = 0; m < N; m++) {
+        long double a = -2.0L * 3.14159265358979323846264338327950288L * m / (long double)N;
+        d[0][m] = (double)cosl(a);
+        d[1][m] = (double)sinl(a);
+        f[0][m] = (float)cosl(a);
+        f[1][m] = (float)sinl(a);
+    }
+    CK(cudaMemcpyToSymbol(sym_d, d, sizeof(d)));
+    CK(cudaMemcpyToSymbol(sym_f, f, sizeof(f)));
+}
+
+static void upload_p_twiddles()
+{
+    upload_ptw<32>(c_ptw32, c_ptw32f);
+    upload_ptw<64>(c_ptw64, c_ptw64f);
+    upload_ptw<128>(c_ptw128, c_ptw128f);
+    upload_ptw<224>(c_ptw224, c_ptw224f);
+}
+
 static void upload_dft_constants()
 {
     // row 0: cos(2 pi m/R), row 1: sin(2 pi m/R); the codelet forms
@@ -315,6 +340,7 @@ static void upload_dft_constants()
         w64[1][m] = (double)sinl(a);
     }
     CK(cudaMemcpyToSymbol(c_w64, w64, sizeof(w64)));
+    upload_p_twiddles();
 }
 
 // ---------------------------------------------------------------------
@@ -676,9 +702,11 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
     return false;
 }
 
-// A whole 3-D sweep with the shared-memory plane kernels of kernels3p.cuh:
-// 64 x 128 x 224 by default, 64^3 with PSCFG_PLANE_P=1 (otherwise the k3c
-// kernels), none with PSCFG_PLANE_P=0.  Returns false where not applicable.
+// A whole 3-D sweep with the shared-memory plane kernels of kernels3p.cuh
+// (64 x 128 x 224 and 64^3; PSCFG_PLANE_P=0 selects the other kernels:
+// run-time shaped at 64 x 128 x 224, k3c at 64^3).  Returns false where not
+// applicable.  64^3, 4 instances, FP64 sweep: 61.3k field-steps/s against
+// 30.8k with the k3c kernels; 64 x 128 x 224, 1 instance: 8.0k against 2.5k.
 template <typename T>
 static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
 {
@@ -716,7 +744,7 @@ static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
             std::integral_constant<int, 16>());
         return true;
     }
-    if (a == 64 && b == 64 && c == 64 && E.plane_p == 1) {
+    if (a == 64 && b == 64 && c == 64) {
         run(std::integral_constant<int, 64>(), std::integral_constant<int, 64>(), std::integral_constant<int, 64>(),
             std::integral_constant<int, 32>());
         return true;
@@ -1149,11 +1177,32 @@ static void stress3r(Engine &E, const StressJob<T> *dj, int s0, int cnt)
     E.launched();
 }
 
+// The stress slice pass with the plane kernels (kernels3p.cuh), for the
+// shapes whose sweep uses them.
+template <typename T, int N1, int N2, int N3, int TC>
+static void stress3p(Engine &E, const StressJob<T> *dj, int s0, int cnt)
+{
+    using PL = PlaneP<T, N1, N2>;
+    const size_t smp = sizeof(cx<T>) * PL::PS, smz = 2 * sizeof(cx<T>) * N3 * TC;
+    CK(allow_dyn_smem((const void *)k3p_stress_xy<T, N1, N2, N3>));
+    CK(allow_dyn_smem((const void *)k3p_stress_z<T, N1, N2, N3, TC>));
+    const int ntile = PL::PS / TC;
+    k3p_stress_xy<T, N1, N2, N3><<<dim3(N3, cnt, 2), 256, smp, E.st>>>(dj, s0, (cx<T> *)E.spec);
+    E.launched();
+    k3p_stress_z<T, N1, N2, N3, TC><<<dim3(ntile, cnt), 256, smz, E.st>>>(dj, s0, (const cx<T> *)E.spec, E.stress_part);
+    E.launched();
+    k3_stress_sum<T><<<cnt, 32, 0, E.st>>>(dj, s0, ntile, E.stress_part);
+    E.launched();
+}
+
 template <typename T>
 static bool stress3_fixed(Engine &E, const StressJob<T> *dj, int s0, int cnt)
 {
     if (E.no_fixed_kernels) return false;
     const int a = E.n[0], b = E.n[1], c = E.n[2];
+    const bool pk = !(E.smem_fft || E.cluster_step || E.line_step || E.plane_p == 0);
+    if (pk && a == 64 && b == 128 && c == 224) { stress3p<T, 64, 128, 224, 8>(E, dj, s0, cnt); return true; }
+    if (pk && a == 64 && b == 64 && c == 64) { stress3p<T, 64, 64, 64, 16>(E, dj, s0, cnt); return true; }
     if (a == 32 && b == 32 && c == 32) {
         if (E.smem_fft) stress3c<T, 32, 32, 32, 8>(E, dj, s0, cnt);
         else stress3r<T, 32, 32, 32, 4>(E, dj, s0, cnt);
@@ -1258,7 +1307,10 @@ static void slice_dots(Engine &E, const std::vector<StressJob<T>> &jobs)
             CK(cudaMalloc(&E.spec, per_slice * cs));
             E.spec_bytes = per_slice * cs;
         }
-        size_t plen = (size_t)cs * ntile * PSCFG_MAXCP;
+        // partial sums per (slice, column tile): the plane kernels' stress
+        // pass (stress3p) tiles by 8 columns, the generic one by Z_TILE
+        const long ntile_max = std::max<long>(ntile, (P + 7) / 8);
+        size_t plen = (size_t)cs * ntile_max * PSCFG_MAXCP;
         if (E.stress_part_len < plen) {
             if (E.stress_part) cudaFree(E.stress_part);
             E.stress_part = nullptr;

@@ -36,11 +36,33 @@ namespace pscfg {
 
 template <> struct Split<224> { static constexpr int P = 16, Q = 14; };
 
+// W_N^m = exp(-2 pi i m / N), m < N, for the line lengths of these kernels,
+// in constant memory: every index used below is the same for all lanes of a
+// warp (the line index varies fastest across lanes), so each read is one
+// broadcast from the constant cache instead of a global load that streaming
+// plane data would evict from L1.  Filled by the host (upload_p_twiddles).
+__constant__ double c_ptw32[2][32], c_ptw64[2][64], c_ptw128[2][128], c_ptw224[2][224];
+__constant__ float c_ptw32f[2][32], c_ptw64f[2][64], c_ptw128f[2][128], c_ptw224f[2][224];
+
+template <typename T, int N> struct PTw;
+#define PSCFG_PTW(N)                                                                                         \
+    template <> struct PTw<double, N> {                                                                      \
+        __device__ __forceinline__ static cx<double> at(int m) { return mk<double>(c_ptw##N[0][m], c_ptw##N[1][m]); } \
+    };                                                                                                       \
+    template <> struct PTw<float, N> {                                                                       \
+        __device__ __forceinline__ static cx<float> at(int m) { return mk<float>(c_ptw##N##f[0][m], c_ptw##N##f[1][m]); } \
+    };
+PSCFG_PTW(32)
+PSCFG_PTW(64)
+PSCFG_PTW(128)
+PSCFG_PTW(224)
+#undef PSCFG_PTW
+
 // Pass A of a forward (S < 0) or the second pass of an inverse (S > 0)
 // transform of NL lines of length N: element e of line l at
-// buf[l * LSTR + e * ESTR]; tw = W_N^m (forward sign), m < N.
+// buf[l * LSTR + e * ESTR].
 template <int N, int S, typename T, int NL, int LSTR, int ESTR>
-__device__ __forceinline__ void lf_passA(cx<T> *buf, const cx<T> *__restrict__ tw)
+__device__ __forceinline__ void lf_passA(cx<T> *buf)
 {
     constexpr int P = Split<N>::P, Q = Split<N>::Q;
     for (int w = threadIdx.x; w < NL * Q; w += blockDim.x) {
@@ -53,7 +75,7 @@ __device__ __forceinline__ void lf_passA(cx<T> *buf, const cx<T> *__restrict__ t
             Dft<P, S, T>::run(v);
             if (Q > 1) {
 #pragma unroll
-                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], __ldg_cx(tw + n2 * k1));
+                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], PTw<T, N>::at(n2 * k1));
             }
 #pragma unroll
             for (int k1 = 0; k1 < P; k1++) b[(Q * k1 + n2) * ESTR] = v[k1];
@@ -62,7 +84,7 @@ __device__ __forceinline__ void lf_passA(cx<T> *buf, const cx<T> *__restrict__ t
             for (int k1 = 0; k1 < P; k1++) v[k1] = b[(Q * k1 + n2) * ESTR];
             if (Q > 1) {
 #pragma unroll
-                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], conjg(__ldg_cx(tw + n2 * k1)));
+                for (int k1 = 1; k1 < P; k1++) v[k1] = cmul(v[k1], conjg(PTw<T, N>::at(n2 * k1)));
             }
             Dft<P, S, T>::run(v);
 #pragma unroll
@@ -93,11 +115,11 @@ __device__ __forceinline__ void lf_passB(cx<T> *buf)
 // Forward (natural in, permuted out) or inverse (permuted in, natural out)
 // of NL lines; begins and ends with __syncthreads.
 template <int N, int S, typename T, int NL, int LSTR, int ESTR>
-__device__ __forceinline__ void lf_fft(cx<T> *buf, const cx<T> *__restrict__ tw)
+__device__ __forceinline__ void lf_fft(cx<T> *buf)
 {
     __syncthreads();
     if (S < 0) {
-        lf_passA<N, S, T, NL, LSTR, ESTR>(buf, tw);
+        lf_passA<N, S, T, NL, LSTR, ESTR>(buf);
         if (Split<N>::Q > 1) {
             __syncthreads();
             lf_passB<N, S, T, NL, LSTR, ESTR>(buf);
@@ -107,9 +129,30 @@ __device__ __forceinline__ void lf_fft(cx<T> *buf, const cx<T> *__restrict__ tw)
             lf_passB<N, S, T, NL, LSTR, ESTR>(buf);
             __syncthreads();
         }
-        lf_passA<N, S, T, NL, LSTR, ESTR>(buf, tw);
+        lf_passA<N, S, T, NL, LSTR, ESTR>(buf);
     }
     __syncthreads();
+}
+
+// 16-byte asynchronous global -> shared copies (cp.async): every copy of a
+// tile is in flight at once and none holds a register.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// bytes (a multiple of 16, both addresses 16-byte aligned) from global to
+// shared memory by all threads of the CTA; the caller synchronises
+template <int BYTES>
+__device__ __forceinline__ void copy_in(void *smem, const void *gmem)
+{
+    static_assert(BYTES % 16 == 0, "16-byte chunks");
+#pragma unroll 8
+    for (int c = threadIdx.x; c < BYTES / 16; c += blockDim.x)
+        cp_async16((char *)smem + 16 * c, (const char *)gmem + 16 * c);
+    cp_async_wait_all();
 }
 
 template <typename T> struct Pair;
@@ -132,28 +175,12 @@ __device__ __forceinline__ void st_pair(T *p, T a, T b)
     *(typename Pair<T>::V *)p = v;
 }
 
-// Twiddle tables of one grid shape (device, precision T, forward sign):
-// W_M (rows), W_N1 (untangling), W_N2 (columns), W_N3 (z).
-template <typename T>
-struct Tw {
-    const cx<T> *M, *N1, *N2, *N3;
-};
-
-template <typename T>
-__host__ __device__ inline Tw<T> twiddles(const PlaneGeom &g)
-{
-    Tw<T> t;
-    t.M = (const cx<T> *)g.row.tw;
-    t.N1 = (const cx<T> *)g.rtw;
-    t.N2 = (const cx<T> *)g.col.tw;
-    t.N3 = (const cx<T> *)g.zp.tw;
-    return t;
-}
-
 // One x-y plane (N1 even, M = N1/2 a power of two >= 8, N2 a power of two).
 template <typename T, int N1, int N2>
 struct PlaneP {
     static constexpr int M = N1 / 2, NH = M + 1, PS = N2 * NH, NP = N1 * N2, H = M / 2;
+    static constexpr int KT = 256;   // threads per CTA of every kernel below
+    static_assert((N2 * M) % KT == 0, "packed-row loops in whole rounds");
 
     // kx of row position x'
     __device__ __forceinline__ static int kx_of(int xp) { return xp < M ? iperm<M>(xp) : M; }
@@ -163,8 +190,8 @@ struct PlaneP {
     __device__ __forceinline__ static void pack(cx<T> *buf, F pair)
     {
 #pragma unroll 4
-        for (int i = threadIdx.x; i < N2 * M; i += blockDim.x) {
-            const int y = i / M, m = i % M;
+        for (int r = 0; r < N2 * M / KT; r++) {
+            const int i = threadIdx.x + r * KT, y = i / M, m = i % M;
             buf[y * NH + m] = pair(y * N1 + 2 * m);
         }
     }
@@ -175,16 +202,16 @@ struct PlaneP {
     __device__ __forceinline__ static void each_pair(cx<T> *buf, F fn)
     {
 #pragma unroll 4
-        for (int i = threadIdx.x; i < N2 * M; i += blockDim.x) {
-            const int y = i / M, m = i % M;
+        for (int r = 0; r < N2 * M / KT; r++) {
+            const int i = threadIdx.x + r * KT, y = i / M, m = i % M;
             fn(buf[y * NH + m], y * N1 + 2 * m);
         }
     }
 
+    // (asynchronous copies; the transform that follows begins with a barrier)
     __device__ __forceinline__ static void load(cx<T> *buf, const cx<T> *src)
     {
-#pragma unroll 4
-        for (int i = threadIdx.x; i < PS; i += blockDim.x) buf[i] = src[i];
+        copy_in<PS * (int)sizeof(cx<T>)>(buf, src);
     }
     __device__ __forceinline__ static void store(cx<T> *dst, const cx<T> *buf)
     {
@@ -193,13 +220,13 @@ struct PlaneP {
     }
 
     // packed natural rows -> plane spectrum (positions).  Ends synchronised.
-    __device__ static void forward(cx<T> *buf, const Tw<T> &tw)
+    __device__ static void forward(cx<T> *buf)
     {
-        lf_fft<M, -1, T, N2, NH, 1>(buf, tw.M);   // rows: permuted kx out
+        lf_fft<M, -1, T, N2, NH, 1>(buf);   // rows: permuted kx out
         // untangle in place (each item reads and writes only the positions
         // of kx = k and M - k); X[0] and X[M] are real and share position 0
         for (int i = threadIdx.x; i < N2 * (H + 1); i += blockDim.x) {
-            const int y = i / (H + 1), k = i % (H + 1);
+            const int k = i / N2, y = i % N2;   // lanes across rows: conflict-free, uniform twiddles
             cx<T> *b = buf + y * NH;
             if (k == 0) {
                 const cx<T> z0 = b[0];
@@ -210,14 +237,14 @@ struct PlaneP {
             } else {
                 const int p = perm<M>(k), pm = perm<M>(M - k);
                 const cx<T> zk = b[p], zm = b[pm];
-                const cx<T> wk = __ldg_cx(tw.N1 + k), wm = __ldg_cx(tw.N1 + (M - k));
+                const cx<T> wk = PTw<T, N1>::at(k), wm = PTw<T, N1>::at(M - k);
                 const cx<T> ak = zk + conjg(zm), dk = zk - conjg(zm);
                 const cx<T> am = zm + conjg(zk), dm = zm - conjg(zk);
                 b[p] = scale(ak + mul_si<-1>(cmul(wk, dk)), (T)0.5);
                 b[pm] = scale(am + mul_si<-1>(cmul(wm, dm)), (T)0.5);
             }
         }
-        lf_fft<N2, -1, T, M, 1, NH>(buf, tw.N2);  // columns x' < M: permuted ky out
+        lf_fft<N2, -1, T, M, 1, NH>(buf);  // columns x' < M: permuted ky out
         // separate column 0 = X0 + i XM into kx = 0 (position 0) and kx = M
         for (int ky = threadIdx.x; ky <= N2 / 2; ky += blockDim.x) {
             const int p = perm<N2>(ky);
@@ -241,16 +268,16 @@ struct PlaneP {
 
     // plane spectrum (positions) -> packed natural rows of the unnormalised
     // c2r.  Ends synchronised.
-    __device__ static void inverse(cx<T> *buf, const Tw<T> &tw)
+    __device__ static void inverse(cx<T> *buf)
     {
         __syncthreads();
         for (int r = threadIdx.x; r < N2; r += blockDim.x) {
             const cx<T> a = buf[r * NH], b = buf[r * NH + M];
             buf[r * NH] = mk<T>(a.x - b.y, a.y + b.x);   // a + i b
         }
-        lf_fft<N2, 1, T, M, 1, NH>(buf, tw.N2);   // columns: natural y out
+        lf_fft<N2, 1, T, M, 1, NH>(buf);   // columns: natural y out
         for (int i = threadIdx.x; i < N2 * (H + 1); i += blockDim.x) {
-            const int y = i / (H + 1), k = i % (H + 1);
+            const int k = i / N2, y = i % N2;
             cx<T> *b = buf + y * NH;
             if (k == 0) {
                 const cx<T> c = b[0];   // (X0, XM), both real
@@ -261,12 +288,12 @@ struct PlaneP {
             } else {
                 const int p = perm<M>(k), pm = perm<M>(M - k);
                 const cx<T> xk = b[p], xm = b[pm];
-                const cx<T> wk = conjg(__ldg_cx(tw.N1 + k)), wm = conjg(__ldg_cx(tw.N1 + (M - k)));
+                const cx<T> wk = conjg(PTw<T, N1>::at(k)), wm = conjg(PTw<T, N1>::at(M - k));
                 b[p] = (xk + conjg(xm)) + mul_si<1>(cmul(wk, xk - conjg(xm)));
                 b[pm] = (xm + conjg(xk)) + mul_si<1>(cmul(wm, xm - conjg(xk)));
             }
         }
-        lf_fft<M, 1, T, N2, NH, 1>(buf, tw.M);    // rows: natural packed out
+        lf_fft<M, 1, T, N2, NH, 1>(buf);    // rows: natural packed out
     }
 };
 
@@ -281,7 +308,6 @@ __global__ void __launch_bounds__(256, 2) k3p_fwd_pair(const SweepField<T> *fiel
     if (!step_slices(f, t, blk, src, dst)) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = (cx<T> *)smem_raw;
-    const Tw<T> tw = twiddles<T>(g);
     const long nr = (long)N1 * N2 * N3;
     const int z = blockIdx.x;
     const T *q = src_slice(f, src, nr) + (long)z * PL::NP;
@@ -290,14 +316,14 @@ __global__ void __launch_bounds__(256, 2) k3p_fwd_pair(const SweepField<T> *fiel
         const cx<T> a = ld_pair(eo2 + e), v = ld_pair(q + e);
         return mk<T>(a.x * (a.x * v.x), a.y * (a.y * v.y));
     });
-    PL::forward(buf, tw);
+    PL::forward(buf);
     PL::store(f.S1 + (long)z * PL::PS, buf);
     __syncthreads();
     PL::pack(buf, [&](int e) {
         const cx<T> a = ld_pair(eo2 + e), v = ld_pair(q + e);
         return mk<T>(a.x * v.x, a.y * v.y);
     });
-    PL::forward(buf, tw);
+    PL::forward(buf);
     PL::store(f.S2 + (long)z * PL::PS, buf);
 }
 
@@ -318,14 +344,19 @@ __global__ void __launch_bounds__(256, 2) k3p_zconv(const SweepField<T> *fields,
     const T *ek = (sel == 1) ? f.ek1[blk] : f.ek2[blk];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = (cx<T> *)smem_raw;
-    const cx<T> *twz = (const cx<T> *)g.zp.tw;
     const int c0 = blockIdx.x * TC;
-#pragma unroll 7
-    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
-        const int z = i / TC, c = i % TC;
-        buf[i] = S[(long)z * P + c0 + c];
+    {
+        // TC consecutive columns of each z row: RB 16-byte chunks per row
+        constexpr int RB = TC * (int)sizeof(cx<T>) / 16;
+        static_assert(RB * 16 == TC * (int)sizeof(cx<T>), "tile rows in 16-byte chunks");
+#pragma unroll 8
+        for (int c = threadIdx.x; c < N3 * RB; c += blockDim.x) {
+            const int z = c / RB, j = c % RB;
+            cp_async16((char *)(buf + z * TC) + 16 * j, (const char *)(S + (long)z * P + c0) + 16 * j);
+        }
+        cp_async_wait_all();
     }
-    lf_fft<N3, -1, T, TC, 1, TC>(buf, twz);
+    lf_fft<N3, -1, T, TC, 1, TC>(buf);
 #pragma unroll 7
     for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
         const int pz = i / TC, c = c0 + i % TC;
@@ -333,7 +364,7 @@ __global__ void __launch_bounds__(256, 2) k3p_zconv(const SweepField<T> *fields,
         const long kidx = PL::kx_of(xp) + (long)NH * (iperm<N2>(yp) + (long)N2 * iperm<N3>(pz));
         buf[i] = scale(buf[i], __ldg(ek + kidx));
     }
-    lf_fft<N3, 1, T, TC, 1, TC>(buf, twz);
+    lf_fft<N3, 1, T, TC, 1, TC>(buf);
 #pragma unroll 7
     for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
         const int z = i / TC, c = i % TC;
@@ -353,26 +384,25 @@ __global__ void __launch_bounds__(256, 2) k3p_mid(const SweepField<T> *fields, P
     if (!step_slices(f, t, blk, src, dst)) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = (cx<T> *)smem_raw;
-    const Tw<T> tw = twiddles<T>(g);
     const T rn = (T)((long)N1 * N2 * N3);
     const int z = blockIdx.x;
     const T *eo2 = f.eo2[blk] + (long)z * PL::NP;
     if (blockIdx.z == 0) {
         T *q1 = f.q1 + (long)z * PL::NP;
         PL::load(buf, f.S1 + (long)z * PL::PS);
-        PL::inverse(buf, tw);
+        PL::inverse(buf);
         PL::each_pair(buf, [&](cx<T> &s, int e) {
             const cx<T> a = ld_pair(eo2 + e);
             st_pair(q1 + e, (a.x * a.x) * s.x / rn, (a.y * a.y) * s.y / rn);
         });
     } else {
         PL::load(buf, f.S2 + (long)z * PL::PS);
-        PL::inverse(buf, tw);
+        PL::inverse(buf);
         PL::each_pair(buf, [&](cx<T> &s, int e) {
             const cx<T> a = ld_pair(eo2 + e);
             s = mk<T>((a.x * a.x) * s.x / rn, (a.y * a.y) * s.y / rn);
         });
-        PL::forward(buf, tw);
+        PL::forward(buf);
         PL::store(f.S2 + (long)z * PL::PS, buf);
     }
 }
@@ -389,7 +419,6 @@ __global__ void __launch_bounds__(256, 2) k3p_final_fwd(const SweepField<T> *fie
     if (!step_slices(f, t, blk, src, dst)) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = (cx<T> *)smem_raw;
-    const Tw<T> tw = twiddles<T>(g);
     const long nr = (long)N1 * N2 * N3;
     const T rn = (T)nr;
     const int z = blockIdx.x;
@@ -400,7 +429,7 @@ __global__ void __launch_bounds__(256, 2) k3p_final_fwd(const SweepField<T> *fie
     const bool next = step_slices(f, t + 1, blk2, src2, dst2);   // the same for the whole CTA
     const T *n2 = f.eo2[next ? blk2 : blk] + (long)z * PL::NP;
     PL::load(buf, f.S2 + (long)z * PL::PS);
-    PL::inverse(buf, tw);
+    PL::inverse(buf);
     PL::each_pair(buf, [&](cx<T> &s, int e) {
         const cx<T> a = ld_pair(eo2 + e), p = ld_pair(q1 + e);
         const T o0 = ((T)4 * (a.x * s.x / rn) - p.x) / (T)3;
@@ -410,7 +439,7 @@ __global__ void __launch_bounds__(256, 2) k3p_final_fwd(const SweepField<T> *fie
         s = mk<T>((b.x * b.x) * o0, (b.y * b.y) * o1);
     });
     if (!next) return;
-    PL::forward(buf, tw);
+    PL::forward(buf);
     PL::store(f.S1 + (long)z * PL::PS, buf);
     __syncthreads();
     // out was written above by the same threads in the same element mapping
@@ -418,8 +447,81 @@ __global__ void __launch_bounds__(256, 2) k3p_final_fwd(const SweepField<T> *fie
         const cx<T> b = ld_pair(n2 + e), o = ld_pair((const T *)out + e);
         return mk<T>(b.x * o.x, b.y * o.y);
     });
-    PL::forward(buf, tw);
+    PL::forward(buf);
     PL::store(f.S2 + (long)z * PL::PS, buf);
+}
+
+// Stress pass (scf_stress, src/scf_mod.fp.f90:451-550), pass 1: x-y
+// forward of slices [s0, s0 + cs) of qf (grid.z = 0) and qr (grid.z = 1)
+// into spec[(s - s0) * 2 + dir][z][positions].  grid = (N3, cs, 2).
+template <typename T, int N1, int N2, int N3>
+__global__ void __launch_bounds__(256, 2) k3p_stress_xy(const StressJob<T> *job, int s0, cx<T> *spec)
+{
+    using PL = PlaneP<T, N1, N2>;
+    const StressJob<T> &J = *job;
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *buf = (cx<T> *)smem_raw;
+    const long nr = (long)N1 * N2 * N3, nk = (long)PL::PS * N3;
+    const int z = blockIdx.x;
+    const T *q = (blockIdx.z == 0 ? J.qf : J.qr) + (long)s * nr + (long)z * PL::NP;
+    PL::pack(buf, [&](int e) { return ld_pair(q + e); });
+    PL::forward(buf);
+    PL::store(spec + ((long)blockIdx.y * 2 + blockIdx.z) * nk + (long)z * PL::PS, buf);
+}
+
+// Pass 2: z forward of a tile of TC columns of both spectra of a slice and
+// the partial sums sum_k wdgsq_b(k) Re(F_qf(k) conj F_qr(k)) of every cell
+// parameter b in one sweep over the tile, into
+// part[((s - s0) * gridDim.x + tile) * PSCFG_MAXCP + b].  grid = (N2 NH / TC, cs).
+template <typename T, int N1, int N2, int N3, int TC>
+__global__ void __launch_bounds__(256, 2) k3p_stress_z(const StressJob<T> *job, int s0, const cx<T> *spec, double *part)
+{
+    using PL = PlaneP<T, N1, N2>;
+    constexpr int NH = PL::NH, P = PL::PS;
+    static_assert(P % TC == 0, "column tiles must divide the plane");
+    const StressJob<T> &J = *job;
+    const int s = s0 + blockIdx.y;
+    if (s >= J.nslices) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *F = (cx<T> *)smem_raw, *R = F + N3 * TC;
+    __shared__ double red[32];
+    const long nk = (long)P * N3;
+    const int c0 = blockIdx.x * TC;
+    const cx<T> *sf = spec + ((long)blockIdx.y * 2) * nk, *sr = sf + nk;
+    {
+        constexpr int RB = TC * (int)sizeof(cx<T>) / 16;
+        static_assert(RB * 16 == TC * (int)sizeof(cx<T>), "tile rows in 16-byte chunks");
+#pragma unroll 8
+        for (int c = threadIdx.x; c < N3 * RB; c += blockDim.x) {
+            const int z = c / RB, j = c % RB;
+            cp_async16((char *)(F + z * TC) + 16 * j, (const char *)(sf + (long)z * P + c0) + 16 * j);
+            cp_async16((char *)(R + z * TC) + 16 * j, (const char *)(sr + (long)z * P + c0) + 16 * j);
+        }
+        cp_async_wait_all();
+    }
+    lf_fft<N3, -1, T, TC, 1, TC>(F);
+    lf_fft<N3, -1, T, TC, 1, TC>(R);
+    double acc[PSCFG_MAXCP] = {0, 0, 0, 0, 0, 0};
+    const int ncp = J.ncp;
+    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+        const int pz = i / TC, c = c0 + i % TC;
+        const int yp = c / NH, xp = c % NH;
+        const long k = PL::kx_of(xp) + (long)NH * (iperm<N2>(yp) + (long)N2 * iperm<N3>(pz));
+        const cx<T> f = F[i], r = R[i];
+        const double pr = (double)f.x * (double)r.x + (double)f.y * (double)r.y;
+#pragma unroll
+        for (int b = 0; b < PSCFG_MAXCP; b++)
+            if (b < ncp) acc[b] += __ldg(J.wdgsq + (long)b * nk + k) * pr;
+    }
+#pragma unroll
+    for (int b = 0; b < PSCFG_MAXCP; b++) {
+        if (b >= ncp) break;   // uniform across the CTA
+        const double tot = block_sum(acc[b], red);
+        if (threadIdx.x == 0) part[((long)blockIdx.y * gridDim.x + blockIdx.x) * PSCFG_MAXCP + b] = tot;
+        __syncthreads();
+    }
 }
 
 }  // namespace pscfg

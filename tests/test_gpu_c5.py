@@ -95,7 +95,7 @@ def _density_path(monkeypatch, plane_p, w, prec=FP64):
 def test_c5_plane_kernels_match_generic(monkeypatch, c5_omega):
     """Full contour (ds = 0.005, 200 steps per chain): the plane kernels
     against the run-time shaped kernels, which the oracle pins elsewhere."""
-    rho_p, q_p, st_p = _density_path(monkeypatch, -1, c5_omega)
+    rho_p, q_p, st_p = _density_path(monkeypatch, 1, c5_omega)
     rho_g, q_g, st_g = _density_path(monkeypatch, 0, c5_omega)
     assert abs(q_p / q_g - 1.0) < 1e-12
     assert rel_err(rho_p, rho_g) < 1e-12, rel_err(rho_p, rho_g)
@@ -104,7 +104,24 @@ def test_c5_plane_kernels_match_generic(monkeypatch, c5_omega):
 
 def test_c5_fp32_propagation_close(monkeypatch, c5_omega):
     """FP32 propagation with FP64 contour sums, against FP64."""
-    rho_d, q_d, _ = _density_path(monkeypatch, -1, c5_omega, FP64)
-    rho_s, q_s, _ = _density_path(monkeypatch, -1, c5_omega, FP32)
+    rho_d, q_d, _ = _density_path(monkeypatch, 1, c5_omega, FP64)
+    rho_s, q_s, _ = _density_path(monkeypatch, 1, c5_omega, FP32)
     assert abs(q_s / q_d - 1.0) < 1e-4
     assert rel_err(rho_s, rho_d) < 1e-4, rel_err(rho_s, rho_d)
+
+
+def test_plane_kernels_64_cubed():
+    """The same plane kernels at 64^3 (the default there) against the oracle."""
+    from tests.cases import diblock, omega_guess
+    s = diblock(3, [64, 64, 64], "cubic", [3.7], fA=0.4, chiN=16.0, ds=0.05)
+    w = omega_guess(s, 21, 2.0)
+    o = O.Oracle(s)
+    rho_ref, q_ref = o.density(w)
+    st_ref = o.stress()
+    e = Engine([s], FP64)
+    rho, q = e.density(w[None])
+    assert rel_err(q[0, :1], q_ref) < 1e-12
+    assert rel_err(rho[0], rho_ref) < 1e-12, rel_err(rho[0], rho_ref)
+    st = e.scf_stress()[0, : len(st_ref)]
+    assert np.max(np.abs(st - st_ref)) < 1e-10 * max(1.0, np.max(np.abs(st_ref))), (st, st_ref)
+    e.close()
