@@ -100,13 +100,31 @@ typedef struct pscfg_am_param {
     double switch_error;     /* PSCFG_MIXED: FP32 -> FP64 below this error (0: 1e-3), on
                                 stagnation within 1000x of it, when the error rises to 10x the
                                 best FP32 error, or after 500 FP32 iterations */
+    /* Stabilisers for starts far from a solution (no counterpart in the
+     * reference, whose iterate_AM always ramps lambda = 1 - 0.9^k to 1 and
+     * keeps its history): 0 selects the reference behaviour. */
+    double mix_max;          /* cap on lambda (0: 1) */
+    double restart;          /* restart the history and the lambda ramp when the error exceeds
+                                restart x its best value since the last restart (0: never) */
 } pscfg_am_param;
+
+/* Per-instance exit status of an Anderson run (pscfg_am_result.status).
+ * The reference stops the whole program on these conditions
+ * (src/iterate_mod.fp.f90:412-420); here each instance retires on its own
+ * and the others go on. */
+#define PSCFG_AM_CONVERGED 0   /* error below error_max */
+#define PSCFG_AM_RUNNING 1     /* not finished yet (pscfg_am_results during a run) */
+#define PSCFG_AM_NONFINITE 2   /* NaN or Inf in the deviation (detected on the device) */
+#define PSCFG_AM_DIVERGED 3    /* error above 1e4 */
+#define PSCFG_AM_MAXITER 4     /* max_itr iterations without converging */
+#define PSCFG_AM_SINGULAR 5    /* singular Anderson coefficient system */
 
 /* Per-instance result of pscfg_iterate_am. */
 typedef struct pscfg_am_result {
     int itr;
     int itr_fp32;            /* PSCFG_MIXED: iterations run with FP32 propagation */
     int converged;           /* 1 converged, 0 not (max_itr or diverged) */
+    int status;              /* PSCFG_AM_* */
     double error;            /* max(|dev|, |stress|) at exit */
     double f_helmholtz;      /* free energy per monomer / kT */
     double pressure;
@@ -259,17 +277,23 @@ int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, 
  * point has no counterpart in the reference.
  *
  * It takes no engine handle and calls no cudaMalloc/cudaFree: its scratch
- * (propagator tables, spectra, working slices, twiddles) is one file-scope
- * device array of about 5.6 MB, sized for grids of at most
- * PSCFG_NOALLOC_MAX_NR points and PSCFG_NOALLOC_MAX_LINE points per axis,
- * which every GPU that loads the library holds until the process exits.
- * Larger grids are rejected with PSCFG_EINVAL and a message from
- * pscfg_last_error(NULL).  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress) with that device current; make that
- * first call before any stream capture.  All calls on a device share the
- * array: calls whose GPU work overlaps (other host threads, or streams with
- * no ordering between them) race on it.  Each call overwrites every scratch
- * entry it reads, so nothing carries over from the previous call.
+ * (propagator tables, spectra, working slices, twiddles, step descriptors)
+ * is one file-scope device array of about 5.6 MB, which every GPU that
+ * loads the library holds until the process exits.  Grids must have at
+ * most PSCFG_NOALLOC_MAX_NR points and PSCFG_NOALLOC_MAX_LINE points per
+ * axis, extents with no prime factor above 7, and fit the shared memory of
+ * the kernels (227 KB): for dim <= 2, 32 n2 (n1/2+1) + 16 n1 n2 bytes
+ * (64 x 64 fits, 128 x 128 does not); for dim = 3, 32 n2 (n1/2+1) and
+ * 512 n3 bytes each.  Other grids are rejected with PSCFG_EINVAL, before
+ * any GPU work is queued, and a message from pscfg_last_error(NULL).  The
+ * first call on a device does a one-time set-up with that device current:
+ * it looks up the array's device address (cudaGetSymbolAddress) and uploads
+ * the codelet constants; make that first call before any stream capture.
+ * A call queues kernel launches only (no host-device copies).  All calls
+ * on a device share the array: calls whose GPU work overlaps (other host
+ * threads, or streams with no ordering between them) race on it.  Each
+ * call writes every scratch entry it reads, so nothing carries over from
+ * the previous call.
  *
  * All arrays are device pointers, FP64, x-fastest: ksq_dev [nk] (the k^2
  * table, e.g. from pscfg_get_ksq), omega_dev [nr] (the block's monomer

@@ -1570,6 +1570,9 @@ struct AmState {
     bool done = false;
     bool converged = false;
     double error = 0;
+    int status = PSCFG_AM_RUNNING;
+    int k0 = 0;                // iteration of the last history restart (lambda ramp origin)
+    double best_run = INFINITY; // best error since the last restart
     int nstore = 0;            // number of valid history entries (<= H+1)
     int head = 0;              // ring slot of the most recent entry
     std::vector<double> gram;  // (H+1)x(H+1) ring-indexed <d_i, d_j>
@@ -1788,7 +1791,10 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
         k_final_sum<<<(unsigned)((na * (PSCFG_MAXH + 1) + 127) / 128), 128, 0, E.st>>>(dpart, nct, 1.0, dres,
                                                                                        na * (PSCFG_MAXH + 1));
         E.launched();
-        const size_t nsm = (size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1);
+        double *dstat = dres + (size_t)na * (PSCFG_MAXH + 1);
+        k_am_status<<<(unsigned)((na + 127) / 128), 128, 0, E.st>>>(emax, dres, PSCFG_MAXH + 1, 100.0 * large, dstat, na);
+        E.launched();
+        const size_t nsm = (size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 2);
         CK(cudaMemcpyAsync(E.hsm(), E.d_small, sizeof(double) * nsm, cudaMemcpyDeviceToHost, E.st));
         CK(cudaStreamSynchronize(E.st));
         density_finish(E, act);
@@ -1821,6 +1827,13 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
             for (int b = 0; b < ncp; b++) e2 = std::max(e2, std::fabs(s.stress[b]));
             s.error = std::max(e1, e2);
             s.nstore = nst;
+            const double word = hsmall[(size_t)na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1) + k];
+            if (word == 1.0 || !std::isfinite(s.error)) {
+                s.error = NAN;
+                s.status = PSCFG_AM_NONFINITE;
+                s.done = true;
+                continue;
+            }
             // mixed precision: an FP32 iteration never counts as converged; the
             // instance moves to FP64 once its error is below the switch error,
             // or once it is within 1000x of it and has not improved by 10% for
@@ -1843,14 +1856,32 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
                 }
                 if (go && E.prec == PSCFG_MIXED) I.prec_now = PSCFG_FP64;
             }
-            if (!(was32 && E.prec == PSCFG_MIXED) && s.error < prm.error_max) { s.converged = true; s.done = true; continue; }
-            if (s.itr > prm.max_itr || !(s.error <= 100.0 * large)) { s.done = true; continue; }
+            if (!(was32 && E.prec == PSCFG_MIXED) && s.error < prm.error_max) {
+                s.converged = true;
+                s.status = PSCFG_AM_CONVERGED;
+                s.done = true;
+                continue;
+            }
+            if (!(s.error <= 100.0 * large)) { s.status = PSCFG_AM_DIVERGED; s.done = true; continue; }
+            if (s.itr > prm.max_itr) { s.status = PSCFG_AM_MAXITER; s.done = true; continue; }
 
-            // lambda and history depth (src/iterate_mod.fp.f90:1147-1153)
+            // optional restart (not in the reference): drop the history and
+            // start the lambda ramp again from this iteration
+            if (prm.restart > 0 && s.itr - s.k0 > 1 && s.error > prm.restart * s.best_run) {
+                s.k0 = s.itr - 1;
+                s.nstore = 1;
+                s.best_run = s.error;
+            }
+            s.best_run = std::min(s.best_run, s.error);
+            // lambda and history depth (src/iterate_mod.fp.f90:1147-1153),
+            // counted from the last restart (the start, by default)
+            const int kk = s.itr - s.k0;
             int itr_prev;
             double lam;
-            if (s.itr < H + 1) { itr_prev = s.itr - 1; lam = 1.0 - std::pow(0.9, s.itr); }
+            if (kk < H + 1) { itr_prev = kk - 1; lam = 1.0 - std::pow(0.9, kk); }
             else { itr_prev = H; lam = 1.0; }
+            itr_prev = std::min(itr_prev, s.nstore - 1);
+            if (prm.mix_max > 0) lam = std::min(lam, prm.mix_max);
             AmMix m;
             std::memset(&m, 0, sizeof(m));
             m.omega = I.omega;
@@ -1882,7 +1913,7 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
                     for (int b = 0; b < ncp; b++) v += (s.devcp[cur][b] - s.devcp[sl[mm]][b]) * s.devcp[cur][b];
                     V[mm] = v;
                 }
-                if (!solve_dense(n, U, V)) { s.done = true; s.error = INFINITY; continue; }
+                if (!solve_dense(n, U, V)) { s.done = true; s.error = INFINITY; s.status = PSCFG_AM_SINGULAR; continue; }
                 m.n = n;
                 for (int nn = 0; nn < n; nn++) {
                     m.C[nn] = V[nn];
@@ -1950,6 +1981,7 @@ static void am_results(Engine &E, AmRun &R, std::vector<pscfg_am_result> &res)
         r.itr = s.itr;
         r.itr_fp32 = s.itr_fp32;
         r.converged = s.converged ? 1 : 0;
+        r.status = s.status;
         r.error = s.error;
         r.f_helmholtz = s.f;
         r.pressure = s.p;

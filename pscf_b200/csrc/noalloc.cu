@@ -43,8 +43,8 @@ constexpr int Z_TILE = 16;
 constexpr size_t al(size_t b) { return (b + 255) / 256 * 256; }
 constexpr size_t TW_BYTES = al(sizeof(cx<double>) * MAX_LINE);    // one twiddle table
 constexpr size_t OFF_TW = 0;                                        // 4 tables
-constexpr size_t OFF_DESC = OFF_TW + 4 * TW_BYTES;                  // TableJob + SweepField
-constexpr size_t DESC_BYTES = al(sizeof(TableJob<double>)) + al(sizeof(SweepField<double>));
+constexpr size_t OFF_DESC = OFF_TW + 4 * TW_BYTES;                  // TableJob + 4 SweepFields
+constexpr size_t DESC_BYTES = al(sizeof(TableJob<double>)) + al(4 * sizeof(SweepField<double>));
 constexpr size_t OFF_REAL = OFF_DESC + DESC_BYTES;                  // eo1, eo2, q1, slab[2]: 5 nr
 constexpr size_t REAL_BYTES = al(sizeof(double) * MAX_NR);
 constexpr size_t OFF_EK = OFF_REAL + 5 * REAL_BYTES;                // ek1, ek2: 2 nk (nk <= nr)
@@ -104,17 +104,34 @@ static int scratch_address(unsigned char **out)
     return PSCFG_OK;
 }
 
-// Twiddle table W_n^m (forward sign) into scratch, from a host stack buffer.
-static int put_twiddles(unsigned char *dst, int n, cudaStream_t st)
+// The descriptors of one call, passed by value to k_setup.  f[0]: first
+// step (reads q_in), f[1]: slice 0 -> 1, f[2]: slice 1 -> 0, f[3]: last step
+// (writes q_out).
+struct Descs {
+    TableJob<double> tj;
+    SweepField<double> f[4];
+};
+
+// Writes the call's descriptors and its four twiddle tables W_n^m (forward
+// sign, m < n, n = lens) into the scratch array, so that a call issues
+// kernel launches only (no host-to-device copies).
+__global__ void k_setup(Descs d, TableJob<double> *dtj, SweepField<double> *dfl, unsigned char *tw0, int4 lens,
+                        long tw_stride)
 {
-    cx<double> h[MAX_LINE];
-    for (int m = 0; m < n; m++) {
-        long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)n;
-        h[m].x = (double)cosl(a);
-        h[m].y = (double)sinl(a);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *dtj = d.tj;
+        for (int k = 0; k < 4; k++) dfl[k] = d.f[k];
     }
-    CKN(cudaMemcpyAsync(dst, h, sizeof(cx<double>) * n, cudaMemcpyHostToDevice, st));
-    return PSCFG_OK;
+    const int ln[4] = {lens.x, lens.y, lens.z, lens.w};
+    for (int k = 0; k < 4; k++) {
+        cx<double> *tw = (cx<double> *)(tw0 + k * tw_stride);
+        for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < ln[k]; m += gridDim.x * blockDim.x) {
+            double sv, cv;
+            sincospi(2.0 * (double)m / (double)ln[k], &sv, &cv);
+            tw[m].x = cv;
+            tw[m].y = -sv;
+        }
+    }
 }
 
 }  // namespace pscfg_noalloc
@@ -125,6 +142,7 @@ extern "C" int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_
                                        double b, double ds, const double *q_in_dev, double *q_out_dev, int nsteps,
                                        void *stream)
 {
+    // every check comes before any GPU work
     if (!n || !ksq_dev || !omega_dev || !q_in_dev || !q_out_dev || nsteps < 1)
         return fail(PSCFG_EINVAL, "null pointer or nsteps < 1");
     if (dim < 1 || dim > 3) return fail(PSCFG_EINVAL, "dim must be 1, 2 or 3");
@@ -132,18 +150,13 @@ extern "C" int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_
     for (int d = 0; d < dim; d++) g3[d] = n[d];
     for (int d = 0; d < 3; d++)
         if (g3[d] < 1 || g3[d] > MAX_LINE)
-            return fail(PSCFG_EINVAL, "grid extent " + std::to_string(g3[d]) + " outside 1.." + std::to_string(MAX_LINE));
+            return fail(PSCFG_EINVAL, "grid extent " + std::to_string(g3[d]) + " outside 1.." +
+                                          std::to_string(MAX_LINE) + " (PSCFG_NOALLOC_MAX_LINE)");
     const long nr = (long)g3[0] * g3[1] * g3[2];
     const long nk = (long)(g3[0] / 2 + 1) * g3[1] * g3[2];
     if (nr > MAX_NR)
         return fail(PSCFG_EINVAL, "grid of " + std::to_string(nr) + " points exceeds the no-allocation limit of " +
-                                      std::to_string(MAX_NR));
-    cudaStream_t st = (cudaStream_t)stream;
-    unsigned char *base = nullptr;
-    int rc = scratch_address(&base);
-    if (rc != PSCFG_OK) return rc;
-
-    // geometry: line plans with twiddles in scratch
+                                      std::to_string(MAX_NR) + " (PSCFG_NOALLOC_MAX_NR)");
     PlaneGeom g;
     std::memset(&g, 0, sizeof(g));
     g.n1 = g3[0];
@@ -153,18 +166,33 @@ extern "C" int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_
     g.even = (g.n1 % 2 == 0) ? 1 : 0;
     g.LS = g.even ? g.n1h : g.n1;
     LinePlan *plans[3] = {&g.row, &g.col, &g.zp};
-    const int lens[3] = {g.even ? g.n1 / 2 : g.n1, g.n2, g.n3};
+    const int lens[4] = {g.even ? g.n1 / 2 : g.n1, g.n2, g.n3, g.n1};
     for (int k = 0; k < 3; k++) {
         plans[k]->n = lens[k];
         if (!plan_radices(lens[k], plans[k]->rad, plans[k]->nst))
             return fail(PSCFG_EINVAL, "grid size has a prime factor other than 2, 3, 5, 7");
-        unsigned char *tw = base + OFF_TW + k * TW_BYTES;
-        if ((rc = put_twiddles(tw, lens[k], st)) != PSCFG_OK) return rc;
-        plans[k]->tw = tw;
     }
-    unsigned char *rtw = base + OFF_TW + 3 * TW_BYTES;
-    if ((rc = put_twiddles(rtw, g.n1, st)) != PSCFG_OK) return rc;
-    g.rtw = rtw;
+    const long P = (long)g.n1h * g.n2;
+    const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+    const size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<double>);
+    const size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<double>);
+    const size_t smpl = smxy + 2 * (size_t)nr * sizeof(double);
+    const size_t smmax = 227 * 1024;
+    if (dim <= 2 && smpl > smmax)
+        return fail(PSCFG_EINVAL, "no-allocation limit: a grid of dim <= 2 is propagated by one CTA in shared "
+                                  "memory and needs " + std::to_string(smpl) + " bytes of it (at most " +
+                                  std::to_string(smmax) + ")");
+    if (dim == 3 && (smxy > smmax || smz > smmax))
+        return fail(PSCFG_EINVAL, "no-allocation limit: an x-y plane spectrum needs " + std::to_string(smxy) +
+                                  " bytes of shared memory and a z tile " + std::to_string(smz) + " (at most " +
+                                  std::to_string(smmax) + " each)");
+
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned char *base = nullptr;
+    int rc = scratch_address(&base);
+    if (rc != PSCFG_OK) return rc;
+    for (int k = 0; k < 3; k++) plans[k]->tw = base + OFF_TW + k * TW_BYTES;
+    g.rtw = base + OFF_TW + 3 * TW_BYTES;
 
     double *eo1 = (double *)(base + OFF_REAL);
     double *eo2 = (double *)(base + OFF_REAL + REAL_BYTES);
@@ -175,15 +203,18 @@ extern "C" int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_
     cx<double> *S1 = (cx<double> *)(base + OFF_SPEC);
     cx<double> *S2 = (cx<double> *)(base + OFF_SPEC + al(sizeof(cx<double>) * MAX_NR));
 
-    TableJob<double> tj;
-    tj.omega = omega_dev;
-    tj.ksq = ksq_dev;
-    tj.eo1 = eo1;
-    tj.eo2 = eo2;
-    tj.ek1 = ek1;
-    tj.ek2 = ek2;
-    tj.ds = ds;
-    tj.b = b;
+    Descs d;
+    std::memset(&d, 0, sizeof(d));
+    d.tj.omega = omega_dev;
+    d.tj.ksq = ksq_dev;
+    d.tj.eo1 = eo1;
+    d.tj.eo2 = eo2;
+    d.tj.ek1 = ek1;
+    d.tj.ek2 = ek2;
+    d.tj.ds = ds;
+    d.tj.b = b;
+    // one step on a two-slice slab: dir +1 reads slice 0 and writes slice 1,
+    // dir -1 the reverse, so that consecutive steps alternate without copies
     SweepField<double> f;
     std::memset(&f, 0, sizeof(f));
     f.slab = slab;
@@ -199,24 +230,24 @@ extern "C" int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_
     f.S1 = S1;
     f.S2 = S2;
     f.q1 = q1;
+    d.f[0] = f;                                   // first step: q_in -> slice 1 (or q_out)
+    d.f[0].in = q_in_dev;
+    if (nsteps == 1) d.f[0].out = q_out_dev;
+    d.f[1] = f;                                   // slice 0 -> slice 1
+    d.f[2] = f;                                   // slice 1 -> slice 0
+    d.f[2].dir = -1;
+    d.f[3] = ((nsteps - 1) % 2 == 1) ? d.f[2] : d.f[1];   // last step (nsteps >= 2) -> q_out
+    d.f[3].out = q_out_dev;
     TableJob<double> *dtj = (TableJob<double> *)(base + OFF_DESC);
     SweepField<double> *dfl = (SweepField<double> *)(base + OFF_DESC + al(sizeof(TableJob<double>)));
-    CKN(cudaMemcpyAsync(dtj, &tj, sizeof(tj), cudaMemcpyHostToDevice, st));
-    CKN(cudaMemcpyAsync(dfl, &f, sizeof(f), cudaMemcpyHostToDevice, st));
-    CKN(cudaMemcpyAsync(slab, q_in_dev, sizeof(double) * nr, cudaMemcpyDeviceToDevice, st));
-
+    k_setup<<<4, 256, 0, st>>>(d, dtj, dfl, base + OFF_TW, make_int4(lens[0], lens[1], lens[2], lens[3]),
+                               (long)TW_BYTES);
+    CKN(cudaGetLastError());
     k_make_tables<double><<<dim3((unsigned)std::min<long>((nr + 255) / 256, 256), 1), 256, 0, st>>>(dtj, nr, nk);
     CKN(cudaGetLastError());
-    const long P = (long)g.n1h * g.n2;
-    const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
-    const size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<double>);
-    const size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<double>);
-    const size_t smpl = smxy + 2 * (size_t)nr * sizeof(double);
     if (dim <= 2) {
-        if (smpl > 227 * 1024) return fail(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
         CKN(allow_dyn_smem((const void *)k_sweep_plane<double>));
     } else {
-        if (smxy > 227 * 1024 || smz > 227 * 1024) return fail(PSCFG_EINVAL, "grid plane too large");
         CKN(allow_dyn_smem((const void *)k3_fwd_pair<double>));
         CKN(allow_dyn_smem((const void *)k3_inv_mid<double>));
         CKN(allow_dyn_smem((const void *)k3_inv_final<double>));
@@ -224,20 +255,20 @@ extern "C" int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_
     }
     const int threads = (int)std::min<long>(256, std::max<long>(32, ((nr / 2 + 31) / 32) * 32));
     for (int s = 0; s < nsteps; s++) {
-        // slice 0 -> slice 1, then slice 1 back into slice 0 (or out)
+        // step 0 reads q_in, then odd steps slice 1 -> 0 and even steps
+        // slice 0 -> 1; the last step writes q_out
+        const SweepField<double> *df = dfl + (s == 0 ? 0 : s == nsteps - 1 ? 3 : (s % 2 == 1 ? 2 : 1));
         if (dim <= 2) {
-            k_sweep_plane<double><<<1, threads, smpl, st>>>(dfl, g, 0, 1);
+            k_sweep_plane<double><<<1, threads, smpl, st>>>(df, g, 0, 1);
             CKN(cudaGetLastError());
         } else {
-            k3_fwd_pair<double><<<dim3(g.n3, 1), 256, smxy, st>>>(dfl, g, 0);
-            k3_zconv<double, Z_TILE><<<dim3(ntile, 1, 2), 256, smz, st>>>(dfl, g, 0, 3);
-            k3_inv_mid<double><<<dim3(g.n3, 1), 256, smxy, st>>>(dfl, g, 0);
-            k3_zconv<double, Z_TILE><<<dim3(ntile, 1, 1), 256, smz, st>>>(dfl, g, 0, 2);
-            k3_inv_final<double><<<dim3(g.n3, 1), 256, smxy, st>>>(dfl, g, 0);
+            k3_fwd_pair<double><<<dim3(g.n3, 1), 256, smxy, st>>>(df, g, 0);
+            k3_zconv<double, Z_TILE><<<dim3(ntile, 1, 2), 256, smz, st>>>(df, g, 0, 3);
+            k3_inv_mid<double><<<dim3(g.n3, 1), 256, smxy, st>>>(df, g, 0);
+            k3_zconv<double, Z_TILE><<<dim3(ntile, 1, 1), 256, smz, st>>>(df, g, 0, 2);
+            k3_inv_final<double><<<dim3(g.n3, 1), 256, smxy, st>>>(df, g, 0);
             CKN(cudaGetLastError());
         }
-        double *dst = (s == nsteps - 1) ? q_out_dev : slab;
-        CKN(cudaMemcpyAsync(dst, slab + nr, sizeof(double) * nr, cudaMemcpyDeviceToDevice, st));
     }
     return PSCFG_OK;
 }

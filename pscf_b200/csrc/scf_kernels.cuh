@@ -346,6 +346,20 @@ static __global__ void k_final_max(const double *part, int npart, double *out, i
     out[j] = m;
 }
 
+// Status word of each instance's Anderson iteration, computed on the device
+// from the iteration's reductions and read back with its other scalars:
+// 0 finite; 1 non-finite (<dev, dev> or max |dev| is NaN or Inf: a NaN or
+// Inf in omega, rho or the propagators; max |dev| alone would miss a NaN,
+// fmax drops NaN operands); 2 diverged (max |dev| above `large`).
+static __global__ void k_am_status(const double *emax, const double *g, int gstride, double large, double *status,
+                                   int njobs)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= njobs) return;
+    const double e = emax[k], g0 = g[(long)k * gstride];
+    status[k] = (!isfinite(e) || !isfinite(g0)) ? 1.0 : (e > large ? 2.0 : 0.0);
+}
+
 // Dot products of the current deviation with the stored ones:
 // g[h] = <dev_cur, dev_h> (sum over monomers and grid), h < nh.
 #define PSCFG_MAXH 32

@@ -64,7 +64,13 @@ class PscfgAmParam(C.Structure):
         ("domain", C.c_int),
         ("error_max", C.c_double),
         ("switch_error", C.c_double),
+        ("mix_max", C.c_double),
+        ("restart", C.c_double),
     ]
+
+
+# pscfg_am_result.status (PSCFG_AM_*)
+AM_STATUS = {0: "converged", 1: "running", 2: "nonfinite", 3: "diverged", 4: "maxiter", 5: "singular"}
 
 
 class PscfgAmResult(C.Structure):
@@ -72,6 +78,7 @@ class PscfgAmResult(C.Structure):
         ("itr", C.c_int),
         ("itr_fp32", C.c_int),
         ("converged", C.c_int),
+        ("status", C.c_int),
         ("error", C.c_double),
         ("f_helmholtz", C.c_double),
         ("pressure", C.c_double),
@@ -309,11 +316,11 @@ class Engine:
         return qf, qr
 
     def iterate_am(self, omega: np.ndarray, error_max=1e-10, max_itr=1000, n_hist=20, domain=False,
-                   switch_error=0.0):
+                   switch_error=0.0, mix_max=0.0, restart=0.0):
         """Anderson-mixing solve of every instance; returns (omega, rho, results)."""
         w = np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr).copy()
         rho = np.zeros_like(w)
-        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error)
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error, mix_max, restart)
         res = (PscfgAmResult * self.n_inst)()
         self._check(self.lib.pscfg_iterate_am(self._h, _ptr(w), C.byref(prm), _ptr(rho), res), allow=(ENOTCONV,))
         return w, rho, self._results(res, domain)
@@ -337,6 +344,7 @@ class Engine:
             ncp = len(self.systems[i].cell_param)
             nch = len(self.systems[i].chains)
             out.append(dict(itr=r.itr, itr_fp32=r.itr_fp32, converged=bool(r.converged), error=r.error,
+                            status=AM_STATUS.get(r.status, str(r.status)),
                             f_helmholtz=r.f_helmholtz, pressure=r.pressure,
                             stress=list(r.stress)[:ncp], cell_param=list(r.cell_param)[:ncp],
                             q=list(r.q)[:nch], mu_chain=list(r.mu_chain)[:nch]))
@@ -344,10 +352,11 @@ class Engine:
                 self.systems[i].cell_param = list(r.cell_param)[:ncp]
         return out
 
-    def am_begin(self, omega, error_max=1e-10, max_itr=1000, n_hist=20, domain=False, switch_error=0.0):
+    def am_begin(self, omega, error_max=1e-10, max_itr=1000, n_hist=20, domain=False, switch_error=0.0,
+                 mix_max=0.0, restart=0.0):
         w = None if omega is None else np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
         self._am_domain = domain
-        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error)
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error, mix_max, restart)
         self._check(self.lib.pscfg_am_begin(self._h, None if w is None else _ptr(w), C.byref(prm)))
 
     def am_iterate(self, iters: int = 1) -> int:

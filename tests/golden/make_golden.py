@@ -1,8 +1,8 @@
 """Extract the reference's golden values into tests/golden/golden.json.
 
-Run once in a checkout that has the reference tree (default
-/root/reference, or the path given as argv[1]); the JSON it writes is
-committed so that tests never read the reference at run time.
+Run once where the reference tree is available, giving its path as
+argv[1] or in the PSCF_REFERENCE environment variable; the JSON it writes
+is committed so that tests never read the reference at run time.
 
 Sources (paths inside the reference project):
   tools/python/tests/outfile/in          converged 1-D lamellar run (thermo)
@@ -16,7 +16,14 @@ import re
 import sys
 from fractions import Fraction
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+def reference_root() -> str:
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PSCF_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py REFERENCE_TREE  (or set PSCF_REFERENCE)")
+    return ref
+
+
+REF = reference_root() if __name__ == "__main__" else None
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

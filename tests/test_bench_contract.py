@@ -23,4 +23,5 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
-    assert d["config"]["grid"] == [32, 32, 32]
+    assert d["config"]["grid"] == [64, 128, 224]
+    assert "64x128x224" in cb["sample"]

@@ -168,22 +168,32 @@ def test_torch_autograd_cell_input():
 def test_gyroid_64_loss_gradients():
     """The gyroid workload (I a -3 d, 64^3, a = 3.7, f_A = 0.40, chi N = 16,
     ds = 0.005, FP64 forward): L = sum_r (phi_A - phi_target)^2 with a seeded
-    smooth target (+-0.1 around f_A); dL/domega at sampled points and dL/da
-    through torch.autograd agree with central differences (h = 1e-6
-    relative for a; 1e-4 for omega, whose single-point effect on the summed
-    loss is below roundoff at 1e-6).  chi does not enter density(omega):
-    dL/dchi = 0."""
+    smooth target (+-0.1 around f_A).  The fields are the workload's
+    parametrisation omega_A = chiN phi_B + delta, omega_B = chiN phi_A - delta
+    with delta the gyroid level-set profile plus noise, projected onto
+    I a -3 d.  Gradients through torch.autograd (the adjoint) against
+    central differences with h = 1e-6 (relative) for a, to 1e-6 relative;
+    dL/dchi N is zero (see below); for omega at single grid points the
+    five-point stencil with h = 1e-3 (relative), to 1e-6 relative: the loss
+    change a one-point step causes is small against the densities' roundoff
+    (about 1e-13 relative per point, summed over 64^3 points), so smaller
+    steps measure that roundoff (1e-5: differences of 4e-6 relative), and
+    the stencil keeps the truncation at O(h^4).  Loss differences are summed
+    from the density difference, L(1) - L(2) = sum (phi1 - phi2)(phi1 + phi2
+    - 2 phi_target), which keeps the roundoff of the two large sums out of
+    the difference."""
     import torch
+    from pscf_b200 import groups
     from pscf_b200.autograd import density
     s = diblock(3, [64, 64, 64], "cubic", [3.7], fA=0.40, chiN=16.0, ds=0.005)
     n = 64
     x = 2 * np.pi * np.arange(n) / n
     Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
     Gy = (np.sin(X) * np.cos(Y) + np.sin(Y) * np.cos(Z) + np.sin(Z) * np.cos(X)).ravel()
-    delta = -(np.abs(Gy) - np.abs(Gy).mean())
-    w0 = s.omega_uniform()
     rng = np.random.default_rng(20261203 + 3)
-    w = np.stack([w0[0] + delta, w0[1] - delta]) + rng.normal(0, 0.01, (2, s.nr))
+    delta = -(np.abs(Gy) - np.abs(Gy).mean()) + rng.normal(0, 0.01, s.nr)
+    delta = groups.symmetrize(delta, "I a -3 d", [n, n, n])
+    phi = s.phi_monomer()
     # target: Gaussian-filtered N(0,1) (sigma = 2 cells), scaled to +-0.1 around f_A
     k = np.fft.fftfreq(n) * n
     KZ, KY, KX = np.meshgrid(k, k, k, indexing="ij")
@@ -192,25 +202,46 @@ def test_gyroid_64_loss_gradients():
     target = 0.40 + 0.1 * t / np.max(np.abs(t))
     e = Engine([s], FP64)
 
-    def loss_np(wv, a):
+    def omega(chi):
+        return np.stack([chi * phi[1] + delta, chi * phi[0] - delta])
+
+    def phi_a(wv, a):
         e.set_cell_param(0, [a])
         rho, _ = e.density(wv[None])
-        return float(((rho[0, 0] - target) ** 2).sum())
+        return rho[0, 0].copy()
 
-    wt = torch.tensor(w[None], dtype=torch.float64, requires_grad=True)
+    def dL(p1, p2):
+        return float(((p1 - p2) * (p1 + p2 - 2.0 * target)).sum())
+
+    chi_t = torch.tensor(16.0, dtype=torch.float64, requires_grad=True)
+    d_t = torch.from_numpy(delta)
+    wt = torch.stack([chi_t * phi[1] + d_t, chi_t * phi[0] - d_t])[None]
+    wt.retain_grad()
     cell = torch.tensor([[3.7]], dtype=torch.float64, requires_grad=True)
     rho, _ = density(wt, e, cell)
     L = ((rho[0, 0] - torch.from_numpy(target)) ** 2).sum()
     L.backward()
     gw = wt.grad.numpy()[0]
-    h = 1e-6 * 3.7
-    fd_a = (loss_np(w, 3.7 + h) - loss_np(w, 3.7 - h)) / (2 * h)
-    assert abs(fd_a - cell.grad.item()) < 1e-5 * max(1.0, abs(fd_a)), (fd_a, cell.grad.item())
+    w = omega(16.0)
+    ha = 1e-6 * 3.7
+    fd_a = dL(phi_a(w, 3.7 + ha), phi_a(w, 3.7 - ha)) / (2 * ha)
+    assert abs(fd_a - cell.grad.item()) < 1e-6 * abs(fd_a), (fd_a, cell.grad.item())
+    # chi N enters omega as a uniform shift of each species' field, which
+    # multiplies qf qr and Q by the same constant: phi, hence L, does not
+    # depend on it.  The adjoint gives that zero (the per-species sums of
+    # dL/domega vanish) and the central difference agrees within its noise.
+    hc = 1e-6 * 16.0
+    fd_chi = dL(phi_a(omega(16.0 + hc), 3.7), phi_a(omega(16.0 - hc), 3.7)) / (2 * hc)
+    assert abs(chi_t.grad.item()) < 1e-10 * abs(fd_a), (chi_t.grad.item(), fd_a)
+    assert abs(fd_chi) < 1e-6 * abs(fd_a), (fd_chi, fd_a)
     for m, r in [(0, 0), (1, 12345), (0, 200000), (1, 77777)]:
-        hw = 1e-4 * max(1.0, abs(w[m, r]))    # a smaller step is below the roundoff of L
-        wp, wm = w.copy(), w.copy()
-        wp[m, r] += hw
-        wm[m, r] -= hw
-        fd = (loss_np(wp, 3.7) - loss_np(wm, 3.7)) / (2 * hw)
-        assert abs(fd - gw[m, r]) < 1e-6 * max(1e-3, abs(fd)) + 1e-10, (m, r, fd, gw[m, r])
+        hw = 1e-3 * abs(w[m, r])
+
+        def at(k):
+            wk = w.copy()
+            wk[m, r] += k * hw
+            return phi_a(wk, 3.7)
+
+        fd = (8.0 * dL(at(1), at(-1)) - dL(at(2), at(-2))) / (12.0 * hw)
+        assert abs(fd - gw[m, r]) < 1e-6 * abs(fd), (m, r, fd, gw[m, r])
     e.close()

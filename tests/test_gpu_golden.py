@@ -52,8 +52,6 @@ def test_bcc_sweep_golden_batched_gpu():
         assert abs(r["mu_chain"][0] - g["mu_chain"][0]) < tol
         assert abs(r["pressure"] - g["pressure"][0]) < tol
         assert abs(r["stress"][0]) < 1e-9
-    np.save(os.path.join(HERE, "..", "gpurun_out", "bcc_sweep_converged.npy"), w) if os.path.isdir(
-        os.path.join(HERE, "..", "gpurun_out")) else None
 
 
 def test_bcc_sweep_relaxed_cells_gpu():

@@ -332,3 +332,32 @@ def test_large_plane_density_uses_line_passes():
     qf, _ = e.propagators(0, 0)
     assert rel_err(qf, qf_ref) < 1e-12
     e.close()
+
+
+ROUGH_CASES = [(3, [64, 64, 64], "cubic", [3.7]), (3, [32, 32, 32], "cubic", [3.9]), (3, [16, 16, 16], "cubic", [3.9])]
+
+
+@pytest.mark.parametrize("dim,ngrid,crystal,cell", ROUGH_CASES)
+@pytest.mark.parametrize("path", ["default", "PSCFG_PLANE_P=0", "PSCFG_GENERIC_KERNELS=1", "PSCFG_SMEM_FFT=1"])
+def test_rough_fields_all_kernel_paths(monkeypatch, dim, ngrid, crystal, cell, path):
+    """White-noise omega and q (every wave vector up to the Nyquist ones
+    carries weight): single steps and a density against the oracle, for
+    each kernel family of the grid."""
+    if path != "default":
+        k, v = path.split("=")
+        monkeypatch.setenv(k, v)
+    s = diblock(dim, ngrid, crystal, cell, fA=0.4, chiN=15.0, ds=0.05)
+    rng = np.random.default_rng(99)
+    w = s.omega_uniform()[:, None] + rng.normal(0.0, 1.0, (2, s.nr))
+    q0 = 1.0 + 0.3 * rng.normal(size=s.nr)
+    o = O.Oracle(s)
+    ksq = o.ksq()
+    e = Engine([s], FP64)
+    ref = O.step(s, ksq, 1.0, 0.05, w[0], q0, 2)
+    got = e.propagate(0, w[0], 1.0, 0.05, q0, 2)
+    assert rel_err(got, ref) < 1e-12, ("step", rel_err(got, ref))
+    rho_ref, q_ref = o.density(w)
+    rho, q = e.density(w[None])
+    assert rel_err(q[0, :1], q_ref) < 1e-12
+    assert rel_err(rho[0], rho_ref) < 1e-12, ("density", rel_err(rho[0], rho_ref))
+    e.close()
