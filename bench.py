@@ -635,11 +635,16 @@ def main():
     ap.add_argument("--no-c4", action="store_true", help="skip the mixed-shape batch leg")
     ap.add_argument("--no-solve", action="store_true",
                     help="time the Anderson iterations only (no full FP64 / mixed solves; profiling runs)")
+    ap.add_argument("--ds", type=float, default=0.0,
+                    help="contour step override (profiling runs on a short contour; same kernels per step)")
     ap.add_argument("--c5-solve", action="store_true",
                     help="also run the full FP64 and mixed-precision solves of the C5 workload (minutes)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.ds > 0:
+        global DS, C5_DS
+        DS = C5_DS = args.ds
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -702,6 +702,51 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
     return false;
 }
 
+// Whether the sweep of this engine runs the plane kernels (kernels3p.cuh).
+static bool plane_kernels_apply(const Engine &E)
+{
+    if (E.dim != 3 || E.no_fixed_kernels || E.smem_fft || E.cluster_step || E.line_step || E.plane_p == 0) return false;
+    const int a = E.n[0], b = E.n[1], c = E.n[2];
+    return (a == 64 && b == 128 && c == 224) || (a == 64 && b == 64 && c == 64);
+}
+
+// Position p of a forward four-step transform of length N (Split<N> of
+// fft_ct.cuh / kernels3p.cuh) -> frequency index.
+static int host_iperm(int N, int p)
+{
+    int P = 1, Q = 1;
+    switch (N) {
+    case 32: P = 4; Q = 8; break;
+    case 64: P = 8; Q = 8; break;
+    case 128: P = 8; Q = 16; break;
+    case 224: P = 16; Q = 14; break;
+    default: P = N; Q = 1; break;
+    }
+    return p / Q + P * (p % Q);
+}
+
+// 1-D factors of exp(-lap k^2/6) and exp(-lap k^2/12) (lap = ds b^2) of an
+// orthogonal cell over the plane kernels' spectrum positions: x (N1/2 + 1),
+// y (N2) and z (N3), each index folded to its minimum image (G_to_bz,
+// src/grid_mod.f90:225-283, along each axis).  Appends 2 (N1/2+1+N2+N3).
+template <typename T>
+static void append_ek_factors(const Engine &E, const Cell &cell, double lap, std::vector<T> &out)
+{
+    const int n1 = E.n[0], n2 = E.n[1], n3 = E.n[2], M = n1 / 2;
+    auto g2 = [&](int axis, int k) {
+        const int n = E.n[axis];
+        const long double kf = (k > n / 2) ? k - n : k;
+        const long double g = (long double)cell.G[axis][axis] * kf;
+        return g * g;
+    };
+    for (int div : {6, 12}) {
+        const long double c = (long double)lap / div;
+        for (int xp = 0; xp <= M; xp++) out.push_back((T)expl(-c * g2(0, xp < M ? host_iperm(M, xp) : M)));
+        for (int yp = 0; yp < n2; yp++) out.push_back((T)expl(-c * g2(1, host_iperm(n2, yp))));
+        for (int zp = 0; zp < n3; zp++) out.push_back((T)expl(-c * g2(2, host_iperm(n3, zp))));
+    }
+}
+
 // A whole 3-D sweep with the shared-memory plane kernels of kernels3p.cuh
 // (64 x 128 x 224 and 64^3; PSCFG_PLANE_P=0 selects the other kernels:
 // run-time shaped at 64 x 128 x 224, k3c at 64^3).  Returns false where not
@@ -877,8 +922,39 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
             }
     }
     if (fl.empty()) return;
+    // separable k-space factors for the plane kernels when every cell of
+    // the launch is orthogonal (written after the descriptors)
+    std::vector<T> ekf;
+    const int L3 = (int)(E.n[0] / 2 + 1) + E.n[1] + E.n[2];
+    if (plane_kernels_apply(E)) {
+        bool ortho = true;
+        for (int i : act)
+            for (int a = 0; a < 3; a++)
+                for (int b2 = 0; b2 < 3; b2++)
+                    if (a != b2 && E.inst[i].cell.G[a][b2] != 0.0) ortho = false;
+        if (ortho) {
+            for (int i : act) {
+                Inst &I = E.inst[i];
+                for (int c = 0; c < I.sys.n_chain; c++)
+                    for (int d = 0; d < 2; d++)
+                        for (int b = 0; b < I.sys.n_block[c]; b++) {
+                            const double kb = I.sys.kuhn[I.sys.block_monomer[c][b]];
+                            append_ek_factors<T>(E, I.cell, I.bds[c][b] * kb * kb, ekf);
+                        }
+            }
+        }
+    }
     TableJob<T> *dtj = E.upload(tj, 0);
     size_t off = ((tj.size() * sizeof(TableJob<T>) + 255) / 256) * 256;
+    if (!ekf.empty()) {
+        const size_t off_tab = off + ((fl.size() * sizeof(SweepField<T>) + 255) / 256) * 256;
+        E.desc(off_tab + ekf.size() * sizeof(T) + 256);   // capacity first: no reallocation below
+        dtj = E.upload(tj, 0);
+        T *dtab = E.upload(ekf, off_tab);
+        size_t k = 0;
+        for (auto &f : fl)
+            for (int b = 0; b < f.nblk; b++, k += 2 * (size_t)L3) f.ekf[b] = dtab + k;
+    }
     SweepField<T> *dfl = E.upload(fl, off);
     {
         dim3 grid((unsigned)std::min<long>((E.nr + 255) / 256, 256), (unsigned)tj.size());

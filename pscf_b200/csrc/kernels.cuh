@@ -29,6 +29,11 @@ struct SweepField {
     // scratch for the multi-pass 3-D step (unused for dim <= 2)
     cx<T> *S1, *S2;
     T *q1;
+    // optional separable k-space factors per block (plane kernels of
+    // kernels3p.cuh, orthogonal cells): exp(-ds b^2 k^2/6) and /12 as
+    // products of 1-D factors over the spectrum's x, y and z positions;
+    // nullptr: the ek1/ek2 tables are read instead
+    const T *ekf[PSCFG_MAXB];
     // optional single-step overrides (adjoint): read `in` instead of the
     // source slice, write `out` instead of the destination slice, and store
     // the step intermediates P1 x (into q1), h = E1 C2 E2 x and P2 x

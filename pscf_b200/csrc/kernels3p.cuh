@@ -357,12 +357,23 @@ __global__ void __launch_bounds__(256, 2) k3p_zconv(const SweepField<T> *fields,
         cp_async_wait_all();
     }
     lf_fft<N3, -1, T, TC, 1, TC>(buf);
+    const T *ekf = f.ekf[blk];
+    if (ekf) {
+        // orthogonal cell: ek = fx[x'] fy[y'] fz[z'] in spectrum positions
+        // (each thread keeps one column: blockDim.x is a multiple of TC)
+        const T *fx = ekf + (sel == 1 ? 0 : NH + N2 + N3), *fy = fx + NH, *fz = fy + N2;
+        const int c = c0 + threadIdx.x % TC;
+        const T exy = fx[c % NH] * fy[c / NH];
 #pragma unroll 7
-    for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
-        const int pz = i / TC, c = c0 + i % TC;
-        const int yp = c / NH, xp = c % NH;
-        const long kidx = PL::kx_of(xp) + (long)NH * (iperm<N2>(yp) + (long)N2 * iperm<N3>(pz));
-        buf[i] = scale(buf[i], __ldg(ek + kidx));
+        for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) buf[i] = scale(buf[i], exy * fz[i / TC]);
+    } else {
+#pragma unroll 7
+        for (int i = threadIdx.x; i < N3 * TC; i += blockDim.x) {
+            const int pz = i / TC, c = c0 + i % TC;
+            const int yp = c / NH, xp = c % NH;
+            const long kidx = PL::kx_of(xp) + (long)NH * (iperm<N2>(yp) + (long)N2 * iperm<N3>(pz));
+            buf[i] = scale(buf[i], __ldg(ek + kidx));
+        }
     }
     lf_fft<N3, 1, T, TC, 1, TC>(buf);
 #pragma unroll 7

@@ -88,10 +88,77 @@ class EngineProvider:
         return dict(rho=rho, q=q, stress=stress)
 
 
+def star_gsq(basis: StarBasis, system: System, cell_param=None) -> np.ndarray:
+    """|G|^2 of every star (its first wave, minimum image over the shifts
+    -1, 0, +1 of each index as in G_to_bz, src/grid_mod.f90:225-283), with
+    the reciprocal basis of the cell (2 pi included, like ksq)."""
+    Gb, _, _ = system.unit_cell(cell_param)
+    dim = system.dim
+    n = np.array(basis.n[:dim])
+    out = np.zeros(basis.n_star)
+    shifts = np.array(np.meshgrid(*[[-1, 0, 1]] * dim, indexing="ij")).reshape(dim, -1).T
+    for s, idx in enumerate(basis.star_idx):
+        w = int(idx[0])
+        g = np.array([w % basis.n[0], (w // basis.n[0]) % basis.n[1], w // (basis.n[0] * basis.n[1])])[:dim]
+        g = np.where(g > n // 2, g - n, g)
+        v = (g[None, :] + shifts * n[None, :]) @ np.asarray(Gb)[:dim, :dim]
+        out[s] = float(np.min((v * v).sum(axis=1)))
+    return out
+
+
+def debye_correlation(system: System, gsq: np.ndarray) -> np.ndarray:
+    """Ideal-chain correlation functions corrlt(alpha, beta, star) of the
+    homogeneous melt at q^2 = |G|^2 (make_correlation,
+    src/response_pd_mod.f90:419-526): per chain, with x_i = L_i b_i^2 q^2/6
+    and f_i = L_i / L, the self terms g1(x_i) f_i^2 phi L and the block-pair
+    terms g2(x_i, x_j) prod_{i<k<j} exp(-x_k) f_i f_j phi L (twice on the
+    diagonal), g1(x) = 2(e^-x + x - 1)/x^2, g2 = (1 - e^-x1)/x1 (1 - e^-x2)/x2."""
+    eps = 1e-14
+
+    def g1(x):
+        return 2.0 * (math.exp(-x) + x - 1.0) / (x * x) if x > eps else 1.0
+
+    def g2(x1, x2):
+        a = (1.0 - math.exp(-x1)) / x1 if x1 > eps else 1.0
+        b = (1.0 - math.exp(-x2)) / x2 if x2 > eps else 1.0
+        return a * b
+
+    M = system.n_monomer
+    kuhn = system.kuhn
+    corr = np.zeros((M, M, len(gsq)))
+    for s, g in enumerate(gsq):
+        q = g / 6.0
+        for ch in system.chains:
+            L = ch.length
+            phiL = ch.phi * L
+            mon = list(ch.block_monomer)
+            x = [lb * kuhn[m] ** 2 * q for lb, m in zip(ch.block_length, mon)]
+            f = [lb / L for lb in ch.block_length]
+            nb = len(mon)
+            for i in range(nb):
+                corr[mon[i], mon[i], s] += g1(x[i]) * f[i] ** 2 * phiL
+            for i in range(nb):
+                for j in range(i + 1, nb):
+                    prop = 1.0
+                    for k in range(i + 1, j):
+                        prop *= math.exp(-x[k])
+                    t = g2(x[i], x[j]) * prop * f[i] * f[j] * phiL
+                    a, b = mon[i], mon[j]
+                    if a == b:
+                        corr[a, a, s] += 2.0 * t
+                    else:
+                        corr[a, b, s] += t
+                        corr[b, a, s] += t
+    return corr
+
+
 def iterate_nr(provider, basis: StarBasis, system: System, omega_grid: np.ndarray, error_max: float = 1e-10,
-               max_itr: int = 100, domain: bool = False, crystal_update=None):
-    """Newton/Broyden solve.  omega_grid [M, nr] (symmetric).  Returns
-    (omega_grid, rho_grid, result dict)."""
+               max_itr: int = 100, domain: bool = False, crystal_update=None, n_cut: Optional[int] = None):
+    """Newton/Broyden solve.  omega_grid [M, nr] (symmetric).  n_cut: the
+    reference's N_cut -- finite-difference Jacobian columns for the first
+    n_cut stars only, the rest from the Debye functions of the homogeneous
+    melt (response_pd_omega, src/response_pd_mod.f90:91-147); None: every
+    star by differences.  Returns (omega_grid, rho_grid, result dict)."""
     M = system.n_monomer
     N = basis.n_star
     ens = system.ensemble
@@ -139,10 +206,14 @@ def iterate_nr(provider, basis: StarBasis, system: System, omega_grid: np.ndarra
         e2 = np.max(np.abs(res[error_index - 1:])) if n_res > 0 else 0.0
         return max(e1, e2 * stress_rescale) if domain else e1
 
+    cut = N if n_cut is None else max(0, min(int(n_cut), N))
+
     def jacobian(om, cl, rho0):
-        # forward differences of rho in every unknown, one batched call
+        # forward differences of rho in the unknowns of the first `cut`
+        # stars, one batched call (response_pd_omega)
         inc = 1e-8
-        cols = [(b, j) for j in range(i0, N) for b in range(M)]
+        nfd = cut if cut > 1 else i0
+        cols = [(b, j) for j in range(i0, nfd) for b in range(M)]
         oms = np.empty((len(cols), M, basis.nr))
         g0 = grid_of(om)
         for c, (b, j) in enumerate(cols):
@@ -156,6 +227,14 @@ def iterate_nr(provider, basis: StarBasis, system: System, omega_grid: np.ndarra
         for c, (b, j) in enumerate(cols):
             p = np.stack([basis.to_basis(out["rho"][c, a]) for a in range(M)])
             drho[:, i0:, b, j] = (p[:, i0:] - rho0[:, i0:]) / inc
+        if nfd < N:
+            # rows of the differenced stars by symmetry, then the diagonal
+            # Debye response beyond them (debye_rsp, :160-180)
+            for j in range(nfd, N):
+                drho[:, i0:nfd, :, j] = np.transpose(drho[:, j, :, i0:nfd], (1, 2, 0))
+            corr = debye_correlation(system, star_gsq(basis, system, cl))
+            for j in range(nfd, N):
+                drho[:, j, :, j] = -corr[:, :, j]
         dxi = np.zeros((N, M, N))                                             # dxi(i, beta, j)
         for j in range(N):
             for b in range(M):

@@ -127,9 +127,12 @@ def test_mixed_precision_matches_fp64_solution():
         assert abs(b["f_helmholtz"] - g["f_Helmholtz"][0]) < 2e-10
 
 
-def test_newton_bcc_golden_batched_jacobian():
+@pytest.mark.parametrize("n_cut", [None, 100])
+def test_newton_bcc_golden_batched_jacobian(n_cut):
     """iterate_NR on the engine: the 290 finite-difference Jacobian columns
-    of the BCC fixture (146 stars) are one batched density call."""
+    of the BCC fixture (146 stars) are one batched density call; with
+    N_cut = 100 (the fixture's own setting) 198 columns are differenced and
+    the 46 shortest-wavelength stars take the Debye tail."""
     from pscf_b200.basis import StarBasis
     from pscf_b200.newton import EngineProvider, iterate_nr
     g = GOLD["bcc_sweep"][0]
@@ -143,7 +146,7 @@ def test_newton_bcc_golden_batched_jacobian():
     w0, _, _ = e.iterate_am(sphere_guess(s, s.chains[0].block_length[0], width=0.05)[None], error_max=1e-3,
                             max_itr=200)
     prov = EngineProvider(s, "I m -3 m", max_batch=146)
-    w, rho, r = iterate_nr(prov, basis, s, w0[0], error_max=1e-10, max_itr=40)
+    w, rho, r = iterate_nr(prov, basis, s, w0[0], error_max=1e-10, max_itr=40, n_cut=n_cut)
     assert r["converged"], r["error"]
     e.density(w[None])
     f, p, mu = e.free_energy()

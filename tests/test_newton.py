@@ -69,3 +69,35 @@ def test_newton_lamellar_golden(domain):
     assert abs(mu[0] - g["mu_chain"][0]) < 1e-10
     if domain:
         assert abs(r["cell_param"][0] - g["cell_param"][0]) < 1e-9
+
+
+@pytest.mark.parametrize("domain", [False, True])
+def test_newton_lamellar_golden_n_cut(domain):
+    """N_cut = 8 of 17 stars: finite differences for the first 8, the
+    Debye tail beyond (response_pd_omega / debye_rsp,
+    src/response_pd_mod.f90:91-180); Newton lands on the same golden state."""
+    g = GOLD["lamellar_outfile"]
+    cell0 = g["cell_param"][0] * (1.03 if domain else 1.0)
+    s = diblock(1, [32], "lamellar", [cell0], fA=0.5, chiN=g["chi"][0])
+    basis = StarBasis("-1", [32])
+    prov = OracleProvider(s, "-1")
+    w, rho, r = iterate_nr(prov, basis, s, lamellar_guess(s), error_max=1e-11, max_itr=80, domain=domain, n_cut=8)
+    assert r["converged"]
+    o = prov.o
+    o.set_cell(r["cell_param"])
+    rr, q = o.density(w)
+    f, p = o.free_energy(w, rr)
+    assert abs(f - g["f_Helmholtz"][0]) < 1e-10
+    if domain:
+        assert abs(r["cell_param"][0] - g["cell_param"][0]) < 1e-9
+
+
+def test_debye_correlation_limits():
+    """q -> 0: corrlt_ab = phi f_a f_b (g1 = g2 = 1); large q: the self term
+    decays like 2/x."""
+    from pscf_b200.newton import debye_correlation
+    s = diblock(1, [32], "lamellar", [1.7], fA=0.3, chiN=15.0)
+    c = debye_correlation(s, np.array([0.0, 1e6]))
+    np.testing.assert_allclose(c[:, :, 0], [[0.09, 0.21], [0.21, 0.49]], rtol=1e-14)
+    x = 0.3 * 1e6 / 6.0
+    assert abs(c[0, 0, 1] - 0.09 * 2.0 * (x - 1.0) / x ** 2) < 1e-15
