@@ -303,6 +303,30 @@ int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, 
 int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_dev, const double *omega_dev, double b,
                             double ds, const double *q_in_dev, double *q_out_dev, int nsteps, void *stream);
 
+/* Star basis of instance `inst` for pscfg_density_basis (the reference's
+ * basis_mod / grid_basis_mod tables, src/basis_mod.f90,
+ * src/grid_basis_mod.f90:47-200): n_wave waves of the r2c half grid, wave j
+ * at flat index wave_k[j] = kx + (n1/2+1)(ky + n2 kz) (0 <= kx <= n1/2), in
+ * star wave_star[j] (0-based), with complex coefficient
+ * (coeff[2j], coeff[2j+1]) of the star's basis function
+ * f_s(r) = sum_G c_s(G) exp(i G.r) over all waves G; the waves outside the
+ * half grid are the Hermitian partners, c_s(-G) = conj c_s(G).  Each
+ * half-grid wave appears at most once; waves of cancelled stars are left
+ * out.  The tables (sorted by star) stay on the device. */
+int pscfg_set_basis(pscfg_engine *e, int inst, int n_star, int n_wave, const int *wave_k, const int *wave_star,
+                    const double *coeff);
+
+/* density() with omega and rho as star coefficients, as the reference's
+ * density(N, omega, rho, qout, q_solvent) takes them
+ * (src/scf_mod.fp.f90:144-229): basis_to_kgrid and the inverse FFT of omega,
+ * the propagators and contour integrals, the forward FFT and kgrid_to_basis
+ * of rho, all on the device (one gather/scatter kernel each).  Coefficients
+ * a_s = <f, f_s> (grid averages).  omega_basis / rho_basis: host
+ * [n_inst][n_monomer][n_star_i], instances one after another (each with its
+ * own n_star); rho_basis may be NULL; q, q_solvent as in pscfg_density.
+ * Every instance needs pscfg_set_basis first (PSCFG_ESTATE otherwise). */
+int pscfg_density_basis(pscfg_engine *e, const double *omega_basis, double *rho_basis, double *q, double *q_solvent);
+
 /* Stored propagators of chain `chain` of instance `inst` after a density
  * call (chain_grid_type%qf/qr, src/chain_mod.f90:39-50): host
  * [n_slices][nr] each (either may be NULL); returns the slice count in

@@ -83,6 +83,33 @@ class StarBasis:
             self.star_gsq.append(float(gsq[w]))
         self.n_star = len(self.star_idx)
 
+    def half_grid_tables(self):
+        """The waves of every star that lie in the r2c half grid
+        (0 <= kx <= n1/2): their flat half-grid index kx + (n1/2+1)(ky + n2 kz),
+        star index and coefficient -- the device tables of
+        pscfg_set_basis.  The partner -G of every wave must belong to the
+        same star with the conjugate coefficient (centrosymmetric groups)."""
+        n = self.n
+        n1h = n[0] // 2 + 1
+        flat = lambda g: g[..., 0] + n[0] * (g[..., 1] + n[1] * g[..., 2])
+        ks, ss, cs = [], [], []
+        for s, (idx, c) in enumerate(zip(self.star_idx, self.star_coef)):
+            x = idx % n[0]
+            rest = idx // n[0]
+            g = np.stack([x, rest % n[1], rest // n[1]], axis=1)
+            neg = flat((-g) % np.array(n))
+            pos = {int(k): i for i, k in enumerate(idx)}
+            for i, kneg in enumerate(neg):
+                j = pos.get(int(kneg), -1)
+                if j < 0 or abs(c[j] - np.conj(c[i])) > 1e-12:
+                    raise NotImplementedError("star basis tables need each wave's partner -G in its star "
+                                              "(centrosymmetric groups)")
+            keep = x <= n[0] // 2
+            ks.append(x[keep] + n1h * rest[keep])
+            ss.append(np.full(int(keep.sum()), s))
+            cs.append(c[keep])
+        return np.concatenate(ks), np.concatenate(ss), np.concatenate(cs)
+
     def _fft(self, f):
         n = self.n
         return np.fft.fftn(np.asarray(f, dtype=np.float64).reshape(n[2], n[1], n[0])).ravel(order="C")

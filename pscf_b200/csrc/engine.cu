@@ -35,6 +35,7 @@
 #include "response.cuh"
 #include "kernels3l.cuh"
 #include "kernels3p.cuh"
+#include "basis.cuh"
 
 namespace pscfg {
 
@@ -109,6 +110,12 @@ struct Inst {
     int *d_orb_perm = nullptr;   // real-space orbits of the group on the grid
     int *d_orb_start = nullptr;
     int norb = 0;
+    // star basis for basis-coefficient fields (pscfg_set_basis): CSR tables
+    // sorted by star in one device buffer
+    int n_star = 0, n_wave = 0;
+    void *basis_buf = nullptr;
+    const int *b_start = nullptr, *b_k = nullptr, *b_star = nullptr;
+    const cx<double> *b_c = nullptr;
     double *kweight = nullptr;    // [nk] star weights (nullptr: exact Parseval weights)
     double *wdg0 = nullptr;       // [MAXCP][nk] stress weights without star weights (set with kweight)
 };
@@ -171,6 +178,8 @@ struct Engine {
     double *hsm() { return hpin + (size_t)hpin_inst * 32; }
     void *spec = nullptr;        // 3-D stress spectra scratch
     void *fe_spec = nullptr;     // spectra for the star-weighted free energy
+    void *basis_scr = nullptr;   // pscfg_density_basis: spectra and coefficients
+    size_t basis_scr_bytes = 0;
     size_t fe_spec_bytes = 0;
     size_t spec_bytes = 0;
     double *stress_part = nullptr;
@@ -190,6 +199,9 @@ struct Engine {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+        for (auto &I : inst)
+            if (I.basis_buf) cudaFree(I.basis_buf);
+        if (basis_scr) cudaFree(basis_scr);
         if (hpin) cudaFreeHost(hpin);
         if (st) cudaStreamDestroy(st);
     }
@@ -3097,6 +3109,190 @@ int pscfg_am_results(pscfg_engine *e, double *omega, double *rho, pscfg_am_resul
     am_results(e->E, e->am, res);
     for (size_t i = 0; i < res.size(); i++) results[i] = res[i];
     store_fields(e->E, omega, rho);
+    ABI_END(e)
+}
+
+int pscfg_set_basis(pscfg_engine *e, int inst, int n_star, int n_wave, const int *wave_k, const int *wave_star,
+                    const double *coeff)
+{
+    if (!e || n_star < 0 || n_wave < 0 || (n_wave > 0 && (!wave_k || !wave_star || !coeff))) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    if (inst < 0 || inst >= (int)E.inst.size()) throw Err(PSCFG_EINVAL, "instance index out of range");
+    Inst &I = E.inst[inst];
+    std::vector<char> seen(E.nk, 0);
+    std::vector<int> order(n_wave), count(n_star + 1, 0);
+    for (int j = 0; j < n_wave; j++) {
+        if (wave_k[j] < 0 || wave_k[j] >= E.nk) throw Err(PSCFG_EINVAL, "wave index outside the half grid");
+        if (wave_star[j] < 0 || wave_star[j] >= n_star) throw Err(PSCFG_EINVAL, "star index out of range");
+        if (seen[wave_k[j]]) throw Err(PSCFG_EINVAL, "a half-grid wave appears twice in the basis");
+        seen[wave_k[j]] = 1;
+        count[wave_star[j] + 1]++;
+    }
+    for (int s2 = 0; s2 < n_star; s2++) count[s2 + 1] += count[s2];
+    {   // stable sort by star
+        std::vector<int> pos(count.begin(), count.end() - 1);
+        for (int j = 0; j < n_wave; j++) order[pos[wave_star[j]]++] = j;
+    }
+    const size_t a256 = 256;
+    auto al = [&](size_t b) { return (b + a256 - 1) / a256 * a256; };
+    const size_t o_k = al(sizeof(int) * (n_star + 1)), o_s = o_k + al(sizeof(int) * n_wave),
+                 o_c = o_s + al(sizeof(int) * n_wave), total = o_c + sizeof(cx<double>) * std::max(n_wave, 1);
+    std::vector<unsigned char> h(total, 0);
+    std::memcpy(h.data(), count.data(), sizeof(int) * (n_star + 1));
+    for (int j = 0; j < n_wave; j++) {
+        const int src = order[j];
+        ((int *)(h.data() + o_k))[j] = wave_k[src];
+        ((int *)(h.data() + o_s))[j] = wave_star[src];
+        ((double *)(h.data() + o_c))[2 * j] = coeff[2 * src];
+        ((double *)(h.data() + o_c))[2 * j + 1] = coeff[2 * src + 1];
+    }
+    if (I.basis_buf) {
+        CK(cudaStreamSynchronize(E.st));
+        cudaFree(I.basis_buf);
+        I.basis_buf = nullptr;
+    }
+    CK(cudaMalloc(&I.basis_buf, total));
+    CK(cudaMemcpy(I.basis_buf, h.data(), total, cudaMemcpyHostToDevice));
+    unsigned char *d = (unsigned char *)I.basis_buf;
+    I.b_start = (const int *)d;
+    I.b_k = (const int *)(d + o_k);
+    I.b_star = (const int *)(d + o_s);
+    I.b_c = (const cx<double> *)(d + o_c);
+    I.n_star = n_star;
+    I.n_wave = n_wave;
+    ABI_END(e)
+}
+
+// Half spectra -> real fields (unnormalised c2r), or real fields -> half
+// spectra (unnormalised r2c), for nf fields.
+static void field_ffts(Engine &E, const std::vector<const double *> &re_in, const std::vector<double *> &re_out,
+                       const std::vector<cx<double> *> &spec, bool inverse)
+{
+    const PlaneGeom &g = E.g64;
+    const int nf = (int)spec.size();
+    if (nf == 0) return;
+    cx<double> **dspec = E.upload(spec, 0);
+    size_t off = ((spec.size() * sizeof(void *) + 255) / 256) * 256;
+    const size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<double>);
+    const long P = (long)g.n1h * g.n2;
+    const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
+    const size_t smz = 2 * (size_t)g.n3 * Z_TILE * sizeof(cx<double>);
+    if (smxy > 227 * 1024 || (E.dim == 3 && smz > 227 * 1024))
+        throw Err(PSCFG_EINVAL, "grid plane too large for the basis maps");
+    if (inverse) {
+        double **dout = E.upload(re_out, off);
+        if (E.dim <= 2) {
+            CK(allow_dyn_smem((const void *)k2_ifft_fields));
+            const int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
+            k2_ifft_fields<<<nf, threads, smxy, E.st>>>((const cx<double> *const *)dspec, dout, g);
+            E.launched();
+        } else {
+            CK(allow_dyn_smem((const void *)k3_ifft_fields_z<Z_TILE>));
+            CK(allow_dyn_smem((const void *)k3_ifft_fields_xy));
+            k3_ifft_fields_z<Z_TILE><<<dim3(ntile, nf), 256, smz, E.st>>>(dspec, g);
+            E.launched();
+            k3_ifft_fields_xy<<<dim3(g.n3, nf), 256, smxy, E.st>>>((const cx<double> *const *)dspec, dout, g);
+            E.launched();
+        }
+    } else {
+        const double **din = (const double **)E.upload(re_in, off);
+        if (E.dim <= 2) {
+            CK(allow_dyn_smem((const void *)k2_fft_fields));
+            const int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
+            k2_fft_fields<<<nf, threads, smxy, E.st>>>(din, dspec, g);
+            E.launched();
+        } else {
+            CK(allow_dyn_smem((const void *)k3_fft_fields_xy));
+            CK(allow_dyn_smem((const void *)k3_fft_fields_z<Z_TILE>));
+            k3_fft_fields_xy<<<dim3(g.n3, nf), 256, smxy, E.st>>>(din, dspec, g);
+            E.launched();
+            k3_fft_fields_z<Z_TILE><<<dim3(ntile, nf), 256, smz, E.st>>>(dspec, g);
+            E.launched();
+        }
+    }
+}
+
+int pscfg_density_basis(pscfg_engine *e, const double *omega_basis, double *rho_basis, double *q, double *q_solvent)
+{
+    if (!e || !omega_basis) return PSCFG_EINVAL;
+    ABI_BEGIN
+    Engine &E = e->E;
+    const int ni = (int)E.inst.size(), M = E.M;
+    long ncoef = 0, max_star = 0, max_wave = 0;
+    for (auto &I : E.inst) {
+        if (!I.basis_buf) throw Err(PSCFG_ESTATE, "pscfg_density_basis needs pscfg_set_basis on every instance");
+        ncoef += (long)M * I.n_star;
+        max_star = std::max<long>(max_star, I.n_star);
+        max_wave = std::max<long>(max_wave, I.n_wave);
+    }
+    // scratch: one half spectrum per (instance, monomer), coefficients in and out
+    const size_t spec_bytes = sizeof(cx<double>) * (size_t)E.nk * ni * M;
+    const size_t need = spec_bytes + 2 * sizeof(double) * (size_t)std::max<long>(ncoef, 1);
+    if (E.basis_scr_bytes < need) {
+        if (E.basis_scr) {
+            CK(cudaStreamSynchronize(E.st));
+            cudaFree(E.basis_scr);
+        }
+        E.basis_scr = nullptr;
+        CK(cudaMalloc(&E.basis_scr, need));
+        E.basis_scr_bytes = need;
+    }
+    cx<double> *spec = (cx<double> *)E.basis_scr;
+    double *cin = (double *)((char *)E.basis_scr + spec_bytes), *cout = cin + std::max<long>(ncoef, 1);
+    CK(cudaMemcpyAsync(cin, omega_basis, sizeof(double) * ncoef, cudaMemcpyHostToDevice, E.st));
+    CK(cudaMemsetAsync(spec, 0, spec_bytes, E.st));
+    std::vector<BasisJob> jobs;
+    std::vector<cx<double> *> sp;
+    std::vector<double *> wout;
+    std::vector<const double *> rin;
+    long off_c = 0;
+    for (int i = 0; i < ni; i++) {
+        Inst &I = E.inst[i];
+        for (int a = 0; a < M; a++) {
+            BasisJob j;
+            j.start = I.b_start;
+            j.wave_k = I.b_k;
+            j.wave_star = I.b_star;
+            j.c = I.b_c;
+            j.n_star = I.n_star;
+            j.n_wave = I.n_wave;
+            j.S = spec + ((size_t)i * M + a) * E.nk;
+            j.a = cin + off_c;
+            j.out = cout + off_c;
+            off_c += I.n_star;
+            jobs.push_back(j);
+            sp.push_back(j.S);
+            wout.push_back(I.omega + (long)a * E.nr);
+            rin.push_back(I.rho + (long)a * E.nr);
+        }
+    }
+    const int nj = (int)jobs.size();
+    // basis_to_kgrid + inverse FFT: omega on the grid
+    BasisJob *dj = E.upload(jobs, (size_t)4 << 20);
+    k_basis_scatter<<<dim3((unsigned)std::max<long>(1, std::min<long>((max_wave + 255) / 256, 1024)), nj), 256, 0, E.st>>>(dj);
+    E.launched();
+    field_ffts(E, {}, wout, sp, true);
+    std::vector<int> all(ni);
+    for (int i = 0; i < ni; i++) all[i] = i;
+    density_all(E, all);
+    if (rho_basis) {
+        // forward FFT + kgrid_to_basis of rho
+        field_ffts(E, rin, {}, sp, false);
+        dj = E.upload(jobs, (size_t)4 << 20);
+        k_basis_gather<<<dim3((unsigned)std::max<long>(1, (max_star + 7) / 8), nj), 256, 0, E.st>>>(dj, E.n[0],
+                                                                                                   1.0 / (double)E.nr);
+        E.launched();
+        CK(cudaMemcpyAsync(rho_basis, cout, sizeof(double) * ncoef, cudaMemcpyDeviceToHost, E.st));
+    }
+    CK(cudaStreamSynchronize(E.st));
+    for (int i = 0; i < ni; i++) {
+        if (q)
+            for (int c = 0; c < PSCFG_MAXC; c++) q[(long)i * PSCFG_MAXC + c] = (c < E.inst[i].sys.n_chain) ? E.inst[i].Q[c] : 0.0;
+        if (q_solvent)
+            for (int s2 = 0; s2 < PSCFG_MAXS; s2++)
+                q_solvent[(long)i * PSCFG_MAXS + s2] = (s2 < E.inst[i].sys.n_solvent) ? E.inst[i].Qs[s2] : 0.0;
+    }
     ABI_END(e)
 }
 

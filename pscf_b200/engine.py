@@ -109,6 +109,8 @@ SIGNATURES = {
     "pscfg_am_iterate": (C.c_int, [_vp, C.c_int, C.POINTER(C.c_int)]),
     "pscfg_am_results": (C.c_int, [_vp, _dp, _dp, C.POINTER(PscfgAmResult)]),
     "pscfg_set_symmetry": (C.c_int, [_vp, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "pscfg_set_basis": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
+    "pscfg_density_basis": (C.c_int, [_vp, _dp, _dp, _dp, _dp]),
     "pscfg_stream": (C.c_void_p, [_vp]),
     "pscfg_set_profiling": (C.c_int, [_vp, C.c_int]),
     "pscfg_get_profile": (C.c_int, [_vp, _dp]),
@@ -334,6 +336,36 @@ class Engine:
         ops[:, :9] = M.reshape(len(M), 9)
         ops[:, 9:] = t
         self._check(self.lib.pscfg_set_symmetry(self._h, inst, len(M), ops.ctypes.data_as(C.POINTER(C.c_int))))
+
+    def set_basis(self, inst: int, basis):
+        """Star basis (pscf_b200.basis.StarBasis of a centrosymmetric group)
+        of instance `inst` for density_basis: the waves of its stars that lie
+        in the r2c half grid, with their coefficients, as device tables."""
+        k, star, coef = basis.half_grid_tables()
+        ck = np.ascontiguousarray(k, dtype=np.int32)
+        cs = np.ascontiguousarray(star, dtype=np.int32)
+        cc = np.ascontiguousarray(np.stack([coef.real, coef.imag], axis=1), dtype=np.float64).ravel()
+        self._check(self.lib.pscfg_set_basis(self._h, inst, basis.n_star, len(ck),
+                                             ck.ctypes.data_as(C.POINTER(C.c_int)),
+                                             cs.ctypes.data_as(C.POINTER(C.c_int)), _ptr(cc)))
+        if not hasattr(self, "_n_star"):
+            self._n_star = [0] * self.n_inst
+        self._n_star[inst] = basis.n_star
+
+    def density_basis(self, omega_basis):
+        """density() in star coefficients: omega_basis is a list (or array)
+        of [n_monomer, n_star_i] per instance; returns (rho_basis list, q)."""
+        ws = [np.ascontiguousarray(w, dtype=np.float64).reshape(self.M, self._n_star[i])
+              for i, w in enumerate(omega_basis)]
+        flat = np.concatenate([w.ravel() for w in ws])
+        rho = np.zeros_like(flat)
+        q = np.zeros((self.n_inst, MAX_CHAIN))
+        self._check(self.lib.pscfg_density_basis(self._h, _ptr(flat), _ptr(rho), _ptr(q), None))
+        out, o = [], 0
+        for w in ws:
+            out.append(rho[o:o + w.size].reshape(w.shape))
+            o += w.size
+        return out, q
 
     def clear_symmetry(self, inst: int):
         self._check(self.lib.pscfg_set_symmetry(self._h, inst, 0, None))
