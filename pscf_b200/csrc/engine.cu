@@ -779,15 +779,19 @@ static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
         CK(allow_dyn_smem((const void *)k3p_zconv<T, N1, N2, N3, TC>));
         const PlaneGeom g = E.geom();
         const unsigned ztiles = (unsigned)(PL::PS / TC);
+        int dev = 0, nsm = 148;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const int pf = 2 * nsm;   // CTAs of k3p_zconv resident at once (2 per SM)
         auto emit = [&]() {
             k3p_fwd_pair<T, N1, N2, N3><<<dim3(N3, nf), 256, smp, E.st>>>(dfl, g, 0);
             E.launched();
             for (int t = 0; t < ns_max; t++) {
-                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 2), 256, smz, E.st>>>(dfl, g, t, 3);
+                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 2), 256, smz, E.st>>>(dfl, g, t, 3, pf);
                 E.launched();
                 k3p_mid<T, N1, N2, N3><<<dim3(N3, nf, 2), 256, smp, E.st>>>(dfl, g, t);
                 E.launched();
-                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 1), 256, smz, E.st>>>(dfl, g, t, 2);
+                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 1), 256, smz, E.st>>>(dfl, g, t, 2, pf);
                 E.launched();
                 k3p_final_fwd<T, N1, N2, N3><<<dim3(N3, nf), 256, smp, E.st>>>(dfl, g, t);
                 E.launched();

@@ -155,6 +155,14 @@ __device__ __forceinline__ void copy_in(void *smem, const void *gmem)
     cp_async_wait_all();
 }
 
+// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned) into L2 by
+// one thread: planes that a kernel reads only after its transforms are in
+// L2 by then, so the pointwise passes wait for L2 instead of DRAM.
+__device__ __forceinline__ void prefetch_l2(const void *p, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
 template <typename T> struct Pair;
 template <> struct Pair<double> { using V = double2; };
 template <> struct Pair<float> { using V = float2; };
@@ -329,9 +337,12 @@ __global__ void __launch_bounds__(256, 2) k3p_fwd_pair(const SweepField<T> *fiel
 
 // K2/K4: S <- Fz^-1[ek . Fz[S]] on a tile of TC columns (positions c =
 // y' NH + x').  which: 1 = S1/ek1, 2 = S2/ek2, 3 = both (grid.z selects).
-// grid = (N2 NH / TC, nfields, 1 or 2), 256 threads.
+// grid = (N2 NH / TC, nfields, 1 or 2), 256 threads.  pf_stride > 0: the
+// first warp also prefetches into L2 the tile of CTA blockIdx.x + pf_stride
+// (the CTA that runs one resident wave later, on the same spectrum).
 template <typename T, int N1, int N2, int N3, int TC>
-__global__ void __launch_bounds__(256, 2) k3p_zconv(const SweepField<T> *fields, PlaneGeom g, int t, int which)
+__global__ void __launch_bounds__(256, 2) k3p_zconv(const SweepField<T> *fields, PlaneGeom g, int t, int which,
+                                                    int pf_stride)
 {
     using PL = PlaneP<T, N1, N2>;
     constexpr int NH = PL::NH, P = PL::PS;
@@ -345,6 +356,10 @@ __global__ void __launch_bounds__(256, 2) k3p_zconv(const SweepField<T> *fields,
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *buf = (cx<T> *)smem_raw;
     const int c0 = blockIdx.x * TC;
+    if (pf_stride > 0 && threadIdx.x < 32 && blockIdx.x + pf_stride < gridDim.x) {
+        const cx<T> *nx = S + (long)(blockIdx.x + pf_stride) * TC;
+        for (int z = threadIdx.x; z < N3; z += 32) prefetch_l2(nx + (long)z * P, TC * (unsigned)sizeof(cx<T>));
+    }
     {
         // TC consecutive columns of each z row: RB 16-byte chunks per row
         constexpr int RB = TC * (int)sizeof(cx<T>) / 16;
@@ -398,6 +413,7 @@ __global__ void __launch_bounds__(256, 2) k3p_mid(const SweepField<T> *fields, P
     const T rn = (T)((long)N1 * N2 * N3);
     const int z = blockIdx.x;
     const T *eo2 = f.eo2[blk] + (long)z * PL::NP;
+    if (threadIdx.x == 0) prefetch_l2(eo2, PL::NP * (unsigned)sizeof(T));
     if (blockIdx.z == 0) {
         T *q1 = f.q1 + (long)z * PL::NP;
         PL::load(buf, f.S1 + (long)z * PL::PS);
@@ -439,6 +455,11 @@ __global__ void __launch_bounds__(256, 2) k3p_final_fwd(const SweepField<T> *fie
     int blk2, src2, dst2;
     const bool next = step_slices(f, t + 1, blk2, src2, dst2);   // the same for the whole CTA
     const T *n2 = f.eo2[next ? blk2 : blk] + (long)z * PL::NP;
+    if (threadIdx.x == 0) {
+        prefetch_l2(eo2, PL::NP * (unsigned)sizeof(T));
+        prefetch_l2(q1, PL::NP * (unsigned)sizeof(T));
+        if (n2 != eo2) prefetch_l2(n2, PL::NP * (unsigned)sizeof(T));
+    }
     PL::load(buf, f.S2 + (long)z * PL::PS);
     PL::inverse(buf);
     PL::each_pair(buf, [&](cx<T> &s, int e) {
