@@ -128,6 +128,11 @@ struct Engine {
     int M = 0;
     std::vector<Inst> inst;
     cudaStream_t st = nullptr;
+    // second branch of the plane-kernel sweeps: the fields of a small batch
+    // split in two independent kernel chains (fork/join events on st)
+    cudaStream_t st2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    bool no_branch = false;          // PSCFG_NO_BRANCH=1: one chain
     std::string err;
     long launches = 0;
     int n_hist_alloc = 0;
@@ -203,6 +208,9 @@ struct Engine {
             if (I.basis_buf) cudaFree(I.basis_buf);
         if (basis_scr) cudaFree(basis_scr);
         if (hpin) cudaFreeHost(hpin);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (st2) cudaStreamDestroy(st2);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -467,8 +475,13 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
         E.planes = pl ? std::atoi(pl) : 0;
         const char *pp = std::getenv("PSCFG_PLANE_P");
         if (pp && pp[0]) E.plane_p = std::atoi(pp);
+        const char *nb = std::getenv("PSCFG_NO_BRANCH");
+        E.no_branch = nb && nb[0] && nb[0] != '0';
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&E.st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
     upload_dft_constants();
     make_geom<double>(E, E.g64);
     if (precision != PSCFG_FP64) make_geom<float>(E, E.g32);
@@ -783,19 +796,38 @@ static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
         const int pf = 2 * nsm;   // CTAs of k3p_zconv resident at once (2 per SM)
-        auto emit = [&]() {
-            k3p_fwd_pair<T, N1, N2, N3><<<dim3(N3, nf), 256, smp, E.st>>>(dfl, g, 0);
-            E.launched();
-            for (int t = 0; t < ns_max; t++) {
-                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 2), 256, smz, E.st>>>(dfl, g, t, 3, pf);
+        // a small batch's fields run as two independent kernel chains (the
+        // qf and qr sweeps of one instance, for instance), so that each
+        // launch's last, partly empty wave overlaps the other chain's work
+        const int h = (nf >= 2 && nf <= 8 && !E.no_branch) ? nf / 2 : 0;
+        auto step = [&](const SweepField<T> *d, int n, cudaStream_t s, int t) {
+            if (t < 0) {
+                k3p_fwd_pair<T, N1, N2, N3><<<dim3(N3, n), 256, smp, s>>>(d, g, 0);
                 E.launched();
-                k3p_mid<T, N1, N2, N3><<<dim3(N3, nf, 2), 256, smp, E.st>>>(dfl, g, t);
-                E.launched();
-                k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, nf, 1), 256, smz, E.st>>>(dfl, g, t, 2, pf);
-                E.launched();
-                k3p_final_fwd<T, N1, N2, N3><<<dim3(N3, nf), 256, smp, E.st>>>(dfl, g, t);
-                E.launched();
+                return;
             }
+            k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, n, 2), 256, smz, s>>>(d, g, t, 3, pf);
+            E.launched();
+            k3p_mid<T, N1, N2, N3><<<dim3(N3, n, 2), 256, smp, s>>>(d, g, t);
+            E.launched();
+            k3p_zconv<T, N1, N2, N3, TC><<<dim3(ztiles, n, 1), 256, smz, s>>>(d, g, t, 2, pf);
+            E.launched();
+            k3p_final_fwd<T, N1, N2, N3><<<dim3(N3, n), 256, smp, s>>>(d, g, t);
+            E.launched();
+        };
+        auto emit = [&]() {
+            if (h == 0) {
+                for (int t = -1; t < ns_max; t++) step(dfl, nf, E.st, t);
+                return;
+            }
+            CK(cudaEventRecord(E.ev_fork, E.st));
+            CK(cudaStreamWaitEvent(E.st2, E.ev_fork, 0));
+            for (int t = -1; t < ns_max; t++) {
+                step(dfl, h, E.st, t);
+                step(dfl + h, nf - h, E.st2, t);
+            }
+            CK(cudaEventRecord(E.ev_join, E.st2));
+            CK(cudaStreamWaitEvent(E.st, E.ev_join, 0));
         };
         graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), emit);
     };
