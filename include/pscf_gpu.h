@@ -50,6 +50,17 @@ extern "C" {
                               to FP64 once its error is below the switch error or
                               stops improving; other calls run in FP64 */
 
+/* OR-ed into pscfg_create's precision: propagator checkpointing.  Each
+ * chain keeps every K-th slice of qf and qr (K = ceil(sqrt(Ns)) of the
+ * batch's longest chain) and two K + 1 slice working segments instead of
+ * all Ns + 1 slices; density, stress and the adjoint recompute each segment
+ * from its checkpoint with the same step kernels (about 1.5x the sweep
+ * work of a density, 2x for the stress and the adjoint).  The reference
+ * stores every slice (chain_grid_type%qf/qr, src/chain_mod.f90:159-165);
+ * results agree with the stored-slice engine to roundoff.  Not available
+ * with pscfg_response. */
+#define PSCFG_CHECKPOINT 0x100
+
 /* crystal systems (src/unit_cell_mod.f90:309-664) */
 #define PSCFG_LAMELLAR 0
 #define PSCFG_SQUARE 10

@@ -116,6 +116,11 @@ struct Inst {
     void *basis_buf = nullptr;
     const int *b_start = nullptr, *b_k = nullptr, *b_star = nullptr;
     const cx<double> *b_c = nullptr;
+    // checkpointing (PSCFG_CHECKPOINT): qf/qr hold the checkpoint slices
+    // min(j K, ns), j = 0..nseg; segA/segB are K + 1 slice working segments
+    int nseg[PSCFG_MAXC] = {};
+    void *segA[PSCFG_MAXC] = {}, *segB[PSCFG_MAXC] = {};
+    double *simp_w[PSCFG_MAXC] = {};   // [ns + 1][MAXM] per-slice Simpson weights
     double *kweight = nullptr;    // [nk] star weights (nullptr: exact Parseval weights)
     double *wdg0 = nullptr;       // [MAXCP][nk] stress weights without star weights (set with kweight)
 };
@@ -133,6 +138,8 @@ struct Engine {
     cudaStream_t st2 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     bool no_branch = false;          // PSCFG_NO_BRANCH=1: one chain
+    bool ckpt = false;               // PSCFG_CHECKPOINT
+    int ckK = 0;                     // checkpoint interval (slices)
     std::string err;
     long launches = 0;
     int n_hist_alloc = 0;
@@ -147,7 +154,7 @@ struct Engine {
     // CUDA graphs of 3-D sweeps, keyed by descriptor address, field and step count
     struct SweepGraph {
         const void *dfl;
-        int nf, ns, tsize;
+        int nf, ns, tsize, t0;
         cudaGraphExec_t exec;
         long launches;
     };
@@ -445,6 +452,13 @@ struct PhaseTimer {
 static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int precision)
 {
     if (n_inst < 1) throw Err(PSCFG_EINVAL, "n_inst must be >= 1");
+    E.ckpt = (precision & PSCFG_CHECKPOINT) != 0;
+    precision &= ~PSCFG_CHECKPOINT;
+    if (E.ckpt && precision != PSCFG_FP64) {
+        long nr = 1;
+        for (int d = 0; d < sys[0].dim && d < 3; d++) nr *= sys[0].n[d];
+        if (nr % 2) throw Err(PSCFG_EINVAL, "PSCFG_CHECKPOINT with FP32 propagation needs an even number of grid points");
+    }
     if (precision != PSCFG_FP64 && precision != PSCFG_FP32 && precision != PSCFG_MIXED)
         throw Err(PSCFG_EINVAL, "unknown precision");
     E.prec = precision;
@@ -487,6 +501,18 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     if (precision != PSCFG_FP64) make_geom<float>(E, E.g32);
 
     const size_t ts = E.tsize();
+    if (E.ckpt) {
+        // K = ceil(sqrt(Ns)) of the longest chain of the batch
+        int ns_max = 1;
+        for (int i = 0; i < n_inst; i++)
+            for (int c = 0; c < sys[i].n_chain && c < PSCFG_MAXC; c++) {
+                if (sys[i].n_block[c] < 1 || sys[i].n_block[c] > PSCFG_MAXB) continue;
+                int bgn[PSCFG_MAXB + 1];
+                double bds[PSCFG_MAXB];
+                ns_max = std::max(ns_max, chain_grid(sys[i].n_block[c], sys[i].block_length[c], sys[i].chain_step, bgn, bds));
+            }
+        E.ckK = std::max(1, (int)std::ceil(std::sqrt((double)ns_max)));
+    }
     E.inst.resize(n_inst);
     for (int i = 0; i < n_inst; i++) {
         pscfg_system s = sys[i];
@@ -507,8 +533,27 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
             I.ns[c] = chain_grid(s.n_block[c], s.block_length[c], s.chain_step, I.bgn[c], I.bds[c]);
             I.length[c] = 0;
             for (int b = 0; b < s.n_block[c]; b++) I.length[c] += s.block_length[c][b];
-            I.qf[c] = E.dalloc(ts * E.nr * (I.ns[c] + 1));
-            I.qr[c] = E.dalloc(ts * E.nr * (I.ns[c] + 1));
+            if (E.ckpt) {
+                const int K = E.ckK;
+                I.nseg[c] = (I.ns[c] + K - 1) / K;
+                I.qf[c] = E.dalloc(ts * E.nr * (I.nseg[c] + 1));
+                I.qr[c] = E.dalloc(ts * E.nr * (I.nseg[c] + 1));
+                I.segA[c] = E.dalloc(ts * E.nr * (K + 1));
+                I.segB[c] = E.dalloc(ts * E.nr * (K + 1));
+                std::vector<double> w((size_t)(I.ns[c] + 1) * PSCFG_MAXM, 0.0);
+                for (int b = 0; b < s.n_block[c]; b++) {
+                    const int ib = I.bgn[c][b], ie = I.bgn[c][b + 1], m = s.block_monomer[c][b];
+                    for (int j = ib; j <= ie; j++) {
+                        const double wt = (j == ib || j == ie) ? 1.0 : (((j - ib) % 2 == 1) ? 4.0 : 2.0);
+                        w[(size_t)j * PSCFG_MAXM + m] += I.bds[c][b] / 3.0 * wt;
+                    }
+                }
+                I.simp_w[c] = (double *)E.dalloc(sizeof(double) * w.size());
+                CK(cudaMemcpy(I.simp_w[c], w.data(), sizeof(double) * w.size(), cudaMemcpyHostToDevice));
+            } else {
+                I.qf[c] = E.dalloc(ts * E.nr * (I.ns[c] + 1));
+                I.qr[c] = E.dalloc(ts * E.nr * (I.ns[c] + 1));
+            }
             I.inc[c] = (double *)E.dalloc(sizeof(double) * PSCFG_MAXCP * (I.ns[c] + 1));
             for (int b = 0; b < s.n_block[c]; b++) {
                 I.eo1[c][b] = E.dalloc(ts * E.nr);
@@ -629,14 +674,14 @@ static int sweep_planes(const Engine &E, int nf, int n3, int pmax)
 // field count, step count, precision) and replayed after each descriptor
 // upload (PSCFG_NO_GRAPHS=1 launches directly).
 template <typename Emit>
-static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsize, Emit emit)
+static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsize, int t0, Emit emit)
 {
     if (E.no_graphs) {
         emit();
         return;
     }
     for (auto &g : E.graphs)
-        if (g.dfl == dfl && g.nf == nf && g.ns == ns_max && g.tsize == tsize) {
+        if (g.dfl == dfl && g.nf == nf && g.ns == ns_max && g.tsize == tsize && g.t0 == t0) {
             CK(cudaGraphLaunch(g.exec, E.st));
             E.launches += g.launches;
             return;
@@ -646,6 +691,7 @@ static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsiz
     sg.nf = nf;
     sg.ns = ns_max;
     sg.tsize = tsize;
+    sg.t0 = t0;
     const long l0 = E.launches;
     CK(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
@@ -661,7 +707,7 @@ static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsiz
     cudaGraphDestroy(graph);
     CK(ie);
     sg.launches = E.launches - l0;
-    if (E.graphs.size() >= 16) {
+    if (E.graphs.size() >= (E.ckpt ? 96u : 16u)) {
         cudaGraphExecDestroy(E.graphs.front().exec);
         E.graphs.erase(E.graphs.begin());
     }
@@ -673,7 +719,7 @@ static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsiz
 // every step fused with the first of the next.  Returns false where the
 // grid has no such kernels (or another path was requested).
 template <typename T>
-static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
+static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int t0 = 0)
 {
     if (E.no_fixed_kernels || E.smem_fft || E.cluster_step) return false;
     // The sweep is a fixed sequence of 1 + 4 ns_max launches whose jobs are
@@ -689,9 +735,9 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
         const dim3 gp(N / PPC, nf);
         const unsigned rtile = (unsigned)((P + 63) / 64);
         auto emit = [&]() {
-            k3r_fwd_pair<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, 0);
+            k3r_fwd_pair<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t0);
             E.launched();
-            for (int t = 0; t < ns_max; t++) {
+            for (int t = t0; t < ns_max; t++) {
                 k3s_zconv<T, N, N, N, true><<<dim3(rtile, nf, 2), 128, 0, E.st>>>(dfl, t, 3);
                 E.launched();
                 k3r_inv_mid<T, N, N, N, PPC><<<gp, 128, sm, E.st>>>(dfl, t);
@@ -702,7 +748,7 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
                 E.launched();
             }
         };
-        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), emit);
+        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), t0, emit);
     };
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 32 && b == 32 && c == 32) {
@@ -778,7 +824,7 @@ static void append_ek_factors(const Engine &E, const Cell &cell, double lap, std
 // applicable.  64^3, 4 instances, FP64 sweep: 61.3k field-steps/s against
 // 30.8k with the k3c kernels; 64 x 128 x 224, 1 instance: 8.0k against 2.5k.
 template <typename T>
-static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
+static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int t0 = 0)
 {
     if (E.no_fixed_kernels || E.smem_fft || E.cluster_step || E.line_step || E.plane_p == 0) return false;
     auto run = [&](auto n1c, auto n2c, auto n3c, auto tcc) {
@@ -801,8 +847,8 @@ static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
         // launch's last, partly empty wave overlaps the other chain's work
         const int h = (nf >= 2 && nf <= 8 && !E.no_branch) ? nf / 2 : 0;
         auto step = [&](const SweepField<T> *d, int n, cudaStream_t s, int t) {
-            if (t < 0) {
-                k3p_fwd_pair<T, N1, N2, N3><<<dim3(N3, n), 256, smp, s>>>(d, g, 0);
+            if (t < t0) {
+                k3p_fwd_pair<T, N1, N2, N3><<<dim3(N3, n), 256, smp, s>>>(d, g, t0);
                 E.launched();
                 return;
             }
@@ -817,19 +863,19 @@ static bool sweep3p(Engine &E, const SweepField<T> *dfl, int nf, int ns_max)
         };
         auto emit = [&]() {
             if (h == 0) {
-                for (int t = -1; t < ns_max; t++) step(dfl, nf, E.st, t);
+                for (int t = t0 - 1; t < ns_max; t++) step(dfl, nf, E.st, t);
                 return;
             }
             CK(cudaEventRecord(E.ev_fork, E.st));
             CK(cudaStreamWaitEvent(E.st2, E.ev_fork, 0));
-            for (int t = -1; t < ns_max; t++) {
+            for (int t = t0 - 1; t < ns_max; t++) {
                 step(dfl, h, E.st, t);
                 step(dfl + h, nf - h, E.st2, t);
             }
             CK(cudaEventRecord(E.ev_join, E.st2));
             CK(cudaStreamWaitEvent(E.st, E.ev_join, 0));
         };
-        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), emit);
+        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), t0, emit);
     };
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 64 && b == 128 && c == 224) {
@@ -919,6 +965,9 @@ static bool step3_fixed(Engine &E, const SweepField<T> *dfl, int nf, int t)
     if (a == 64 && b == 64 && c == 64) { step3c<T, 64, 64, 64, 1>(E, dfl, nf, t); return true; }
     return false;
 }
+
+template <typename T>
+static void sweep_steps(Engine &E, const SweepField<T> *dfl, int nf, int t0, int t1);
 
 template <typename T>
 static void run_sweeps(Engine &E, const std::vector<int> &act)
@@ -1012,13 +1061,22 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
         k_init_ends<T><<<g2, 256, 0, E.st>>>(dfl, E.nr);
         E.launched();
     }
-    const int nf = (int)fl.size();
+    sweep_steps<T>(E, dfl, (int)fl.size(), 0, ns_max);
+}
+
+// Steps t in [t0, t1) of every field at dfl (t counts the steps of each
+// field's own sweep, step_slices), on whichever kernels the grid has.
+template <typename T>
+static void sweep_steps(Engine &E, const SweepField<T> *dfl, int nf, int t0, int t1)
+{
+    const PlaneGeom &g = E.geom();
+    const int ns_max = t1;
     if (E.dim <= 2) {
         size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)E.nr * sizeof(T);
         if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
         CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
         int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
-        k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, 0, ns_max);
+        k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, t0, t1);
         E.launched();
     } else {
         size_t smxy = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>);
@@ -1032,9 +1090,9 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
         const long P = (long)g.n1h * g.n2;
         const int ntile = (int)((P + Z_TILE - 1) / Z_TILE);
         const int txy = 256, tz = 256;
-        if (sweep3r<T>(E, dfl, nf, ns_max)) return;
-        if (sweep3p<T>(E, dfl, nf, ns_max)) return;
-        for (int t = 0; t < ns_max; t++) {
+        if (sweep3r<T>(E, dfl, nf, ns_max, t0)) return;
+        if (sweep3p<T>(E, dfl, nf, ns_max, t0)) return;
+        for (int t = t0; t < ns_max; t++) {
             if (step3_fixed<T>(E, dfl, nf, t)) continue;
             if (step3l<T>(E, dfl, nf, t)) continue;
             k3_fwd_pair<T><<<dim3(g.n3, nf), txy, smxy, E.st>>>(dfl, g, t);
@@ -1061,7 +1119,7 @@ static void run_contour(Engine &E, const std::vector<int> &act)
     for (int i : act) {
         Inst &I = E.inst[i];
         for (int c = 0; c < I.sys.n_chain; c++) {
-            qp.push_back((const T *)I.qf[c] + (long)I.ns[c] * E.nr);
+            qp.push_back((const T *)I.qf[c] + (long)(E.ckpt ? I.nseg[c] : I.ns[c]) * E.nr);
             qout.push_back(I.Qdev + c);
         }
     }
@@ -1140,6 +1198,18 @@ static void run_contour(Engine &E, const std::vector<int> &act)
             for (int s = 0; s < I.sys.n_solvent; s++) I.sys.phi_solvent[s] = I.Qs[s] * std::exp(I.sys.mu_solvent[s]);
         }
     }
+    if (E.ckpt) {
+        // the checkpointed density accumulates its Simpson sums segment by
+        // segment (density_ckpt); start rho from the solvent part or zero
+        for (int i : act) {
+            Inst &I = E.inst[i];
+            if (I.sys.n_solvent == 0) {
+                k_zero<<<(unsigned)std::min<long>((E.M * E.nr + 255) / 256, 1024), 256, 0, E.st>>>(I.rho, (long)E.M * E.nr);
+                E.launched();
+            }
+        }
+        return;
+    }
     // Simpson jobs grouped by instance
     std::vector<SimpsonJob> simp;
     std::vector<int> start;
@@ -1177,9 +1247,294 @@ static void run_contour(Engine &E, const std::vector<int> &act)
     E.launched();
 }
 
+
+static void copy_list(Engine &E, const std::vector<CopyJob> &jobs, long maxn);
+template <typename T>
+static void slice_dots(Engine &E, const std::vector<StressJob<T>> &jobs);
+
+// ---------------------------------------------------------------------
+// Propagator checkpointing (PSCFG_CHECKPOINT)
+// ---------------------------------------------------------------------
+// A chain's slices are cut into segments [j K, min((j+1) K, ns)], j < nseg.
+// qf/qr hold the checkpoint slices min(j K, ns), j = 0..nseg; a segment is
+// recomputed from its checkpoint into segA (qf, upward) or segB (qr,
+// downward) by the ordinary sweep kernels, through descriptors whose slab
+// points K slices before the segment buffer (step_slices indexes the
+// absolute slice).  A recomputed segment repeats the checkpointing pass's
+// operations exactly, so it equals the slices that pass produced; against
+// an uninterrupted sweep the slices agree to the last bits (a segment's
+// first step starts from the checkpoint in global memory, where the fused
+// sweep kernels carry it over from the previous step).
+struct CkChain {
+    int inst, c;
+};
+
+// the k-space tables of every block, and the separable factors of the plane
+// kernels, for the chains of `act` (as run_sweeps builds them)
+template <typename T>
+static void ckpt_tables(Engine &E, const std::vector<int> &act, std::vector<const T *> &ekf_of)
+{
+    std::vector<TableJob<T>> tj;
+    for (int i : act) {
+        Inst &I = E.inst[i];
+        for (int c = 0; c < I.sys.n_chain; c++)
+            for (int b = 0; b < I.sys.n_block[c]; b++) {
+                TableJob<T> j;
+                int m = I.sys.block_monomer[c][b];
+                j.omega = I.omega + (long)m * E.nr;
+                j.ksq = I.ksq;
+                j.eo1 = (T *)I.eo1[c][b];
+                j.eo2 = (T *)I.eo2[c][b];
+                j.ek1 = (T *)I.ek1[c][b];
+                j.ek2 = (T *)I.ek2[c][b];
+                j.ds = I.bds[c][b];
+                j.b = I.sys.kuhn[m];
+                tj.push_back(j);
+            }
+    }
+    ekf_of.clear();
+    std::vector<T> ekf;
+    const int L3 = (int)(E.n[0] / 2 + 1) + E.n[1] + E.n[2];
+    bool sep = plane_kernels_apply(E);
+    for (int i : act)
+        for (int a = 0; a < 3; a++)
+            for (int b2 = 0; b2 < 3; b2++)
+                if (a != b2 && E.inst[i].cell.G[a][b2] != 0.0) sep = false;
+    const size_t off_tab = (size_t)6 << 20;
+    if (sep) {
+        for (int i : act) {
+            Inst &I = E.inst[i];
+            for (int c = 0; c < I.sys.n_chain; c++)
+                for (int b = 0; b < I.sys.n_block[c]; b++) {
+                    const double kb = I.sys.kuhn[I.sys.block_monomer[c][b]];
+                    append_ek_factors<T>(E, I.cell, I.bds[c][b] * kb * kb, ekf);
+                }
+        }
+        if (ekf.size() * sizeof(T) > ((size_t)2 << 20)) sep = false;   // keep below the geometry region
+    }
+    E.desc(((size_t)8 << 20) + 256);
+    TableJob<T> *dtj = E.upload(tj, 0);
+    dim3 grid((unsigned)std::min<long>((E.nr + 255) / 256, 256), (unsigned)tj.size());
+    k_make_tables<T><<<grid, 256, 0, E.st>>>(dtj, E.nr, E.nk);
+    E.launched();
+    if (sep) {
+        T *dtab = E.upload(ekf, off_tab);
+        size_t k = 0;
+        for (int i : act) {
+            Inst &I = E.inst[i];
+            for (int c = 0; c < I.sys.n_chain; c++) {
+                ekf_of.push_back(dtab + k);
+                k += (size_t)I.sys.n_block[c] * 2 * L3;
+            }
+        }
+    }
+}
+
+// Recomputes (or, with store, computes and checkpoints) segment j of the
+// chains `ch`: dir > 0 qf into segA from checkpoint j (store: its top into
+// checkpoint j + 1); dir < 0 qr into segB from checkpoint j + 1 (store: its
+// bottom into checkpoint j).  Chains whose nseg <= j are skipped.
+template <typename T>
+static void ckpt_segment(Engine &E, const std::vector<CkChain> &ch, const std::vector<const T *> &ekf_of, int j,
+                         int dir, bool store)
+{
+    const int K = E.ckK;
+    const long nr = E.nr;
+    const int L3 = (int)(E.n[0] / 2 + 1) + E.n[1] + E.n[2];
+    // qr segments of chains with different ns need different step ranges:
+    // one launch group per ns
+    std::vector<int> groups;
+    for (size_t k = 0; k < ch.size(); k++) {
+        const Inst &I = E.inst[ch[k].inst];
+        if (j >= I.nseg[ch[k].c]) continue;
+        const int key = dir > 0 ? 0 : I.ns[ch[k].c];
+        if (std::find(groups.begin(), groups.end(), key) == groups.end()) groups.push_back(key);
+    }
+    for (int key : groups) {
+        std::vector<SweepField<T>> fl;
+        std::vector<CopyJob> pre, post;
+        int t0 = 0, t1 = 0;
+        for (size_t k = 0; k < ch.size(); k++) {
+            Inst &I = E.inst[ch[k].inst];
+            const int c = ch[k].c, ns = I.ns[c];
+            if (j >= I.nseg[c] || (dir < 0 && ns != key)) continue;
+            const int s0 = j * K, s1 = std::min((j + 1) * K, ns), len = s1 - s0;
+            T *seg = (T *)(dir > 0 ? I.segA[c] : I.segB[c]);
+            T *ck = (T *)(dir > 0 ? I.qf[c] : I.qr[c]);
+            SweepField<T> f;
+            std::memset(&f, 0, sizeof(f));
+            f.slab = seg - (long)s0 * nr;   // slice s at seg + (s - s0) nr
+            f.ns = ns;
+            f.dir = dir;
+            f.nblk = I.sys.n_block[c];
+            for (int b = 0; b <= f.nblk; b++) f.bgn[b] = I.bgn[c][b];
+            for (int b = 0; b < f.nblk; b++) {
+                f.eo1[b] = (const T *)I.eo1[c][b];
+                f.eo2[b] = (const T *)I.eo2[c][b];
+                f.ek1[b] = (const T *)I.ek1[c][b];
+                f.ek2[b] = (const T *)I.ek2[c][b];
+                if (!ekf_of.empty()) f.ekf[b] = ekf_of[k] + (size_t)b * 2 * L3;
+            }
+            const int d = dir > 0 ? 0 : 1;
+            f.S1 = (cx<T> *)I.S1[2 * c + d];
+            f.S2 = (cx<T> *)I.S2[2 * c + d];
+            f.q1 = (T *)I.q1[2 * c + d];
+            fl.push_back(f);
+            if (dir > 0) {
+                pre.push_back(CopyJob{(const double *)(ck + (long)j * nr), (double *)seg, 0});
+                if (store) post.push_back(CopyJob{(const double *)(seg + (long)len * nr), (double *)(ck + (long)(j + 1) * nr), 0});
+                t0 = s0;
+                t1 = std::max(t1, s1);
+            } else {
+                pre.push_back(CopyJob{(const double *)(ck + (long)(j + 1) * nr), (double *)(seg + (long)len * nr), 0});
+                if (store) post.push_back(CopyJob{(const double *)seg, (double *)(ck + (long)j * nr), 0});
+                t0 = ns - s1;
+                t1 = ns - s0;
+            }
+        }
+        if (fl.empty()) continue;
+        // CopyJob counts doubles: a slice of nr T is nr * sizeof(T) / 8 doubles
+        const long ncopy = nr * (long)sizeof(T) / (long)sizeof(double);
+        for (auto &cj : pre) cj.n = ncopy;
+        for (auto &cj : post) cj.n = ncopy;
+        copy_list(E, pre, ncopy);
+        SweepField<T> *dfl = E.upload(fl, 0);
+        sweep_steps<T>(E, dfl, (int)fl.size(), t0, t1);
+        if (store) copy_list(E, post, ncopy);
+    }
+}
+
+// density() with checkpoints: qf segment by segment (checkpointing), Q and
+// solvents, then from the last segment down: qf recomputed, qr propagated
+// (checkpointing), and the segment's Simpson sums added to rho.
+template <typename T>
+static void density_ckpt(Engine &E, const std::vector<int> &act)
+{
+    std::vector<CkChain> ch;
+    int nseg_max = 0;
+    for (int i : act)
+        for (int c = 0; c < E.inst[i].sys.n_chain; c++) {
+            ch.push_back(CkChain{i, c});
+            nseg_max = std::max(nseg_max, E.inst[i].nseg[c]);
+        }
+    {
+        long l0 = E.launches;
+        PhaseTimer pt(E, &E.t_sweep);
+        std::vector<const T *> ekf_of;
+        ckpt_tables<T>(E, act, ekf_of);
+        // qf(0) = 1 and qr(ns) = 1: the first and the last checkpoints
+        std::vector<SweepField<T>> ends;
+        for (auto &k : ch) {
+            Inst &I = E.inst[k.inst];
+            SweepField<T> f;
+            std::memset(&f, 0, sizeof(f));
+            f.slab = (T *)I.qf[k.c];
+            f.ns = I.nseg[k.c];
+            f.dir = 1;
+            ends.push_back(f);
+            f.slab = (T *)I.qr[k.c];
+            f.dir = -1;
+            ends.push_back(f);
+        }
+        SweepField<T> *de = E.upload(ends, 0);
+        dim3 g2((unsigned)std::min<long>((E.nr + 255) / 256, 256), (unsigned)ends.size());
+        k_init_ends<T><<<g2, 256, 0, E.st>>>(de, E.nr);
+        E.launched();
+        for (int j = 0; j < nseg_max; j++) ckpt_segment<T>(E, ch, ekf_of, j, +1, true);
+        if (E.profiling) {
+            for (int i : act)
+                for (int c = 0; c < E.inst[i].sys.n_chain; c++) E.n_steps_timed += 2L * E.inst[i].ns[c];
+            E.sweep_launches += E.launches - l0;
+        }
+    }
+    {
+        PhaseTimer pc(E, &E.t_contour);
+        run_contour<T>(E, act);   // Q from the last checkpoint, solvents, rho zeroed
+    }
+    {
+        PhaseTimer pt(E, &E.t_sweep);
+        std::vector<const T *> ekf_of;
+        ckpt_tables<T>(E, act, ekf_of);
+        const int K = E.ckK;
+        for (int j = nseg_max - 1; j >= 0; j--) {
+            ckpt_segment<T>(E, ch, ekf_of, j, +1, false);
+            ckpt_segment<T>(E, ch, ekf_of, j, -1, true);
+            std::vector<SimpsonSegJob> sj;
+            std::vector<int> start;
+            for (int i : act) {
+                Inst &I = E.inst[i];
+                start.push_back((int)sj.size());
+                for (int c = 0; c < I.sys.n_chain; c++) {
+                    if (j >= I.nseg[c]) continue;
+                    SimpsonSegJob J;
+                    J.qf = I.segA[c];
+                    J.qr = I.segB[c];
+                    J.w = I.simp_w[c];
+                    J.Q = I.Qdev + c;
+                    J.phi_over_L = I.sys.phi_chain[c] / I.length[c];
+                    J.s0 = j * K;
+                    J.s1 = (j == I.nseg[c] - 1) ? I.ns[c] + 1 : (j + 1) * K;   // each slice once
+                    J.n_monomer = E.M;
+                    J.rho = I.rho;
+                    sj.push_back(J);
+                }
+            }
+            start.push_back((int)sj.size());
+            if (sj.empty()) continue;
+            SimpsonSegJob *dsj = E.upload(sj, 0);
+            const size_t o2 = ((sj.size() * sizeof(SimpsonSegJob) + 255) / 256) * 256;
+            int *dst = E.upload(start, o2);
+            dim3 grid((unsigned)std::min<long>((E.nr + 255) / 256, 1024), (unsigned)act.size());
+            k_simpson_seg<T><<<grid, 256, 0, E.st>>>(dsj, dst, E.nr);
+            E.launched();
+        }
+    }
+}
+
+// The stress slice sums with checkpoints: both propagators of every
+// segment recomputed from their checkpoints, then slice_dots on the
+// segment buffers into the slice sums of its slices.
+template <typename T>
+static void stress_slices_ckpt(Engine &E, const std::vector<int> &act)
+{
+    std::vector<CkChain> ch;
+    int nseg_max = 0;
+    for (int i : act)
+        for (int c = 0; c < E.inst[i].sys.n_chain; c++) {
+            ch.push_back(CkChain{i, c});
+            nseg_max = std::max(nseg_max, E.inst[i].nseg[c]);
+        }
+    std::vector<const T *> ekf_of;
+    ckpt_tables<T>(E, act, ekf_of);
+    const int K = E.ckK;
+    for (int j = 0; j < nseg_max; j++) {
+        ckpt_segment<T>(E, ch, ekf_of, j, +1, false);
+        ckpt_segment<T>(E, ch, ekf_of, j, -1, false);
+        std::vector<StressJob<T>> jobs;
+        for (auto &k : ch) {
+            Inst &I = E.inst[k.inst];
+            if (j >= I.nseg[k.c]) continue;
+            const int s0 = j * K, s1 = std::min((j + 1) * K, I.ns[k.c]);
+            StressJob<T> sjob;
+            sjob.qf = (const T *)I.segA[k.c];
+            sjob.qr = (const T *)I.segB[k.c];
+            sjob.wdgsq = I.wdgsq;
+            sjob.ncp = I.cell.ncp;
+            sjob.nslices = s1 - s0 + 1;
+            sjob.inc = I.inc[k.c] + (long)s0 * PSCFG_MAXCP;
+            jobs.push_back(sjob);
+        }
+        if (!jobs.empty()) slice_dots<T>(E, jobs);
+    }
+}
+
 template <typename T>
 static void density_impl(Engine &E, const std::vector<int> &act)
 {
+    if (E.ckpt) {
+        density_ckpt<T>(E, act);
+        return;
+    }
     {
         long l0 = E.launches;
         PhaseTimer pt(E, &E.t_sweep);
@@ -1461,6 +1816,7 @@ static void stress_impl(Engine &E, const std::vector<int> &act)
 {
     const PlaneGeom &g = E.geom();
     std::vector<StressJob<T>> jobs;
+    if (E.ckpt) stress_slices_ckpt<T>(E, act);
     for (int i : act) {
         Inst &I = E.inst[i];
         for (int c = 0; c < I.sys.n_chain; c++) {
@@ -1475,7 +1831,7 @@ static void stress_impl(Engine &E, const std::vector<int> &act)
         }
     }
     if (jobs.empty()) return;
-    slice_dots<T>(E, jobs);
+    if (!E.ckpt) slice_dots<T>(E, jobs);
     const size_t off = ((jobs.size() * sizeof(StressJob<T>) + 255) / 256) * 256;
     std::vector<StressFinal> fin;
     for (int i : act) {
@@ -2264,8 +2620,48 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
         cg = (double *)cscr.get(sizeof(double) * PSCFG_MAXCP * act.size());
         CK(cudaMemsetAsync(cg, 0, sizeof(double) * PSCFG_MAXCP * act.size(), E.st));
     }
-    std::vector<double> Sc(ov.size());
-    {
+    std::vector<double> Sc(ov.size(), 0.0);
+    std::vector<const T *> ekf_of;
+    if (E.ckpt) {
+        // overlaps segment by segment from the recomputed propagators
+        ckpt_tables<T>(E, act, ekf_of);
+        std::vector<CkChain> ch;
+        int nseg_max = 0;
+        for (auto &ic : ov_ic) {
+            ch.push_back(CkChain{act[ic.first], ic.second});
+            nseg_max = std::max(nseg_max, E.inst[act[ic.first]].nseg[ic.second]);
+        }
+        const int K = E.ckK;
+        for (int j = 0; j < nseg_max; j++) {
+            ckpt_segment<T>(E, ch, ekf_of, j, +1, false);
+            ckpt_segment<T>(E, ch, ekf_of, j, -1, false);
+            std::vector<AdjOverlap> os;
+            std::vector<size_t> idx;
+            for (size_t q = 0; q < ov.size(); q++) {
+                Inst &I = E.inst[ch[q].inst];
+                const int c = ch[q].c;
+                if (j >= I.nseg[c]) continue;
+                AdjOverlap o = ov[q];
+                o.qf = I.segA[c];
+                o.qr = I.segB[c];
+                o.coef = I.adj_coef[c] + (size_t)j * K * PSCFG_MAXM;
+                o.nslices = (j == I.nseg[c] - 1) ? I.ns[c] + 1 - j * K : K;
+                os.push_back(o);
+                idx.push_back(q);
+            }
+            if (os.empty()) continue;
+            AdjOverlap *dov = E.upload(os, 0);
+            double *part = E.part((size_t)nct * os.size());
+            k_adj_overlap<T><<<dim3(nct, (unsigned)os.size()), 256, 0, E.st>>>(dov, nr, part);
+            E.launched();
+            k_final_sum<<<(unsigned)((os.size() + 127) / 128), 128, 0, E.st>>>(part, nct, 1.0, E.d_small, (int)os.size());
+            E.launched();
+            std::vector<double> h(os.size());
+            CK(cudaMemcpyAsync(h.data(), E.d_small, sizeof(double) * os.size(), cudaMemcpyDeviceToHost, E.st));
+            CK(cudaStreamSynchronize(E.st));
+            for (size_t q = 0; q < os.size(); q++) Sc[idx[q]] += h[q];
+        }
+    } else {
         AdjOverlap *dov = E.upload(ov, off);
         off += ((ov.size() * sizeof(AdjOverlap) + 255) / 256) * 256;
         double *part = E.part((size_t)nct * ov.size());
@@ -2289,7 +2685,10 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
             std::memset(&a, 0, sizeof(a));
             a.lam = S.lam[0];
             a.G = G[k];
-            a.other = (S.d == 0) ? (const T *)I.qr[S.c] + (long)j * nr : (const T *)I.qf[S.c] + (long)j * nr;
+            if (E.ckpt)   // the end slices are the checkpoints nseg (qr) and 0 (qf)
+                a.other = (S.d == 0) ? (const T *)I.qr[S.c] + (long)I.nseg[S.c] * nr : (const T *)I.qf[S.c];
+            else
+                a.other = (S.d == 0) ? (const T *)I.qr[S.c] + (long)j * nr : (const T *)I.qf[S.c] + (long)j * nr;
             for (int m = 0; m < E.M; m++) a.coef[m] = S.coef[(size_t)j * PSCFG_MAXM + m];
             a.M = E.M;
             if (S.d == 0) {
@@ -2308,10 +2707,18 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
     int ns_max = 0;
     for (auto &S : sw) ns_max = std::max(ns_max, S.ns);
     const PlaneGeom &g = E.geom();
-    for (int t = 0; t < ns_max; t++) {
+    // slice s of chain c of instance I: propagator 0 = qf, 1 = qr (stored
+    // slabs, or the loaded checkpoint segment j_seg)
+    int j_seg = -1;
+    auto slice = [&](const Inst &I, int c, int which, int sl) -> const T * {
+        if (!E.ckpt) return (const T *)(which == 0 ? I.qf[c] : I.qr[c]) + (long)sl * nr;
+        return (const T *)(which == 0 ? I.segA[c] : I.segB[c]) + (long)(sl - j_seg * E.ckK) * nr;
+    };
+    auto adj_step = [&](int t, const std::vector<size_t> &sel) {
         std::vector<SweepField<T>> fl;
         std::vector<AdjPoint> pts;
-        for (auto &S : sw) {
+        for (size_t si : sel) {
+            auto &S = sw[si];
             if (t >= S.ns) continue;
             Inst &I = E.inst[S.inst];
             size_t k = 0;
@@ -2323,14 +2730,14 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
                 qslice = S.ns - 1 - t;            // step qf_j -> qf_{j+1}
                 newslice = qslice;
                 blk = seg_block(I, S.c, qslice);
-                qsrc = (const T *)I.qf[S.c] + (long)qslice * nr;
-                other = (const T *)I.qr[S.c] + (long)newslice * nr;
+                qsrc = slice(I, S.c, 0, qslice);
+                other = slice(I, S.c, 1, newslice);
             } else {
                 qslice = t + 1;                   // step qr_s -> qr_{s-1}
                 newslice = qslice;
                 blk = seg_block(I, S.c, qslice - 1);
-                qsrc = (const T *)I.qr[S.c] + (long)qslice * nr;
-                other = (const T *)I.qf[S.c] + (long)newslice * nr;
+                qsrc = slice(I, S.c, 1, qslice);
+                other = slice(I, S.c, 0, newslice);
             }
             for (int f = 0; f < 2; f++) {
                 SweepField<T> F;
@@ -2387,7 +2794,8 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
             std::vector<StressJob<double>> cj;
             std::vector<AdjCellAcc> ca;
             int k = 0;
-            for (auto &S : sw) {
+            for (size_t si : sel) {
+                auto &S = sw[si];
                 if (t >= S.ns) continue;
                 Inst &I = E.inst[S.inst];
                 size_t kin = 0;
@@ -2434,6 +2842,37 @@ static void adjoint_impl(Engine &E, const std::vector<int> &act, const std::vect
                 AdjCellAcc *dca = E.upload(ca, (size_t)9 << 20);
                 k_adj_cellacc<<<1, 32, 0, E.st>>>(dca, k);
                 E.launched();
+            }
+        }
+    };
+    if (!E.ckpt) {
+        std::vector<size_t> all(sw.size());
+        for (size_t q = 0; q < sw.size(); q++) all[q] = q;
+        for (int t = 0; t < ns_max; t++) adj_step(t, all);
+    } else {
+        // one chain and direction at a time, the segment holding the step's
+        // slices recomputed when the step leaves the loaded one
+        const int K = E.ckK;
+        for (size_t q = 0; q < sw.size(); q++) {
+            auto &S = sw[q];
+            const std::vector<CkChain> one{CkChain{S.inst, S.c}};
+            j_seg = -1;
+            for (int t = 0; t < S.ns; t++) {
+                const int sl = (S.d == 0) ? S.ns - 1 - t : t + 1;
+                const int j = (S.d == 0) ? sl / K : (sl - 1) / K;
+                if (j != j_seg) {
+                    std::vector<const T *> ekf1;
+                    if (!ekf_of.empty()) {
+                        size_t pos = 0;
+                        for (size_t r = 0; r < ov_ic.size(); r++)
+                            if (act[ov_ic[r].first] == S.inst && ov_ic[r].second == S.c) pos = r;
+                        ekf1.push_back(ekf_of[pos]);
+                    }
+                    ckpt_segment<T>(E, one, ekf1, j, +1, false);
+                    ckpt_segment<T>(E, one, ekf1, j, -1, false);
+                    j_seg = j;
+                }
+                adj_step(t, std::vector<size_t>{q});
             }
         }
     }
@@ -2528,6 +2967,7 @@ static void response_impl(Engine &E, int inst, const double kvec[3], double ktra
                           const double *read_coef, double *out)
 {
     Inst &I = E.inst[inst];
+    if (E.ckpt) throw Err(PSCFG_ESTATE, "pscfg_response reads every stored propagator slice (not kept with PSCFG_CHECKPOINT)");
     if (!I.have_density) throw Err(PSCFG_ESTATE, "the response requires a preceding density call");
     if (E.prec == PSCFG_FP32 || I.dens_prec != PSCFG_FP64)
         throw Err(PSCFG_EINVAL, "the response runs on FP64 propagators");
@@ -3554,6 +3994,45 @@ int pscfg_get_propagators(pscfg_engine *e, int inst, int chain, double *qf, doub
     if (chain < 0 || chain >= I.sys.n_chain) throw Err(PSCFG_EINVAL, "chain index out of range");
     const long ns = I.ns[chain] + 1;
     if (n_slices) *n_slices = (int)ns;
+    if (E.ckpt && (qf || qr)) {
+        // rebuild the slices from the checkpoints, segment by segment
+        if (!I.have_density) throw Err(PSCFG_ESTATE, "no propagators before a density call");
+        const bool f32 = I.dens_prec == PSCFG_FP32;
+        E.cur = f32 ? PSCFG_FP32 : PSCFG_FP64;
+        const std::vector<int> one{inst};
+        const std::vector<CkChain> ch{CkChain{inst, chain}};
+        const int K = E.ckK;
+        std::vector<float> hf;
+        auto seg_out = [&](const void *seg, int s0, int cnt, double *dst) {
+            if (!dst || cnt <= 0) return;
+            if (!f32) {
+                CK(cudaMemcpyAsync(dst + (long)s0 * E.nr, seg, sizeof(double) * E.nr * cnt, cudaMemcpyDeviceToHost, E.st));
+                CK(cudaStreamSynchronize(E.st));
+            } else {
+                hf.resize((size_t)E.nr * cnt);
+                CK(cudaMemcpyAsync(hf.data(), seg, sizeof(float) * E.nr * cnt, cudaMemcpyDeviceToHost, E.st));
+                CK(cudaStreamSynchronize(E.st));
+                for (long k = 0; k < E.nr * cnt; k++) dst[(long)s0 * E.nr + k] = hf[k];
+            }
+        };
+        for (int j = 0; j < I.nseg[chain]; j++) {
+            const int s0 = j * K, cnt = (j == I.nseg[chain] - 1) ? I.ns[chain] + 1 - s0 : K;
+            if (f32) {
+                std::vector<const float *> ekf;
+                ckpt_tables<float>(E, one, ekf);
+                ckpt_segment<float>(E, ch, ekf, j, +1, false);
+                ckpt_segment<float>(E, ch, ekf, j, -1, false);
+            } else {
+                std::vector<const double *> ekf;
+                ckpt_tables<double>(E, one, ekf);
+                ckpt_segment<double>(E, ch, ekf, j, +1, false);
+                ckpt_segment<double>(E, ch, ekf, j, -1, false);
+            }
+            seg_out(I.segA[chain], s0, cnt, qf);
+            seg_out(I.segB[chain], s0, cnt, qr);
+        }
+        return PSCFG_OK;
+    }
     for (int d = 0; d < 2; d++) {
         double *dst = d == 0 ? qf : qr;
         if (!dst) continue;

@@ -390,6 +390,45 @@ struct SimpsonJob {
     int n_monomer;
 };
 
+// Simpson contributions of the slices [s0, s1) of one chain, held in
+// segment buffers (slice s at qf + (s - s0) nr), added to rho:
+// rho_a += scale sum_s w[s][a] qf_s qr_s with w the per-slice Simpson
+// weights (ds/3 x 1, 4, 2 of each block containing the slice) and
+// scale = phi / (L Q).  Jobs grouped per instance (grid.y), as k_simpson.
+struct SimpsonSegJob {
+    const void *qf, *qr;
+    const double *w;        // [ns + 1][PSCFG_MAXM]
+    const double *Q;
+    double phi_over_L;
+    int s0, s1;
+    int n_monomer;
+    double *rho;
+};
+
+template <typename T>
+__global__ void k_simpson_seg(const SimpsonSegJob *jobs, const int *job_start, long nr)
+{
+    const int inst = blockIdx.y;
+    const int j0 = job_start[inst], j1 = job_start[inst + 1];
+    if (j1 <= j0) return;
+    const int M = jobs[j0].n_monomer;
+    double *rho = jobs[j0].rho;
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += (long)gridDim.x * blockDim.x) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int a = 0; a < M; a++) acc[a] = rho[(long)a * nr + r];
+        for (int jb = j0; jb < j1; jb++) {
+            const SimpsonSegJob &J = jobs[jb];
+            const T *qf = (const T *)J.qf, *qr = (const T *)J.qr;
+            const double scale = J.phi_over_L / *J.Q;
+            for (int s = J.s0; s < J.s1; s++) {
+                const double p = (double)qf[(long)(s - J.s0) * nr + r] * (double)qr[(long)(s - J.s0) * nr + r] * scale;
+                for (int a = 0; a < M; a++) acc[a] += J.w[s * PSCFG_MAXM + a] * p;
+            }
+        }
+        for (int a = 0; a < M; a++) rho[(long)a * nr + r] = acc[a];
+    }
+}
+
 // Jobs of one instance must run in order (they accumulate into one rho);
 // jobs are grouped per instance in grid.y = instance, looping over its chains.
 template <typename T>

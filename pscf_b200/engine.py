@@ -28,6 +28,7 @@ LIB_PATH = os.environ.get("PSCFG_LIB") or os.path.join(_HERE, "_lib", "libpscfgp
 FP64 = 0
 FP32 = 1
 MIXED = 2
+CHECKPOINT = 0x100   # OR into the precision: sqrt(Ns) propagator checkpoints (PSCFG_CHECKPOINT)
 
 OK, EINVAL, ECUDA, ENOMEM, ESTATE, ENOTCONV = 0, 1, 2, 3, 4, 5
 
