@@ -65,9 +65,12 @@ def test_checkpointed_triblock_uneven_chains_and_fp32():
         c.close()
 
 
-@pytest.mark.parametrize("dim,ngrid,crystal,cell", [(1, [24], "lamellar", [1.6]), (3, [16, 16, 16], "cubic", [2.0])])
-def test_checkpointed_adjoint_matches_stored(dim, ngrid, crystal, cell):
-    s = diblock(dim, ngrid, crystal, cell, fA=0.35, chiN=14.0, ds=0.02)
+@pytest.mark.parametrize("dim,ngrid,crystal,cell,fA,chiN,ds", [(1, [24], "lamellar", [1.6], 0.35, 14.0, 0.02),
+                                                        (3, [16, 16, 16], "cubic", [2.0], 0.35, 14.0, 0.02),
+                                                        (3, [64, 64, 64], "cubic", [3.7], 0.40, 16.0, 0.005)])
+def test_checkpointed_adjoint_matches_stored(dim, ngrid, crystal, cell, fA, chiN, ds):
+    """The last case is the gyroid workload's grid and contour (Ns = 200)."""
+    s = diblock(dim, ngrid, crystal, cell, fA=fA, chiN=chiN, ds=ds)
     rng = np.random.default_rng(5)
     w = omega_guess(s, 3, 2.0)[None]
     G = rng.normal(size=(1, 2, s.nr))
