@@ -54,8 +54,9 @@ extern "C" {
  * chain keeps every K-th slice of qf and qr (K = ceil(sqrt(Ns)) of the
  * batch's longest chain) and two K + 1 slice working segments instead of
  * all Ns + 1 slices; density, stress and the adjoint recompute each segment
- * from its checkpoint with the same step kernels (about 1.5x the sweep
- * work of a density, 2x for the stress and the adjoint).  The reference
+ * from its checkpoint with the same step kernels: a density takes 3 Ns
+ * steps per chain instead of 2 Ns; the stress and the adjoint recompute
+ * both propagators, 2 Ns steps more each.  The reference
  * stores every slice (chain_grid_type%qf/qr, src/chain_mod.f90:159-165);
  * results agree with the stored-slice engine to roundoff.  Not available
  * with pscfg_response. */
