@@ -118,6 +118,15 @@ typedef struct pscfg_am_param {
     double mix_max;          /* cap on lambda (0: 1) */
     double restart;          /* restart the history and the lambda ramp when the error exceeds
                                 restart x its best value since the last restart (0: never) */
+    /* 0: the host drives each iteration (one synchronisation per iteration,
+     * the coefficient solve on the host).  n > 0: every iteration -- density,
+     * stress, free energy, Anderson sums, coefficient solve, mixing,
+     * projection, cell update -- replays from one captured CUDA graph with
+     * its control on the device, and the host reads the instances' status
+     * words every n iterations (the graph is rebuilt without the finished
+     * instances once a quarter of them have finished).  FP64 engines without
+     * PSCFG_CHECKPOINT. */
+    int graph_check;
 } pscfg_am_param;
 
 /* Per-instance exit status of an Anderson run (pscfg_am_result.status).

@@ -36,6 +36,7 @@
 #include "kernels3l.cuh"
 #include "kernels3p.cuh"
 #include "basis.cuh"
+#include "am_graph.cuh"
 
 namespace pscfg {
 
@@ -197,8 +198,24 @@ struct Engine {
     double *stress_part = nullptr;
     size_t stress_part_len = 0;
 
+    // Graph-driven Anderson iterations: amg selects the device-side forms
+    // of the iteration's host steps (no host copies or waits, table k-space
+    // factors); while capturing, descriptors go to an arena that lives as
+    // long as the captured graph (amg_exec), copied on st_up outside the
+    // capture.
+    bool amg = false;
+    bool capturing = false;
+    cudaStream_t st_up = nullptr;
+    std::vector<void *> cap_blocks;
+    char *cap_cur = nullptr;
+    size_t cap_left = 0;
+    cudaGraphExec_t amg_exec = nullptr;
+
     ~Engine()
     {
+        if (amg_exec) cudaGraphExecDestroy(amg_exec);
+        for (void *p : cap_blocks) cudaFree(p);
+        if (st_up) cudaStreamDestroy(st_up);
         for (void *p : allocs) cudaFree(p);
         if (d_desc) cudaFree(d_desc);
         for (void *p : desc_retired) cudaFree(p);
@@ -251,10 +268,48 @@ struct Engine {
         return d_desc;
     }
     std::vector<void *> desc_retired;
+    void *cap_alloc(size_t bytes)
+    {
+        bytes = (bytes + 255) / 256 * 256;
+        if (bytes > cap_left) {
+            const size_t nb = std::max(bytes, (size_t)4 << 20);
+            void *p = nullptr;
+            CK(cudaMalloc(&p, nb));
+            cap_blocks.push_back(p);
+            cap_cur = (char *)p;
+            cap_left = nb;
+        }
+        void *r = cap_cur;
+        cap_cur += bytes;
+        cap_left -= bytes;
+        return r;
+    }
+    // the arena of a destroyed graph (the stream must be idle)
+    void cap_free()
+    {
+        for (void *p : cap_blocks) cudaFree(p);
+        cap_blocks.clear();
+        cap_cur = nullptr;
+        cap_left = 0;
+    }
+    // a scratch buffer would have to grow inside a capture
+    void no_growth_in_capture() const
+    {
+        if (capturing) throw Err(PSCFG_ECUDA, "scratch buffer growth while capturing an Anderson iteration");
+    }
     // upload host descriptors into a sub-range of the descriptor scratch
+    // (while capturing: into the arena, each upload its own range)
     template <typename D>
     D *upload(const std::vector<D> &v, size_t offset_bytes)
     {
+        if (capturing) {
+            D *p = (D *)cap_alloc(v.size() * sizeof(D) + 16);
+            if (!v.empty()) {
+                CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(D), cudaMemcpyHostToDevice, st_up));
+                CK(cudaStreamSynchronize(st_up));
+            }
+            return p;
+        }
         char *base = (char *)desc(offset_bytes + v.size() * sizeof(D) + 256);
         D *p = (D *)(base + offset_bytes);
         if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(D), cudaMemcpyHostToDevice, st));
@@ -263,6 +318,7 @@ struct Engine {
     double *part(size_t len)
     {
         if (len > d_part_len) {
+            no_growth_in_capture();
             if (d_part) cudaFree(d_part);
             d_part = nullptr;
             CK(cudaMalloc(&d_part, len * sizeof(double)));
@@ -494,6 +550,7 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
     }
     CK(cudaStreamCreateWithFlags(&E.st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&E.st2, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&E.st_up, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
     upload_dft_constants();
@@ -676,7 +733,7 @@ static int sweep_planes(const Engine &E, int nf, int n3, int pmax)
 template <typename Emit>
 static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsize, int t0, Emit emit)
 {
-    if (E.no_graphs) {
+    if (E.no_graphs || E.capturing) {   // inside a captured Anderson iteration: its own nodes
         emit();
         return;
     }
@@ -1023,7 +1080,7 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
     // the launch is orthogonal (written after the descriptors)
     std::vector<T> ekf;
     const int L3 = (int)(E.n[0] / 2 + 1) + E.n[1] + E.n[2];
-    if (plane_kernels_apply(E)) {
+    if (plane_kernels_apply(E) && !E.amg) {   // graph-driven iterations: the cell lives on the device
         bool ortho = true;
         for (int i : act)
             for (int a = 0; a < 3; a++)
@@ -1183,7 +1240,8 @@ static void run_contour(Engine &E, const std::vector<int> &act)
     }
     // grand ensemble: phi = Q exp(mu) (mu_phi_chain/mu_phi_solvent,
     // src/scf_mod.fp.f90:202-209) is needed by the chain weights below
-    if (any_grand) {
+    // (graph-driven iterations: formed from the device Q by k_simpson)
+    if (any_grand && !E.amg) {
         for (int i : act) {
             Inst &I = E.inst[i];
             if (I.sys.ensemble != 1) continue;
@@ -1233,6 +1291,8 @@ static void run_contour(Engine &E, const std::vector<int> &act)
             }
             j.n_monomer = I.sys.n_monomer;
             j.accumulate = I.sys.n_solvent > 0 ? 1 : 0;
+            j.grand = (E.amg && I.sys.ensemble == 1) ? 1 : 0;
+            j.mu = I.sys.mu_chain[c];
             simp.push_back(j);
         }
         if (I.sys.n_chain == 0 && I.sys.n_solvent == 0)
@@ -1585,6 +1645,13 @@ static void density_all(Engine &E, const std::vector<int> &act, bool finish = tr
     // pull Q to the host (needed for mu and for the caller): gathered on the
     // device, one copy into the pinned staging buffer; finish = false leaves
     // the synchronisation and density_finish to the caller
+    if (E.amg) {   // graph-driven iterations: Q stays on the device (k_amg_finish)
+        for (int i : act) {
+            E.inst[i].have_density = true;
+            E.inst[i].dens_prec = E.inst[i].prec_now;
+        }
+        return;
+    }
     std::vector<CopyJob> cj;
     for (int i : act) {
         Inst &I = E.inst[i];
@@ -1711,6 +1778,7 @@ static bool slice_dots_r(Engine &E, const StressJob<T> *dj, int njobs, int maxs)
         const size_t per_slice = 2 * (size_t)E.nk * sizeof(cx<T>);
         const int cs = (int)std::max<size_t>(1, std::min<size_t>((size_t)maxs, ((size_t)1 << 30) / (per_slice * njobs)));
         if (E.spec_bytes < per_slice * cs * njobs) {
+            E.no_growth_in_capture();
             if (E.spec) cudaFree(E.spec);
             E.spec = nullptr;
             CK(cudaMalloc(&E.spec, per_slice * cs * njobs));
@@ -1718,6 +1786,7 @@ static bool slice_dots_r(Engine &E, const StressJob<T> *dj, int njobs, int maxs)
         }
         const size_t plen = (size_t)cs * njobs * ntile * PSCFG_MAXCP;
         if (E.stress_part_len < plen) {
+            E.no_growth_in_capture();
             if (E.stress_part) cudaFree(E.stress_part);
             E.stress_part = nullptr;
             CK(cudaMalloc(&E.stress_part, plen * sizeof(double)));
@@ -1781,6 +1850,7 @@ static void slice_dots(Engine &E, const std::vector<StressJob<T>> &jobs)
         const size_t per_slice = 2 * (size_t)E.nk * sizeof(cx<T>);
         int cs = (int)std::max<size_t>(1, std::min<size_t>(256, ((size_t)1 << 30) / per_slice));
         if (E.spec_bytes < per_slice * cs) {
+            E.no_growth_in_capture();
             if (E.spec) cudaFree(E.spec);
             E.spec = nullptr;
             CK(cudaMalloc(&E.spec, per_slice * cs));
@@ -1791,6 +1861,7 @@ static void slice_dots(Engine &E, const std::vector<StressJob<T>> &jobs)
         const long ntile_max = std::max<long>(ntile, (P + 7) / 8);
         size_t plen = (size_t)cs * ntile_max * PSCFG_MAXCP;
         if (E.stress_part_len < plen) {
+            E.no_growth_in_capture();
             if (E.stress_part) cudaFree(E.stress_part);
             E.stress_part = nullptr;
             CK(cudaMalloc(&E.stress_part, plen * sizeof(double)));
@@ -1885,13 +1956,14 @@ static void stress_all(Engine &E, const std::vector<int> &act)
 // ---------------------------------------------------------------------
 // Field term sum_k w r [..] / nr^2 for instances with star weights, from
 // the spectra of rho and omega (FP64 forward FFTs).
-static void fe_spectral(Engine &E, const std::vector<int> &which, double *hout)
+static void fe_spectral(Engine &E, const std::vector<int> &which, double *hout, bool dev_out = false)
 {
     const PlaneGeom &g = E.g64;
     const int M = E.M;
     const size_t per = (size_t)2 * M * E.nk * sizeof(cx<double>);
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>(which.size(), ((size_t)512 << 20) / per));
     if (E.fe_spec_bytes < per * chunk) {
+        E.no_growth_in_capture();
         if (E.fe_spec) cudaFree(E.fe_spec);
         E.fe_spec = nullptr;
         CK(cudaMalloc(&E.fe_spec, per * chunk));
@@ -1953,7 +2025,8 @@ static void fe_spectral(Engine &E, const std::vector<int> &which, double *hout)
         const double rn2 = (double)E.nr * (double)E.nr;
         k_final_sum<<<(unsigned)((cn + 127) / 128), 128, 0, E.st>>>(part, nct, rn2, E.d_small, cn);
         E.launched();
-        CK(cudaMemcpyAsync(hout + c0, E.d_small, sizeof(double) * cn, cudaMemcpyDeviceToHost, E.st));
+        CK(cudaMemcpyAsync(hout + c0, E.d_small, sizeof(double) * cn,
+                           dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, E.st));
     }
 }
 
@@ -1968,13 +2041,16 @@ static void fe_partition(Engine &E, const std::vector<int> &act, std::vector<siz
 static void fe_finish(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p);
 
 // Field terms of the free energy into the staging buffer; with finish, the
-// synchronisation and the assembly (fe_finish) follow.
+// synchronisation and the assembly (fe_finish) follow.  dterms (device):
+// the terms go there instead, plain instances first, in act order, then
+// the star-weighted ones (graph-driven iterations).
 static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<double> &f, std::vector<double> &p,
-                            bool finish = true)
+                            bool finish = true, double *dterms = nullptr)
 {
     std::vector<size_t> pos_plain, pos_w;
     fe_partition(E, act, pos_plain, pos_w);
-    double *hfe = E.hfe();
+    double *hfe = dterms ? dterms : E.hfe();
+    const cudaMemcpyKind kind = dterms ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     if (!pos_plain.empty()) {
         std::vector<FieldJob> fj;
         for (size_t k : pos_plain) {
@@ -1995,14 +2071,14 @@ static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<
         E.launched();
         k_final_sum<<<(unsigned)((fj.size() + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small, (int)fj.size());
         E.launched();
-        CK(cudaMemcpyAsync(hfe, E.d_small, sizeof(double) * fj.size(), cudaMemcpyDeviceToHost, E.st));
+        CK(cudaMemcpyAsync(hfe, E.d_small, sizeof(double) * fj.size(), kind, E.st));
     }
     if (!pos_w.empty()) {
         std::vector<int> weighted;
         for (size_t k : pos_w) weighted.push_back(act[k]);
-        fe_spectral(E, weighted, hfe + pos_plain.size());
+        fe_spectral(E, weighted, hfe + pos_plain.size(), dterms != nullptr);
     }
-    if (finish) {
+    if (finish && !dterms) {
         CK(cudaStreamSynchronize(E.st));
         fe_finish(E, act, f, p);
     }
@@ -2090,7 +2166,30 @@ struct AmRun {
     bool active = false;
     pscfg_am_param prm;
     std::vector<AmState> st;
+    // graph-driven iterations (prm.graph_check > 0): device state and the
+    // per-act-position job arrays the device control kernels write
+    bool graph = false;
+    int g_ninst = 0;
+    AmgInst *g_st = nullptr;
+    int *g_act = nullptr, *g_tidx = nullptr;
+    double *g_terms = nullptr;
+    AmJob *g_aj = nullptr;
+    AmFix *g_fx = nullptr;
+    AmDot *g_dots = nullptr;
+    AmMix *g_mix = nullptr;
+    CopyJob *g_hc = nullptr;
+    GeomJob *g_geo = nullptr;
+    SymJob *g_sym = nullptr;
+    int g_maxorb = 0;
+    std::vector<int> g_cap;         // instances of the captured iteration
+    long g_launches = 0;            // kernel launches per replay
+    std::vector<AmgInst> g_host;    // read-back mirror
 };
+
+static int am_iterate_graph(Engine &E, AmRun &R, int iters);
+static void amg_alloc(Engine &E, AmRun &R);
+static void amg_init(Engine &E, AmRun &R);
+static void amg_drop_graph(Engine &E);
 
 // Space-group projection of omega for the given instances, in place.
 static void symmetrize_omega(Engine &E, const std::vector<int> &which)
@@ -2101,6 +2200,7 @@ static void symmetrize_omega(Engine &E, const std::vector<int> &which)
         Inst &I = E.inst[i];
         if (I.nops <= 0) continue;
         SymJob j;
+        std::memset(&j, 0, sizeof(j));
         j.f = I.omega;
         j.perm = I.d_orb_perm;
         j.start = I.d_orb_start;
@@ -2121,6 +2221,10 @@ static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
     const int H = prm.n_hist;
     if (H < 1 || H > PSCFG_MAXH - 1) throw Err(PSCFG_EINVAL, "n_hist out of range");
     if (prm.max_itr < 0) throw Err(PSCFG_EINVAL, "max_itr must be >= 0");
+    if (prm.graph_check < 0) throw Err(PSCFG_EINVAL, "graph_check must be >= 0");
+    if (prm.graph_check > 0 && (E.prec != PSCFG_FP64 || E.ckpt))
+        throw Err(PSCFG_EINVAL, "graph_check needs an FP64 engine without PSCFG_CHECKPOINT");
+    amg_drop_graph(E);
     const int S = H + 1;
     const long fl = (long)E.M * E.nr;
     const int ninst = (int)E.inst.size();
@@ -2169,6 +2273,12 @@ static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
         st.nstore = 0;
     }
     CK(cudaStreamSynchronize(E.st));
+    R.graph = prm.graph_check > 0;
+    R.g_cap.clear();
+    if (R.graph) {
+        amg_alloc(E, R);
+        amg_init(E, R);
+    }
     R.active = true;
 }
 
@@ -2177,6 +2287,7 @@ static void am_begin(Engine &E, AmRun &R, const pscfg_am_param &prm)
 static int am_iterate(Engine &E, AmRun &R, int iters)
 {
     if (!R.active) throw Err(PSCFG_ESTATE, "no Anderson run in progress");
+    if (R.graph) return am_iterate_graph(E, R, iters);
     const pscfg_am_param &prm = R.prm;
     const int H = prm.n_hist, S = H + 1;
     const long fl = (long)E.M * E.nr;
@@ -2358,7 +2469,7 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
             const int kk = s.itr - s.k0;
             int itr_prev;
             double lam;
-            if (kk < H + 1) { itr_prev = kk - 1; lam = 1.0 - std::pow(0.9, kk); }
+            if (kk < H + 1) { itr_prev = kk - 1; lam = am_lambda_ramp(kk); }
             else { itr_prev = H; lam = 1.0; }
             itr_prev = std::min(itr_prev, s.nstore - 1);
             if (prm.mix_max > 0) lam = std::min(lam, prm.mix_max);
@@ -2435,6 +2546,329 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
         for (int i = 0; i < ninst; i++)
             if (!st[i].done) remaining++;
     }
+    return remaining;
+}
+
+// ---------------------------------------------------------------------
+// Graph-driven Anderson iterations (pscfg_am_param.graph_check > 0)
+// ---------------------------------------------------------------------
+// One iteration of the instances `act` is a fixed sequence of launches
+// whose control data live on the device (am_graph.cuh), so it is captured
+// once into a CUDA graph and replayed graph_check times between host
+// checks.  The graph is rebuilt without the finished instances once the
+// running ones are fewer than three quarters of those it holds.
+
+static void amg_alloc(Engine &E, AmRun &R)
+{
+    const int n = (int)E.inst.size();
+    if (R.g_ninst >= n) return;
+    R.g_st = (AmgInst *)E.dalloc(sizeof(AmgInst) * n);
+    R.g_act = (int *)E.dalloc(sizeof(int) * n);
+    R.g_tidx = (int *)E.dalloc(sizeof(int) * n);
+    R.g_terms = (double *)E.dalloc(sizeof(double) * n);
+    R.g_aj = (AmJob *)E.dalloc(sizeof(AmJob) * n);
+    R.g_fx = (AmFix *)E.dalloc(sizeof(AmFix) * n);
+    R.g_dots = (AmDot *)E.dalloc(sizeof(AmDot) * n);
+    R.g_mix = (AmMix *)E.dalloc(sizeof(AmMix) * n);
+    R.g_hc = (CopyJob *)E.dalloc(sizeof(CopyJob) * n);
+    R.g_geo = (GeomJob *)E.dalloc(sizeof(GeomJob) * n);
+    R.g_sym = (SymJob *)E.dalloc(sizeof(SymJob) * n);
+    R.g_ninst = n;
+}
+
+// Initial device state of every instance (after am_begin's first density).
+static void amg_init(Engine &E, AmRun &R)
+{
+    const int n = (int)E.inst.size();
+    const int S = R.prm.n_hist + 1;
+    std::vector<AmgInst> h(n);
+    for (int i = 0; i < n; i++) {
+        Inst &I = E.inst[i];
+        AmgInst &A = h[i];
+        std::memset(&A, 0, sizeof(A));
+        A.n_chain = I.sys.n_chain;
+        A.n_solvent = I.sys.n_solvent;
+        A.ensemble = I.sys.ensemble;
+        A.ncp = I.cell.ncp;
+        A.dim = E.dim;
+        A.crystal = I.sys.crystal_system;
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            A.length[c] = I.length[c];
+            A.phi[c] = I.sys.phi_chain[c];
+            A.mu[c] = I.sys.mu_chain[c];
+            A.Qv[c] = I.Q[c];
+        }
+        for (int v = 0; v < I.sys.n_solvent; v++) {
+            A.solvent_size[v] = I.sys.solvent_size[v];
+            A.phis[v] = I.sys.phi_solvent[v];
+            A.mus[v] = I.sys.mu_solvent[v];
+            A.Qsv[v] = I.Qs[v];
+        }
+        A.omega = I.omega;
+        A.om_hist = I.om_hist;
+        A.dev_hist = I.dev_hist;
+        A.fl = (long)E.M * E.nr;
+        A.Q = I.Qdev;
+        A.Qs = I.Qsolv;
+        A.stress_dev = I.stress_dev;
+        A.status = PSCFG_AM_RUNNING;
+        A.best_run = INFINITY;
+        for (int b = 0; b < I.cell.ncp; b++) {
+            A.cell[b] = I.sys.cell_param[b];
+            A.cph[0][b] = I.sys.cell_param[b];
+        }
+        (void)S;
+        if (I.kweight && !I.wdg0) I.wdg0 = (double *)E.dalloc(sizeof(double) * PSCFG_MAXCP * E.nk);
+    }
+    CK(cudaMemcpyAsync(R.g_st, h.data(), sizeof(AmgInst) * n, cudaMemcpyHostToDevice, E.st));
+    CK(cudaStreamSynchronize(E.st));
+    R.g_host.assign(n, AmgInst());
+}
+
+// The job fields the device does not write, for the act positions.
+static void amg_setup(Engine &E, AmRun &R, const std::vector<int> &act)
+{
+    const int na = (int)act.size();
+    std::vector<AmJob> aj(na);
+    std::vector<AmFix> fx(na);
+    std::vector<GeomJob> geo(na);
+    std::vector<SymJob> sym(na);
+    std::vector<int> tidx(na);
+    std::vector<size_t> pos_plain, pos_w;
+    fe_partition(E, act, pos_plain, pos_w);
+    for (size_t k = 0; k < pos_plain.size(); k++) tidx[pos_plain[k]] = (int)k;
+    for (size_t k = 0; k < pos_w.size(); k++) tidx[pos_w[k]] = (int)(pos_plain.size() + k);
+    R.g_maxorb = 0;
+    for (int k = 0; k < na; k++) {
+        Inst &I = E.inst[act[k]];
+        std::memset(&aj[k], 0, sizeof(AmJob));
+        aj[k].omega = I.omega;
+        aj[k].rho = I.rho;
+        aj[k].M = E.M;
+        for (int a = 0; a < E.M; a++)
+            for (int b = 0; b < E.M; b++) aj[k].chi[a][b] = I.sys.chi[a][b];
+        std::memset(&fx[k], 0, sizeof(AmFix));
+        fx[k].mean = E.d_small + (size_t)k * PSCFG_MAXM;
+        fx[k].M = E.M;
+        GeomJob &g = geo[k];
+        std::memset(&g, 0, sizeof(g));
+        std::memcpy(g.G, I.cell.G, sizeof(g.G));
+        std::memcpy(g.dGG, I.cell.dGG, sizeof(g.dGG));
+        g.ncp = I.cell.ncp;
+        g.ksq = I.ksq;
+        g.wdgsq = I.wdgsq;
+        g.kweight = I.kweight;
+        g.wdg0 = I.kweight ? I.wdg0 : nullptr;
+        g.gate = &R.g_st[act[k]].mixed;
+        SymJob &y = sym[k];
+        std::memset(&y, 0, sizeof(y));
+        y.f = I.omega;
+        y.perm = I.d_orb_perm;
+        y.start = I.d_orb_start;
+        y.norb = I.nops > 0 ? I.norb : 0;
+        y.M = E.M;
+        y.gate = &R.g_st[act[k]].mixed;
+        R.g_maxorb = std::max(R.g_maxorb, y.norb);
+    }
+    CK(cudaMemcpyAsync(R.g_act, act.data(), sizeof(int) * na, cudaMemcpyHostToDevice, E.st));
+    CK(cudaMemcpyAsync(R.g_tidx, tidx.data(), sizeof(int) * na, cudaMemcpyHostToDevice, E.st));
+    CK(cudaMemcpyAsync(R.g_aj, aj.data(), sizeof(AmJob) * na, cudaMemcpyHostToDevice, E.st));
+    CK(cudaMemcpyAsync(R.g_fx, fx.data(), sizeof(AmFix) * na, cudaMemcpyHostToDevice, E.st));
+    CK(cudaMemcpyAsync(R.g_geo, geo.data(), sizeof(GeomJob) * na, cudaMemcpyHostToDevice, E.st));
+    CK(cudaMemcpyAsync(R.g_sym, sym.data(), sizeof(SymJob) * na, cudaMemcpyHostToDevice, E.st));
+    CK(cudaStreamSynchronize(E.st));
+}
+
+// Enqueue one iteration of the instances `act` (their jobs set up by
+// amg_setup): the host iteration's launches with the Anderson step,
+// mixing, history and cell update on the device.
+static void amg_iteration(Engine &E, AmRun &R, const std::vector<int> &act)
+{
+    struct Flag {
+        bool &f;
+        explicit Flag(bool &x) : f(x) { f = true; }
+        ~Flag() { f = false; }
+    } on(E.amg);
+    const pscfg_am_param &prm = R.prm;
+    const int na = (int)act.size();
+    const int S = prm.n_hist + 1;
+    const long fl = (long)E.M * E.nr;
+    const int nct = red_ctas(E.nr);
+    const double large = 100.0;
+    const unsigned g1 = (unsigned)((na + 127) / 128);
+    density_all(E, act, false);
+    if (prm.domain) stress_all(E, act);
+    std::vector<double> fe, pe;
+    free_energy_all(E, act, fe, pe, false, R.g_terms);
+    amg_launch_finish(E.st, R.g_st, R.g_act, na, R.g_terms, R.g_tidx);
+    E.launched();
+    amg_launch_prep(E.st, R.g_st, R.g_act, na, S, R.g_aj, R.g_fx, R.g_dots);
+    E.launched();
+    double *part = E.part((size_t)nct * na * (PSCFG_MAXM + 1 + PSCFG_MAXH + 1) + 64);
+    double *mpart = part + (size_t)nct * na * PSCFG_MAXM;
+    double *dpart = mpart + (size_t)nct * na;
+    k_am_dev<<<dim3(nct, na), 256, 0, E.st>>>(R.g_aj, E.nr, part);
+    E.launched();
+    k_final_sum<<<(unsigned)((na * PSCFG_MAXM + 127) / 128), 128, 0, E.st>>>(part, nct, (double)E.nr, E.d_small,
+                                                                              na * PSCFG_MAXM);
+    E.launched();
+    k_am_fix<<<dim3(nct, na), 256, 0, E.st>>>(R.g_fx, E.nr, mpart);
+    E.launched();
+    double *emax = E.d_small + (size_t)na * PSCFG_MAXM;
+    k_final_max<<<g1, 128, 0, E.st>>>(mpart, nct, emax, na);
+    E.launched();
+    k_am_dots<<<dim3(nct, na), 256, 0, E.st>>>(R.g_dots, dpart);
+    E.launched();
+    double *dres = E.d_small + (size_t)na * (PSCFG_MAXM + 1);
+    k_final_sum<<<(unsigned)((na * (PSCFG_MAXH + 1) + 127) / 128), 128, 0, E.st>>>(dpart, nct, 1.0, dres,
+                                                                                   na * (PSCFG_MAXH + 1));
+    E.launched();
+    double *dstat = dres + (size_t)na * (PSCFG_MAXH + 1);
+    k_am_status<<<g1, 128, 0, E.st>>>(emax, dres, PSCFG_MAXH + 1, 100.0 * large, dstat, na);
+    E.launched();
+    AmgParam P;
+    P.H = prm.n_hist;
+    P.max_itr = prm.max_itr;
+    P.domain = prm.domain;
+    P.error_max = prm.error_max;
+    P.mix_max = prm.mix_max;
+    P.restart = prm.restart;
+    P.large = large;
+    P.nr = (double)E.nr;
+    amg_launch_update(E.st, P, R.g_st, R.g_act, na, emax, dres, dstat, R.g_mix, R.g_hc, R.g_geo);
+    E.launched();
+    k_am_mix<<<dim3(nct, na), 256, 0, E.st>>>(R.g_mix);
+    E.launched();
+    if (R.g_maxorb > 0) {
+        dim3 grid((unsigned)std::max(1, std::min((R.g_maxorb + 127) / 128, 256)), (unsigned)na);
+        k_symmetrize<<<grid, 128, 0, E.st>>>(R.g_sym, E.nr);
+        E.launched();
+    }
+    const unsigned gx = (unsigned)std::max<long>(1, std::min<long>((fl + 255) / 256, 64));
+    k_copy_list<<<dim3(gx, na), 256, 0, E.st>>>(R.g_hc);
+    E.launched();
+    if (prm.domain) {
+        dim3 grid((unsigned)std::min<long>((E.nk + 255) / 256, 512), (unsigned)na);
+        k_make_geom<<<grid, 256, 0, E.st>>>(R.g_geo, E.dim, E.n[0], E.n[1], E.n[2]);
+        E.launched();
+    }
+}
+
+// Capture one iteration of `act` into E.amg_exec (the stream is idle).
+static void amg_capture(Engine &E, AmRun &R, const std::vector<int> &act)
+{
+    const bool prof = E.profiling;
+    E.profiling = false;
+    E.capturing = true;
+    const long l0 = E.launches;
+    cudaGraph_t graph = nullptr;
+    cudaError_t be = cudaStreamBeginCapture(E.st, cudaStreamCaptureModeRelaxed);
+    if (be != cudaSuccess) {
+        E.capturing = false;
+        E.profiling = prof;
+        CK(be);
+    }
+    try {
+        amg_iteration(E, R, act);
+    } catch (...) {
+        cudaStreamEndCapture(E.st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        E.capturing = false;
+        E.profiling = prof;
+        E.launches = l0;
+        throw;
+    }
+    E.capturing = false;
+    E.profiling = prof;
+    CK(cudaStreamEndCapture(E.st, &graph));
+    cudaError_t ie = cudaGraphInstantiate(&E.amg_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(ie);
+    R.g_launches = E.launches - l0;
+    E.launches = l0;
+    R.g_cap = act;
+}
+
+// Host view of the device state: AmState, the chemistry, Q and the cell.
+static void amg_readback(Engine &E, AmRun &R)
+{
+    const int n = (int)E.inst.size();
+    const size_t head = offsetof(AmgInst, devcp);
+    CK(cudaMemcpy2DAsync(R.g_host.data(), sizeof(AmgInst), R.g_st, sizeof(AmgInst), head, n, cudaMemcpyDeviceToHost,
+                         E.st));
+    CK(cudaStreamSynchronize(E.st));
+    for (int i = 0; i < n; i++) {
+        const AmgInst &A = R.g_host[i];
+        AmState &s = R.st[i];
+        Inst &I = E.inst[i];
+        s.itr = A.itr;
+        s.status = A.status;
+        s.done = A.done != 0;
+        s.converged = A.status == PSCFG_AM_CONVERGED;
+        s.error = A.error;
+        s.f = A.f;
+        s.p = A.p;
+        for (int b = 0; b < PSCFG_MAXCP; b++) s.stress[b] = A.stress[b];
+        for (int c = 0; c < I.sys.n_chain; c++) {
+            I.sys.phi_chain[c] = A.phi[c];
+            I.sys.mu_chain[c] = A.mu[c];
+            I.Q[c] = A.Qv[c];
+        }
+        for (int v = 0; v < I.sys.n_solvent; v++) {
+            I.sys.phi_solvent[v] = A.phis[v];
+            I.sys.mu_solvent[v] = A.mus[v];
+            I.Qs[v] = A.Qsv[v];
+        }
+        if (R.prm.domain) {
+            for (int b = 0; b < I.cell.ncp; b++) I.sys.cell_param[b] = A.cell[b];
+            Cell c;
+            if (make_unit_cell(E.dim, I.sys.crystal_system, I.sys.cell_param, c)) I.cell = c;
+        }
+    }
+}
+
+static void amg_drop_graph(Engine &E)
+{
+    CK(cudaStreamSynchronize(E.st));
+    if (E.amg_exec) {
+        CK(cudaGraphExecDestroy(E.amg_exec));
+        E.amg_exec = nullptr;
+    }
+    E.cap_free();
+}
+
+static int am_iterate_graph(Engine &E, AmRun &R, int iters)
+{
+    const int ninst = (int)E.inst.size();
+    int it = 0;
+    while (it < iters) {
+        std::vector<int> act;
+        for (int i = 0; i < ninst; i++)
+            if (!R.st[i].done) act.push_back(i);
+        if (act.empty()) break;
+        if (!E.amg_exec || act.size() * 4 < R.g_cap.size() * 3) {
+            // (re)build: one iteration of the new set launched directly
+            // sizes the scratch buffers (their sizes depend on the set), then
+            // the same sequence is captured
+            amg_drop_graph(E);
+            amg_setup(E, R, act);
+            amg_iteration(E, R, act);
+            it++;
+            amg_capture(E, R, act);
+            if (it >= iters) {
+                amg_readback(E, R);
+                break;
+            }
+        }
+        const int n = std::min(R.prm.graph_check, iters - it);
+        for (int r = 0; r < n; r++) CK(cudaGraphLaunch(E.amg_exec, E.st));
+        E.launches += (long)n * R.g_launches;
+        it += n;
+        amg_readback(E, R);
+    }
+    int remaining = 0;
+    for (int i = 0; i < ninst; i++)
+        if (!R.st[i].done) remaining++;
     return remaining;
 }
 

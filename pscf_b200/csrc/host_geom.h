@@ -1,12 +1,20 @@
 // host_geom.h -- host-side geometry for the engine: unit cell, k^2 table,
 // stress weights, contour discretisation, FFT plans.  Plain C++ (runs on
-// the CPU at setup and after each cell update).
+// the CPU at setup and after each cell update); make_unit_cell is also
+// compiled for the device, where the graph-driven Anderson iteration
+// updates the cell.
 #pragma once
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "../../include/pscf_gpu.h"
+
+#ifdef __CUDACC__
+#define PSCFG_HD __host__ __device__
+#else
+#define PSCFG_HD
+#endif
 
 namespace pscfg {
 
@@ -30,6 +38,16 @@ inline int chain_grid(int nblk, const double *blen, double ds, int *bgn, double 
     return s;
 }
 
+// Anderson mixing parameter lambda = 1 - 0.9^k of iteration k of the ramp
+// (src/iterate_mod.fp.f90:1147-1153), the power by repeated multiplication
+// so that host and device agree to the bit.
+PSCFG_HD inline double am_lambda_ramp(int k)
+{
+    double p = 1.0;
+    for (int j = 0; j < k; j++) p *= 0.9;
+    return 1.0 - p;
+}
+
 struct Cell {
     int dim = 1;
     int ncp = 0;
@@ -39,12 +57,14 @@ struct Cell {
 
 // make_unit_cell + make_G_basis (src/unit_cell_mod.f90:309-664, 723-757).
 // Returns false for an unknown crystal system.
-inline bool make_unit_cell(int dim, int sys, const double *cp, Cell &c)
+PSCFG_HD inline bool make_unit_cell(int dim, int sys, const double *cp, Cell &c)
 {
     double R[3][3] = {{0}}, dR[3][3][PSCFG_MAXCP];
-    std::memset(dR, 0, sizeof(dR));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < PSCFG_MAXCP; k++) dR[i][j][k] = 0.0;
     int ncp = 0;
-    const double s75 = std::sqrt(0.75);
+    const double s75 = sqrt(0.75);
     switch (sys) {
     case PSCFG_LAMELLAR: ncp = 1; R[0][0] = cp[0]; dR[0][0][0] = 1; break;
     case PSCFG_SQUARE: ncp = 1; R[0][0] = R[1][1] = cp[0]; dR[0][0][0] = dR[1][1][0] = 1; break;
@@ -54,9 +74,9 @@ inline bool make_unit_cell(int dim, int sys, const double *cp, Cell &c)
         dR[0][0][0] = 1; dR[1][0][0] = -0.5; dR[1][1][0] = s75; break;
     case PSCFG_OBLIQUE:
         // dR(1,1,1) = a as written in src/unit_cell_mod.f90:630
-        ncp = 3; R[0][0] = cp[0]; R[1][0] = cp[1] * std::cos(cp[2]); R[1][1] = cp[1] * std::sin(cp[2]);
-        dR[0][0][0] = cp[0]; dR[1][0][1] = std::cos(cp[2]); dR[1][1][1] = std::sin(cp[2]);
-        dR[1][0][2] = -cp[1] * std::sin(cp[2]); dR[1][1][2] = cp[1] * std::cos(cp[2]); break;
+        ncp = 3; R[0][0] = cp[0]; R[1][0] = cp[1] * cos(cp[2]); R[1][1] = cp[1] * sin(cp[2]);
+        dR[0][0][0] = cp[0]; dR[1][0][1] = cos(cp[2]); dR[1][1][1] = sin(cp[2]);
+        dR[1][0][2] = -cp[1] * sin(cp[2]); dR[1][1][2] = cp[1] * cos(cp[2]); break;
     case PSCFG_CUBIC: ncp = 1; R[0][0] = R[1][1] = R[2][2] = cp[0]; dR[0][0][0] = dR[1][1][0] = dR[2][2][0] = 1; break;
     case PSCFG_TETRAGONAL:
         ncp = 2; R[0][0] = R[1][1] = cp[0]; R[2][2] = cp[1]; dR[0][0][0] = dR[1][1][0] = 1; dR[2][2][1] = 1; break;
@@ -66,12 +86,12 @@ inline bool make_unit_cell(int dim, int sys, const double *cp, Cell &c)
         ncp = 2; R[0][0] = cp[0]; R[1][0] = -0.5 * cp[0]; R[1][1] = cp[0] * s75; R[2][2] = cp[1];
         dR[0][0][0] = 1; dR[1][0][0] = -0.5; dR[1][1][0] = s75; dR[2][2][1] = 1; break;
     case PSCFG_MONOCLINIC:
-        ncp = 4; R[0][0] = cp[0]; R[1][1] = cp[1]; R[2][0] = cp[2] * std::cos(cp[3]); R[2][2] = cp[2] * std::sin(cp[3]);
-        dR[0][0][0] = 1; dR[1][1][1] = 1; dR[2][0][2] = std::cos(cp[3]); dR[2][2][2] = std::sin(cp[3]);
-        dR[2][0][3] = -cp[2] * std::sin(cp[3]); dR[2][2][3] = cp[2] * std::cos(cp[3]); break;
+        ncp = 4; R[0][0] = cp[0]; R[1][1] = cp[1]; R[2][0] = cp[2] * cos(cp[3]); R[2][2] = cp[2] * sin(cp[3]);
+        dR[0][0][0] = 1; dR[1][1][1] = 1; dR[2][0][2] = cos(cp[3]); dR[2][2][2] = sin(cp[3]);
+        dR[2][0][3] = -cp[2] * sin(cp[3]); dR[2][2][3] = cp[2] * cos(cp[3]); break;
     default: return false;
     }
-    const double twopi = 4.0 * std::acos(0.0);
+    const double twopi = 2.0 * 3.141592653589793;
     double a[3][3];
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) a[i][j] = (i < dim && j < dim) ? R[i][j] : (i == j ? 1.0 : 0.0);
@@ -93,7 +113,9 @@ inline bool make_unit_cell(int dim, int sys, const double *cp, Cell &c)
     for (int i = 0; i < dim; i++)
         for (int j = 0; j < dim; j++) c.G[i][j] = twopi * inv[j][i];
     double dG[3][3][PSCFG_MAXCP];
-    std::memset(dG, 0, sizeof(dG));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            for (int k = 0; k < PSCFG_MAXCP; k++) dG[i][j][k] = 0.0;
     for (int k = 0; k < ncp; k++)
         for (int i = 0; i < dim; i++)
             for (int j = 0; j < dim; j++) {

@@ -388,6 +388,8 @@ struct SimpsonJob {
     double bds[PSCFG_MAXB];
     int accumulate;             // 1: add to the existing rho (solvent terms already there)
     int n_monomer;
+    int grand;                  // 1: phi = Q exp(mu) from the device Q (grand ensemble)
+    double mu;
 };
 
 // Simpson contributions of the slices [s0, s1) of one chain, held in
@@ -444,6 +446,7 @@ __global__ void k_simpson(const SimpsonJob *jobs, const int *job_start, long nr)
             const SimpsonJob &J = jobs[jb];
             const T *qf = (const T *)J.qf, *qr = (const T *)J.qr;
             const double Q = *J.Q;
+            const double phi = J.grand ? Q * exp(J.mu) : J.phi;
             for (int b = 0; b < J.nblk; b++) {
                 const int ib = J.bgn[b], ie = J.bgn[b + 1];
                 double s = (double)qf[(long)ib * nr + r] * (double)qr[(long)ib * nr + r];
@@ -454,7 +457,7 @@ __global__ void k_simpson(const SimpsonJob *jobs, const int *job_start, long nr)
                     s = s + (double)qf[(long)j * nr + r] * (double)qr[(long)j * nr + r] * 2.0;
                 s = s * J.bds[b] / 3.0;
                 s = s / J.length / Q;
-                acc[J.mon[b]] = acc[J.mon[b]] + J.phi * s;
+                acc[J.mon[b]] = acc[J.mon[b]] + phi * s;
             }
         }
         if (j1 > j0) {

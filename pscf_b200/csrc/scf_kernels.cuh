@@ -434,6 +434,7 @@ struct GeomJob {
     double *wdgsq;   // [PSCFG_MAXCP][nk]
     const double *kweight;   // [nk] star weights or nullptr (all 1)
     double *wdg0;            // [PSCFG_MAXCP][nk] w(kx) G^T dGG_b G without star weights, or nullptr
+    const int *gate;         // nullptr, or a device flag: the job runs only when it is nonzero
 };
 
 __device__ __forceinline__ double gnorm_dev(int dim, const int Gt[3], const double G[3][3])
@@ -453,6 +454,7 @@ __device__ __forceinline__ double gnorm_dev(int dim, const int Gt[3], const doub
 static __global__ void k_make_geom(const GeomJob *jobs, int dim, int n1, int n2, int n3)
 {
     const GeomJob &J = jobs[blockIdx.y];
+    if (J.gate && *J.gate == 0) return;
     const int n1h = n1 / 2 + 1;
     const long nk = (long)n1h * n2 * n3;
     const int n[3] = {n1, n2, n3};
@@ -504,6 +506,7 @@ struct SymJob {
     const int *start;       // orbit o = perm[start[o] .. start[o+1])
     int norb;
     int M;
+    const int *gate;        // nullptr, or a device flag: project only when it is nonzero
 };
 
 // Space-group projection f <- (1/|G|) sum_g f(g r) as the orbit mean: a
@@ -512,6 +515,7 @@ struct SymJob {
 static __global__ void k_symmetrize(const SymJob *jobs, long nr)
 {
     const SymJob &J = jobs[blockIdx.y];
+    if (J.gate && *J.gate == 0) return;
     for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < J.norb; o += gridDim.x * blockDim.x) {
         const int b = J.start[o], e = J.start[o + 1];
         const double inv = 1.0 / (double)(e - b);

@@ -67,6 +67,7 @@ class PscfgAmParam(C.Structure):
         ("switch_error", C.c_double),
         ("mix_max", C.c_double),
         ("restart", C.c_double),
+        ("graph_check", C.c_int),
     ]
 
 
@@ -319,11 +320,15 @@ class Engine:
         return qf, qr
 
     def iterate_am(self, omega: np.ndarray, error_max=1e-10, max_itr=1000, n_hist=20, domain=False,
-                   switch_error=0.0, mix_max=0.0, restart=0.0):
-        """Anderson-mixing solve of every instance; returns (omega, rho, results)."""
+                   switch_error=0.0, mix_max=0.0, restart=0.0, graph_check=0):
+        """Anderson-mixing solve of every instance; returns (omega, rho, results).
+        graph_check > 0: whole iterations replay from a captured CUDA graph
+        with the Anderson step on the device, the host checking the
+        instances every graph_check iterations."""
         w = np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr).copy()
         rho = np.zeros_like(w)
-        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error, mix_max, restart)
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error, mix_max, restart,
+                           graph_check)
         res = (PscfgAmResult * self.n_inst)()
         self._check(self.lib.pscfg_iterate_am(self._h, _ptr(w), C.byref(prm), _ptr(rho), res), allow=(ENOTCONV,))
         return w, rho, self._results(res, domain)
@@ -386,10 +391,11 @@ class Engine:
         return out
 
     def am_begin(self, omega, error_max=1e-10, max_itr=1000, n_hist=20, domain=False, switch_error=0.0,
-                 mix_max=0.0, restart=0.0):
+                 mix_max=0.0, restart=0.0, graph_check=0):
         w = None if omega is None else np.ascontiguousarray(omega, dtype=np.float64).reshape(self.n_inst, self.M, self.nr)
         self._am_domain = domain
-        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error, mix_max, restart)
+        prm = PscfgAmParam(max_itr, n_hist, 1 if domain else 0, error_max, switch_error, mix_max, restart,
+                           graph_check)
         self._check(self.lib.pscfg_am_begin(self._h, None if w is None else _ptr(w), C.byref(prm)))
 
     def am_iterate(self, iters: int = 1) -> int:
