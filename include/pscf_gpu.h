@@ -328,12 +328,14 @@ int pscfg_propagate_noalloc(int dim, const int *n, const double *ksq_dev, const 
  * basis_mod / grid_basis_mod tables, src/basis_mod.f90,
  * src/grid_basis_mod.f90:47-200): n_wave waves of the r2c half grid, wave j
  * at flat index wave_k[j] = kx + (n1/2+1)(ky + n2 kz) (0 <= kx <= n1/2), in
- * star wave_star[j] (0-based), with complex coefficient
- * (coeff[2j], coeff[2j+1]) of the star's basis function
- * f_s(r) = sum_G c_s(G) exp(i G.r) over all waves G; the waves outside the
- * half grid are the Hermitian partners, c_s(-G) = conj c_s(G).  Each
- * half-grid wave appears at most once; waves of cancelled stars are left
- * out.  The tables (sorted by star) stay on the device. */
+ * real basis function wave_star[j] (0-based), with complex coefficient
+ * (coeff[2j], coeff[2j+1]) of f_s(r) = sum_G c_s(G) exp(i G.r) over all
+ * waves G; the waves outside the half grid are the Hermitian partners,
+ * c_s(-G) = conj c_s(G).  A half-grid wave belongs to one function, or to
+ * two: the cosine- and sine-like functions (phi +- conj phi) / sqrt(+-2) of
+ * a pair of stars related by inversion in a group without inversion (the
+ * reference's star_invert = +1 / -1); waves of cancelled stars are left
+ * out.  The tables (sorted by function) stay on the device. */
 int pscfg_set_basis(pscfg_engine *e, int inst, int n_star, int n_wave, const int *wave_k, const int *wave_star,
                     const double *coeff);
 

@@ -5,15 +5,25 @@ functions, one per star of waves related by the space group
 (make_waves / make_stars, src/basis_mod.f90:453-1227; basis_to_kgrid /
 kgrid_to_basis, src/grid_basis_mod.f90:47-200).  Here a star is the orbit
 of a wave index G under the point operations G -> M^T G (mod n) of the
-group's action on the grid, and its basis function is the projection of the
+group's action on the grid, and its star function is the projection of the
 plane wave e^{iG.r} onto the group-invariant fields,
 
-    P e_G = (1/|g|) sum_g exp(2 pi i G.t_g / n) e_{M_g^T G},
+    phi = P e_G = (1/|g|) sum_g exp(2 pi i G.t_g / n) e_{M_g^T G},
 
-made real (centrosymmetric groups give a real function up to a phase) and
-normalised to a grid average of 1 for its square.  Stars whose projection
+normalised to a grid average of 1 for |phi|^2.  Stars whose projection
 vanishes are the reference's cancelled stars and are dropped.  Stars are
 ordered by |G|^2 of their minimum-image wave, like the reference.
+
+A star closed under inversion (-G in the star for every G; every star of a
+centrosymmetric group) gives one real basis function: phi itself, or -i phi
+when phi is odd under inversion (the reference's sine-like closed stars,
+basis_sign = -1).  In a group without inversion, stars also come in pairs
+related by inversion (star_invert = +1 / -1, src/basis_mod.f90:206-310):
+the second star's function is conj(phi), and the pair gives the two real
+functions (phi + conj phi)/sqrt(2) and (phi - conj phi)/(i sqrt(2)), listed
+one after the other (cosine-like first).  Every basis function is thus
+real, with coefficients c(-G) = conj c(G) over a wave set closed under
+inversion, and the functions are orthonormal.
 
 Coefficients are taken by FFT: a_s = <f, f_s> = sum_G conj(c_s(G)) F[f](G)/N.
 """
@@ -47,11 +57,11 @@ class StarBasis:
         gsq = (v * v).sum(axis=1)
         order = np.lexsort((np.arange(self.nr), np.round(gsq, 10)))
         nvec = np.array(n)
-        visited = np.zeros(self.nr, dtype=bool)
         flat = lambda g: g[..., 0] + n[0] * (g[..., 1] + n[1] * g[..., 2])
-        self.star_idx: List[np.ndarray] = []
-        self.star_coef: List[np.ndarray] = []
-        self.star_gsq: List[float] = []
+        # stars: wave indices, normalised projection coefficients, |G|^2
+        visited = np.zeros(self.nr, dtype=bool)
+        orb_idx, orb_coef, orb_gsq = [], [], []
+        orbit_of = {}
         for w in order:
             if visited[w]:
                 continue
@@ -64,31 +74,62 @@ class StarBasis:
             np.add.at(coef, inv, ph)
             coef /= nops
             visited[uniq] = True
-            # real part or imaginary part, whichever survives (with the
-            # conjugate partner -G inside the orbit for centrosymmetric groups)
-            neg = flat((-G[uniq]) % nvec)
-            pos = {int(k): i for i, k in enumerate(uniq)}
-            partner = np.array([pos.get(int(k), -1) for k in neg])
-            if np.any(partner < 0):
-                cre, cim = coef, np.zeros_like(coef)
-            else:
-                cre = 0.5 * (coef + np.conj(coef[partner]))
-                cim = 0.5 * (coef - np.conj(coef[partner])) / 1j
-            best = cre if np.sum(np.abs(cre) ** 2) >= np.sum(np.abs(cim) ** 2) else cim
-            nrm = np.sum(np.abs(best) ** 2)
+            nrm = np.sum(np.abs(coef) ** 2)
             if nrm < 1e-20:
                 continue                                                     # cancelled star
-            self.star_idx.append(uniq)
-            self.star_coef.append(best / np.sqrt(nrm))
-            self.star_gsq.append(float(gsq[w]))
+            for k in uniq:
+                orbit_of[int(k)] = len(orb_idx)
+            orb_idx.append(uniq)
+            orb_coef.append(coef / np.sqrt(nrm))
+            orb_gsq.append(float(gsq[w]))
+        # inverse partner of every star (itself when closed under inversion)
+        partner = []
+        for idx in orb_idx:
+            g = np.stack([idx % n[0], (idx // n[0]) % n[1], idx // (n[0] * n[1])], axis=1)
+            neg = flat((-g) % nvec)
+            partner.append(orbit_of[int(neg[0])])
+        self.orbit_idx, self.orbit_coef, self.orbit_partner = orb_idx, orb_coef, partner
+        # real basis functions
+        self.star_idx: List[np.ndarray] = []
+        self.star_coef: List[np.ndarray] = []
+        self.star_gsq: List[float] = []
+        self.star_invert: List[int] = []
+        self.star_orbit: List[int] = []
+        for o, (idx, c) in enumerate(zip(orb_idx, orb_coef)):
+            p = partner[o]
+            if p == o:
+                # phi(-G) = +- conj phi(G): real (cosine-like) or i x real
+                g = np.stack([idx % n[0], (idx // n[0]) % n[1], idx // (n[0] * n[1])], axis=1)
+                pos = {int(k): i for i, k in enumerate(idx)}
+                j = np.array([pos[int(k)] for k in flat((-g) % nvec)])
+                odd = np.sum(np.abs(c + np.conj(c[j])) ** 2) < np.sum(np.abs(c - np.conj(c[j])) ** 2)
+                self.star_idx.append(idx)
+                self.star_coef.append(-1j * c if odd else c)
+                self.star_gsq.append(orb_gsq[o])
+                self.star_invert.append(0)
+                self.star_orbit.append(o)
+            elif p > o:
+                # the pair (o, p): conj phi on the inverse waves of p
+                g = np.stack([idx % n[0], (idx // n[0]) % n[1], idx // (n[0] * n[1])], axis=1)
+                neg = flat((-g) % nvec)
+                both = np.concatenate([idx, neg])
+                r2 = np.sqrt(2.0)
+                self.star_idx += [both, both]
+                self.star_coef += [np.concatenate([c, np.conj(c)]) / r2,
+                                   np.concatenate([c, -np.conj(c)]) / (1j * r2)]
+                self.star_gsq += [orb_gsq[o], orb_gsq[o]]
+                self.star_invert += [1, -1]
+                self.star_orbit += [o, p]
         self.n_star = len(self.star_idx)
 
     def half_grid_tables(self):
-        """The waves of every star that lie in the r2c half grid
+        """The waves of every basis function that lie in the r2c half grid
         (0 <= kx <= n1/2): their flat half-grid index kx + (n1/2+1)(ky + n2 kz),
-        star index and coefficient -- the device tables of
-        pscfg_set_basis.  The partner -G of every wave must belong to the
-        same star with the conjugate coefficient (centrosymmetric groups)."""
+        basis-function index and coefficient -- the device tables of
+        pscfg_set_basis.  Every function is real (the partner -G of each of
+        its waves is in its wave set with the conjugate coefficient); a wave
+        belongs to two functions for the pairs of stars related by
+        inversion."""
         n = self.n
         n1h = n[0] // 2 + 1
         flat = lambda g: g[..., 0] + n[0] * (g[..., 1] + n[1] * g[..., 2])
@@ -102,8 +143,7 @@ class StarBasis:
             for i, kneg in enumerate(neg):
                 j = pos.get(int(kneg), -1)
                 if j < 0 or abs(c[j] - np.conj(c[i])) > 1e-12:
-                    raise NotImplementedError("star basis tables need each wave's partner -G in its star "
-                                              "(centrosymmetric groups)")
+                    raise ValueError(f"basis function {s} is not real")
             keep = x <= n[0] // 2
             ks.append(x[keep] + n1h * rest[keep])
             ss.append(np.full(int(keep.sum()), s))

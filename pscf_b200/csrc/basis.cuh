@@ -6,10 +6,16 @@
 // wave's coefficient into the half k-grid, an inverse FFT gives the grid
 // field; kgrid_to_basis (:124-200) reads the forward FFT of rho back into
 // star coefficients.  Here the star structure of an instance is held as
-// device tables sorted by star (CSR): the half-grid index k, the star and the
-// complex coefficient c of each wave, so both maps are one kernel each:
-//   scatter  S[k_j] = a[star_j] c_j          (every half-grid wave at most once)
+// device tables sorted by basis function (CSR): the half-grid index k, the
+// function and the complex coefficient c of each wave, so both maps are one
+// kernel each:
+//   scatter  S[k_j] += a[star_j] c_j
 //   gather   a_s = sum_{j in s} w_j Re(conj(c_j) S[k_j]) / N
+// A half-grid wave belongs to one function, or to the two real functions
+// (cosine- and sine-like) of a pair of stars related by inversion in a group
+// without inversion (star_invert = +-1, src/grid_basis_mod.f90:82-110); its
+// two contributions are added atomically into the zeroed S, and a sum of
+// two terms onto zero does not depend on their order.
 // with w = 2 for the half-grid waves whose Hermitian partner lies outside the
 // half grid (0 < kx < n1/2) and 1 otherwise.  The gather sums each star in a
 // fixed order (one warp per star), so results are reproducible.
@@ -29,15 +35,17 @@ struct BasisJob {
     double *out;             // gather: coefficients out [n_star]
 };
 
-// grid = (ceil(max n_wave / 256), njobs): S[k_j] = a[star_j] c_j
-// (S zeroed beforehand).
+// grid = (ceil(max n_wave / 256), njobs): S[k_j] += a[star_j] c_j
+// (S zeroed beforehand; at most two terms per wave).
 static __global__ void k_basis_scatter(const BasisJob *jobs)
 {
     const BasisJob &J = jobs[blockIdx.y];
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < J.n_wave; j += gridDim.x * blockDim.x) {
         const double a = J.a[J.wave_star[j]];
         const cx<double> c = J.c[j];
-        J.S[J.wave_k[j]] = mk<double>(a * c.x, a * c.y);
+        double *S = (double *)(J.S + J.wave_k[j]);
+        atomicAdd(S, a * c.x);
+        atomicAdd(S + 1, a * c.y);
     }
 }
 

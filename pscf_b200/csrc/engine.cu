@@ -4035,8 +4035,9 @@ int pscfg_set_basis(pscfg_engine *e, int inst, int n_star, int n_wave, const int
     for (int j = 0; j < n_wave; j++) {
         if (wave_k[j] < 0 || wave_k[j] >= E.nk) throw Err(PSCFG_EINVAL, "wave index outside the half grid");
         if (wave_star[j] < 0 || wave_star[j] >= n_star) throw Err(PSCFG_EINVAL, "star index out of range");
-        if (seen[wave_k[j]]) throw Err(PSCFG_EINVAL, "a half-grid wave appears twice in the basis");
-        seen[wave_k[j]] = 1;
+        // at most two functions per wave: the pair of a star and its inverse
+        if (seen[wave_k[j]] >= 2) throw Err(PSCFG_EINVAL, "a half-grid wave appears more than twice in the basis");
+        seen[wave_k[j]]++;
         count[wave_star[j] + 1]++;
     }
     for (int s2 = 0; s2 < n_star; s2++) count[s2 + 1] += count[s2];

@@ -344,9 +344,9 @@ class Engine:
         self._check(self.lib.pscfg_set_symmetry(self._h, inst, len(M), ops.ctypes.data_as(C.POINTER(C.c_int))))
 
     def set_basis(self, inst: int, basis):
-        """Star basis (pscf_b200.basis.StarBasis of a centrosymmetric group)
-        of instance `inst` for density_basis: the waves of its stars that lie
-        in the r2c half grid, with their coefficients, as device tables."""
+        """Star basis (pscf_b200.basis.StarBasis) of instance `inst` for
+        density_basis: the waves of its basis functions that lie in the r2c
+        half grid, with their coefficients, as device tables."""
         k, star, coef = basis.half_grid_tables()
         ck = np.ascontiguousarray(k, dtype=np.int32)
         cs = np.ascontiguousarray(star, dtype=np.int32)

@@ -6,13 +6,19 @@ Basis format (input_field / output_field, :55-135): a header
 then one line per star: the N_monomer coefficients (ES20.12), the star's
 first wave G (I4 each, in first-Brillouin-zone form) and the number of
 waves in the star (I6).  A reader finds the star by its wave, so the line
-order does not matter (input_field :71-79).  The reference's basis
-function of a star is sum_G c_G exp(iG.r) with the coefficient of its first
-wave real and positive, 1/sqrt(N) with sqrt taken in single precision
-(src/basis_mod.f90:916-936), and the first wave is the largest in the
-ordering of G_lt (components compared in turn, :1576-1620).  Only stars
-closed under inversion are handled (the centrosymmetric groups); for
-other groups use the grid format.
+order does not matter (input_field :71-79).  The reference's star function
+is sum_G c_G exp(iG.r) with the coefficient of the star's wave real and
+positive, 1/sqrt(N) with sqrt taken in single precision
+(src/basis_mod.f90:916-936); the waves of a star are ordered by G_lt
+(components compared in turn, :1576-1620) and the star's wave is the first
+(largest) one.  A star closed under inversion is one real basis function,
+its coefficients multiplied by -i when the function is odd (sine-like,
+:1160-1192).  In a group without inversion two stars related by inversion
+form a pair (star_invert = +1, -1): the +1 star is the one holding the
+larger wave, the -1 star's wave is its last one (the inverse of the +1
+star's wave) and its coefficients are real and positive there; their
+coefficients a, b weigh the waves as (a -+ i b) c_G / sqrt(2)
+(basis_to_kgrid / kgrid_to_basis, src/grid_basis_mod.f90:47-200).
 
 Grid format (output_field_grid :151-200, read back by RGRID_TO_FIELD,
 src/pscf.fp.f90:890-980): the same header up to N_monomer, then ngrid and
@@ -100,16 +106,13 @@ def _spectrum(field: np.ndarray, n: Sequence[int]) -> np.ndarray:
     return (np.fft.fftn(field.reshape(n[2], n[1], n[0])) / nr).ravel()
 
 
-def _centrosymmetric_star(idx: np.ndarray, n: Sequence[int]) -> bool:
-    g = _grid_waves(idx, n)
-    neg = (-g) % np.array(n)
-    key = lambda w: set(map(tuple, w.tolist()))
-    return key(neg) == key(g)
-
-
 class FieldBasis:
     """Star basis of a group on a grid with the reference's file
-    conventions (first wave, coefficient normalisation)."""
+    conventions (star waves, coefficient phases and normalisation, the
+    +1 / -1 pairs of a group without inversion), in the line order of
+    StarBasis.  stars[k]: dict(idx = flat waves, cref = their coefficients,
+    kind = 0 (closed), 1 or -1, wave = flat index of the star's wave,
+    wave_bz = its first-zone form, count)."""
 
     def __init__(self, group_name: str, system):
         self.group = group_name
@@ -117,37 +120,100 @@ class FieldBasis:
         self.n = list(system.n)
         self.nr = system.nr
         self.basis = StarBasis(group_name, system.ngrid)
-        Gb = make_unit_cell(system.dim, system.crystal_system, system.cell_param)[0]
-        self.first = []        # flat grid index of the reference's first wave
-        self.first_bz = []     # its first-zone form
-        self.count = []
+        self.Gb = make_unit_cell(system.dim, system.crystal_system, system.cell_param)[0]
+        b = self.basis
+        self.stars: List[Dict] = []
+        done = set()
+        for s in range(b.n_star):
+            o = b.star_orbit[s]
+            if o in done:
+                continue
+            p = b.orbit_partner[o]
+            if p == o:
+                self.stars.append(self._closed(o))
+                done.add(o)
+            else:
+                self.stars += self._pair(o, p)
+                done |= {o, p}
         self.star_of = {}
-        for s, idx in enumerate(self.basis.star_idx):
-            if not _centrosymmetric_star(idx, self.n):
-                raise ValueError(f"group {group_name!r}: stars not closed under inversion are not "
-                                 "supported in the basis format (use the grid format)")
-            bz = _g_to_bz(_grid_waves(np.asarray(idx), self.n), self.n, Gb, self.dim)
-            order = sorted(range(len(idx)), key=lambda j: tuple(bz[j][:self.dim]), reverse=True)
-            j0 = order[0]
-            self.first.append(int(idx[j0]))
-            self.first_bz.append(bz[j0][:self.dim].astype(int))
-            self.count.append(len(idx))
-            for i in idx:
-                self.star_of[int(i)] = s
+        for k, st in enumerate(self.stars):
+            for i in st["idx"]:
+                self.star_of[int(i)] = k
+        # first-zone waves and counts of the file lines
+        self.first = [st["wave"] for st in self.stars]
+        self.first_bz = [st["wave_bz"] for st in self.stars]
+        self.count = [st["count"] for st in self.stars]
+
+    def _sorted(self, o):
+        """Waves of star o in G_lt order (largest first), their first-zone forms."""
+        idx = np.asarray(self.basis.orbit_idx[o])
+        bz = _g_to_bz(_grid_waves(idx, self.n), self.n, self.Gb, self.dim)
+        order = sorted(range(len(idx)), key=lambda j: tuple(bz[j][:self.dim]), reverse=True)
+        return idx, bz, order
+
+    def _flat(self, g):
+        n = self.n
+        g = np.asarray(g) % np.array(n)
+        return int(g[0] + n[0] * (g[1] + n[1] * g[2]))
+
+    def _closed(self, o):
+        idx, bz, order = self._sorted(o)
+        c = np.asarray(self.basis.orbit_coef[o])
+        j0 = order[0]
+        g0 = _grid_waves(idx[j0:j0 + 1], self.n)[0]
+        jm = int(np.nonzero(idx == self._flat(-g0))[0][0])
+        ratio = c[jm] / c[j0]
+        if abs(ratio - 1) < 1e-8:
+            phase = 1.0
+        elif abs(ratio + 1) < 1e-8:
+            phase = -1j                                    # sine-like closed star
+        else:
+            raise ValueError(f"closed star {o} is neither cosine- nor sine-like")
+        cref = c / c[j0] / _fl32_sqrt(len(idx)) * phase
+        return dict(idx=idx, cref=cref, kind=0, wave=int(idx[j0]), wave_pos=j0,
+                    wave_bz=bz[j0][:self.dim].astype(int), count=len(idx))
+
+    def _pair(self, o, p):
+        so, sp = self._sorted(o), self._sorted(p)
+        first = lambda srt: tuple(srt[1][srt[2][0]][:self.dim])
+        (ip, bzp, ordp), (im, bzm, ordm) = (so, sp) if first(so) > first(sp) else (sp, so)
+        op, om = (o, p) if first(so) > first(sp) else (p, o)
+        j0 = ordp[0]
+        jl = ordm[-1]
+        g0 = _grid_waves(ip[j0:j0 + 1], self.n)[0]
+        if int(im[jl]) != self._flat(-g0):
+            raise ValueError(f"stars {op}, {om}: the last wave of the -1 star is not the inverse of the +1 star's wave")
+        cp = np.asarray(self.basis.orbit_coef[op])
+        cm = np.asarray(self.basis.orbit_coef[om])
+        plus = dict(idx=ip, cref=cp / cp[j0] / _fl32_sqrt(len(ip)), kind=1, wave=int(ip[j0]), wave_pos=j0,
+                    wave_bz=bzp[j0][:self.dim].astype(int), count=len(ip))
+        minus = dict(idx=im, cref=cm / cm[jl] / _fl32_sqrt(len(im)), kind=-1, wave=int(im[jl]), wave_pos=jl,
+                     wave_bz=bzm[jl][:self.dim].astype(int), count=len(im))
+        return [plus, minus]
 
     def to_coeffs(self, field: np.ndarray) -> np.ndarray:
-        """Reference basis coefficients [n_star] of a grid field."""
+        """Reference basis coefficients [n_star] of a grid field
+        (kgrid_to_basis)."""
         F = _spectrum(np.asarray(field, dtype=np.float64), self.n)
-        return np.array([float(np.real(F[i])) * _fl32_sqrt(c) for i, c in zip(self.first, self.count)])
+        out = np.zeros(len(self.stars))
+        r2 = np.sqrt(2.0)
+        for k, st in enumerate(self.stars):
+            z = F[st["wave"]] / st["cref"][st["wave_pos"]]
+            out[k] = z.real if st["kind"] == 0 else (r2 * z.real if st["kind"] == 1 else r2 * z.imag)
+        return out
 
     def to_grid(self, coeffs: Sequence[float]) -> np.ndarray:
-        """Grid field sum_s a_s f_s with the reference's basis functions."""
+        """Grid field of the reference's basis coefficients (basis_to_kgrid)."""
         F = np.zeros(self.nr, dtype=complex)
-        for s, a in enumerate(coeffs):
-            idx = np.asarray(self.basis.star_idx[s])
-            c = np.asarray(self.basis.star_coef[s])
-            j0 = int(np.nonzero(idx == self.first[s])[0][0])
-            F[idx] += a * c / c[j0] / _fl32_sqrt(self.count[s])
+        r2 = np.sqrt(2.0)
+        for k, st in enumerate(self.stars):
+            if st["kind"] == 0:
+                z = coeffs[k]
+            elif st["kind"] == 1:
+                z = complex(coeffs[k], -coeffs[k + 1]) / r2
+            else:
+                z = complex(coeffs[k - 1], coeffs[k]) / r2
+            F[st["idx"]] += z * st["cref"]
         n = self.n
         f = np.fft.ifftn(F.reshape(n[2], n[1], n[0])) * self.nr
         return np.real(f).ravel()
@@ -160,8 +226,8 @@ def write_field(path: str, fields: np.ndarray, system, group_name: str) -> None:
     coeffs = np.stack([fb.to_coeffs(f) for f in fields])          # [M][n_star]
     cell = {"dim": system.dim, "crystal_system": system.crystal_system, "cell_param": system.cell_param}
     out = _header(cell, group_name, len(fields))
-    out += [_label("N_star"), f"{fb.basis.n_star:>20d}"]
-    for s in range(fb.basis.n_star):
+    out += [_label("N_star"), f"{len(fb.stars):>20d}"]
+    for s in range(len(fb.stars)):
         line = "".join(f"{a:20.12E}" for a in coeffs[:, s]) + "    "
         line += "".join(f"{g:4d}" for g in fb.first_bz[s]) + f"{fb.count[s]:6d}"
         out.append(line)
@@ -180,7 +246,7 @@ def read_field(path: str, system, group_name: str = None) -> Tuple[Dict, np.ndar
     nstar = int(lines[i + 1].split()[0])
     M = h["N_monomer"]
     fb = FieldBasis(group_name or h["group_name"], system)
-    coeffs = np.zeros((M, fb.basis.n_star))
+    coeffs = np.zeros((M, len(fb.stars)))
     n = np.array(system.n)
     for line in lines[i + 2:i + 2 + nstar]:
         v = line.split()

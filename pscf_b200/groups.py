@@ -107,9 +107,14 @@ _GENERATORS: Dict[str, Tuple[int, List[str]]] = {
                      "-x,-y,-z", "x+1/2,y+1/2,z+1/2"]),
     "F d d d : 2": (3, ["-x+3/4,-y+3/4,z", "-x+3/4,y,-z+3/4", "-x,-y,-z",
                         "x,y+1/2,z+1/2", "x+1/2,y,z+1/2", "x+1/2,y+1/2,z"]),
+    # no inversion: the alternating gyroid of ABC triblocks (stars in pairs
+    # related by inversion, star_invert = +-1)
+    "I 41 3 2": (3, ["-x+1/2,-y,z+1/2", "-x,y+1/2,-z+1/2", "z,x,y", "y+3/4,x+1/4,-z+1/4",
+                     "x+1/2,y+1/2,z+1/2"]),
 }
 
-ALIASES = {"P 6 m m": "p 6 m m", "229": "I m -3 m", "230": "I a -3 d", "70": "F d d d : 2", "17": "p 6 m m"}
+ALIASES = {"P 6 m m": "p 6 m m", "229": "I m -3 m", "230": "I a -3 d", "70": "F d d d : 2", "17": "p 6 m m",
+           "214": "I 41 3 2", "I 4_1 3 2": "I 41 3 2"}
 # 1-D names as the reference spells them in 3-D notation (response_startup
 # maps 'P 1' to '1' for dim = 1, src/response_mod.f90:227)
 ALIASES_1D = {"P 1": "1", "P -1": "-1", "p -1": "-1"}

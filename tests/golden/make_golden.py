@@ -91,7 +91,7 @@ def main():
     g["bcc_sweep"] = [thermo(os.path.join(REF, "tools/python/tests/sweep/out/%d.out" % i)) for i in range(12)]
     src = os.path.join(REF, "src/space_groups_mod.f90")
     g["groups"] = {name: group_table(src, name)
-                   for name in ["-1", "p 6 m m", "I m -3 m", "I a -3 d", "F d d d : 2"]}
+                   for name in ["-1", "p 6 m m", "I m -3 m", "I a -3 d", "F d d d : 2", "I 41 3 2"]}
     g["source"] = {
         "lamellar_outfile": "tools/python/tests/outfile/in",
         "bcc_sweep": "tools/python/tests/sweep/out/{0..11}.out",

@@ -77,7 +77,33 @@ def test_rgrid_round_trip(tmp_path):
     assert _lines(str(p))[14].split()[0] == "12"
 
 
-def test_non_centrosymmetric_basis_rejected():
-    s = diblock(1, [16], "lamellar", [1.5])
-    with pytest.raises(ValueError):
-        F.FieldBasis("1", s)
+@pytest.mark.parametrize("group,dim,ngrid,crystal,cell", [
+    ("1", 1, [16], "lamellar", [1.5]),
+    ("P 1", 3, [4, 6, 8], "orthorhombic", [1.0, 1.5, 2.0]),
+    ("I 41 3 2", 3, [16, 16, 16], "cubic", [3.7]),
+])
+def test_basis_file_without_inversion(tmp_path, group, dim, ngrid, crystal, cell):
+    """Groups without inversion: stars related by inversion are written as
+    +1 / -1 pairs (the -1 line carries the inverse of the +1 line's wave),
+    and a symmetric field survives the round trip."""
+    s = diblock(dim, ngrid, crystal, cell)
+    w = omega_guess(s, 5, 2.0)
+    w = np.stack([G.symmetrize(w[m], group, ngrid) for m in range(2)])
+    p = tmp_path / "w"
+    F.write_field(str(p), w, s, group)
+    _, back = F.read_field(str(p), s)
+    assert np.max(np.abs(back - w)) < 1e-10 * max(1.0, np.max(np.abs(w)))
+    fb = F.FieldBasis(group, s)
+    kinds = [st["kind"] for st in fb.stars]
+    assert len(fb.stars) == fb.basis.n_star and kinds.count(1) == kinds.count(-1) > 0
+    for k, st in enumerate(fb.stars):
+        if st["kind"] == 1:
+            assert fb.stars[k + 1]["kind"] == -1
+            g = np.array(st["wave_bz"])
+            gm = np.array(fb.stars[k + 1]["wave_bz"])
+            assert np.all((g + gm) % np.array(ngrid) == 0)
+    # coefficients of one basis function come back as a unit vector
+    for k in range(min(len(fb.stars), 12)):
+        a = np.zeros(len(fb.stars))
+        a[k] = 1.0
+        np.testing.assert_allclose(fb.to_coeffs(fb.to_grid(a)), a, atol=1e-12)

@@ -18,7 +18,11 @@ CASES = [("I m -3 m", 3, [20, 20, 20], "cubic", [3.9]),
          ("I a -3 d", 3, [16, 16, 16], "cubic", [3.7]),
          ("p 6 m m", 2, [24, 24], "hexagonal", [1.9]),
          ("-1", 1, [32], "lamellar", [1.7]),
-         ("-1", 1, [27], "lamellar", [1.4])]
+         ("-1", 1, [27], "lamellar", [1.4]),
+         # groups without inversion: cosine / sine pairs of stars share their
+         # half-grid waves (I 41 3 2 also has sine-like closed stars)
+         ("I 41 3 2", 3, [16, 16, 16], "cubic", [3.7]),
+         ("1", 1, [32], "lamellar", [1.7])]
 
 
 def _symmetric_omega(s, group, seed):
