@@ -407,7 +407,7 @@ def run_ours(args, rank, world, local_rank):
     if args.config == "c5" and not args.no_c2:
         nested["c2_bcc32_x64"] = c2_leg(args, rank, world, barrier, dev, local_rank)
     if not args.no_c4:
-        nested["mixed_shape_batch"] = c4_leg(rank, world, barrier, dev)
+        nested["mixed_shape_batch"] = c4_leg(rank, world, barrier, dev, args.c4_graph_check)
 
     if rank != 0:
         return
@@ -593,16 +593,18 @@ def c2_leg(args, rank, world, barrier, dev, local_rank):
     return out
 
 
-def c4_leg(rank, world, barrier, dev):
+def c4_leg(rank, world, barrier, dev, graph_check=0):
     """Concurrent solve of the mixed-shape batch (one engine and stream per
-    grid shape), wall clock."""
+    grid shape), wall clock; graph_check > 0 runs the iterations from
+    captured graphs with the Anderson step on the device."""
     import torch
     import torch.distributed as dist
     from pscf_b200.batch import solve_batches
     batches = c4_batches(20261203 + 3 + 1000 * rank)
     barrier()
     t0 = time.perf_counter()
-    results = solve_batches(batches, error_max=1e-9, max_itr=1000, n_hist=20, domain=True)
+    results = solve_batches(batches, error_max=1e-9, max_itr=1000, n_hist=20, domain=True,
+                            graph_check=graph_check)
     torch.cuda.synchronize()
     c4_s = time.perf_counter() - t0
     nconv = sum(1 for rs in results for r in rs if r["converged"])
@@ -616,6 +618,7 @@ def c4_leg(rank, world, barrier, dev):
     out = {"instances": int(tc[2].item()), "converged": int(tc[1].item()), "seconds": float(tc[0].item()),
            "solves_per_s": float(tc[1].item()) / float(tc[0].item()),
            "per_shape_converged": [sum(1 for r in rs if r["converged"]) for rs in results],
+           "graph_check": graph_check,
            "note": "wall clock of concurrent engines (one host thread and stream per grid shape)"}
     for b in batches:
         b.engine.close()
@@ -633,6 +636,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c2", action="store_true", help="skip the nested BCC 32^3 x 64 leg")
     ap.add_argument("--no-c4", action="store_true", help="skip the mixed-shape batch leg")
+    ap.add_argument("--c4-graph-check", type=int, default=0,
+                    help="mixed-shape batch: iterations per host check of the graph-driven Anderson loop "
+                         "(0: host-driven iterations)")
     ap.add_argument("--no-solve", action="store_true",
                     help="time the Anderson iterations only (no full FP64 / mixed solves; profiling runs)")
     ap.add_argument("--ds", type=float, default=0.0,
