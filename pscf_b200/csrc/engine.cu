@@ -18,6 +18,8 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -155,11 +157,23 @@ struct Engine {
     // CUDA graphs of 3-D sweeps, keyed by descriptor address, field and step count
     struct SweepGraph {
         const void *dfl;
-        int nf, ns, tsize, t0;
+        int nf, ns, tsize, t0, variant;
         cudaGraphExec_t exec;
         long launches;
     };
     std::vector<SweepGraph> graphs;
+    // planes-per-CTA measurements of the register sweep in progress, per
+    // (grid, precision, field count, step count): one timed sweep per candidate
+    struct PlaneTune {
+        int cand[4] = {0, 0, 0, 0};
+        int ncand = 0;
+        int uses[4] = {0, 0, 0, 0};
+        float ms[4] = {0, 0, 0, 0};
+        int pending = -1;            // candidate whose timed sweep awaits its events
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+    };
+    std::map<long, PlaneTune> tune;
+    PlaneTune *tune_now = nullptr;   // set while a timed sweep is being enqueued
     // optional CUDA-event timing of the phases (ms, accumulated)
     bool profiling = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -213,6 +227,10 @@ struct Engine {
 
     ~Engine()
     {
+        for (auto &t : tune) {
+            if (t.second.e0) cudaEventDestroy(t.second.e0);
+            if (t.second.e1) cudaEventDestroy(t.second.e1);
+        }
         if (amg_exec) cudaGraphExecDestroy(amg_exec);
         for (void *p : cap_blocks) cudaFree(p);
         if (st_up) cudaStreamDestroy(st_up);
@@ -715,15 +733,61 @@ static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
 // SMs share the work: at 32^3, 20 Anderson iterations of one BCC instance
 // sweep in 61 ms with one plane per CTA against 107 ms with four, while 64
 // instances are fastest with four (465 ms against 473 with two).
-static int sweep_planes(const Engine &E, int nf, int n3, int pmax)
+// Planes per CTA of the register sweep (pmax, pmax/2, ..., 1), measured:
+// for each (grid, precision, field count, step count) every candidate runs
+// one real sweep (every choice gives identical results), its graph replay
+// timed with CUDA events on the engine stream (after any capture), and the
+// fastest is kept for the process (all engines).  PSCFG_PLANES forces a choice; inside a captured
+// Anderson iteration the decided choice, or until then the launch-size
+// rule (the largest count whose launch still has >= 512 CTAs), is used.
+static std::mutex g_planes_mu;
+static std::map<long, int> g_planes_best;
+
+static int planes_rule(int nf, int n3, int pmax)
 {
+    int p = pmax;
+    while (p > 1 && (long)nf * (n3 / p) < 512) p /= 2;
+    return p;
+}
+
+static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, int nsteps)
+{
+    E.tune_now = nullptr;
     if (E.planes > 0) {
         for (int p = pmax; p >= 1; p /= 2)
             if (E.planes == p) return p;
     }
-    int p = pmax;
-    while (p > 1 && (long)nf * (n3 / p) < 512) p /= 2;
-    return p;
+    const long key = (((long)n3 * 16 + tsize) * 100000 + nf) * 100000 + nsteps;
+    {
+        std::lock_guard<std::mutex> lk(g_planes_mu);
+        auto it = g_planes_best.find(key);
+        if (it != g_planes_best.end()) return it->second;
+    }
+    if (E.capturing || E.no_graphs) return planes_rule(nf, n3, pmax);
+    Engine::PlaneTune &T = E.tune[key];
+    if (T.ncand == 0) {
+        for (int p = pmax; p >= 1 && T.ncand < 4; p /= 2) T.cand[T.ncand++] = p;
+        CK(cudaEventCreate(&T.e0));
+        CK(cudaEventCreate(&T.e1));
+    }
+    if (T.pending >= 0) {
+        CK(cudaEventSynchronize(T.e1));
+        CK(cudaEventElapsedTime(&T.ms[T.pending], T.e0, T.e1));
+        T.pending = -1;
+    }
+    for (int i = 0; i < T.ncand; i++)
+        if (T.uses[i] < 1) {
+            T.uses[i] = 1;
+            T.pending = i;
+            E.tune_now = &T;
+            return T.cand[i];
+        }
+    int best = 0;
+    for (int i = 1; i < T.ncand; i++)
+        if (T.ms[i] < T.ms[best]) best = i;
+    std::lock_guard<std::mutex> lk(g_planes_mu);
+    g_planes_best[key] = T.cand[best];
+    return T.cand[best];
 }
 
 // Runs emit() -- a fixed sequence of sweep launches whose jobs are read from
@@ -731,14 +795,16 @@ static int sweep_planes(const Engine &E, int nf, int n3, int pmax)
 // field count, step count, precision) and replayed after each descriptor
 // upload (PSCFG_NO_GRAPHS=1 launches directly).
 template <typename Emit>
-static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsize, int t0, Emit emit)
+static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsize, int t0, Emit emit,
+                        int variant = 0, cudaEvent_t before = nullptr)
 {
     if (E.no_graphs || E.capturing) {   // inside a captured Anderson iteration: its own nodes
         emit();
         return;
     }
     for (auto &g : E.graphs)
-        if (g.dfl == dfl && g.nf == nf && g.ns == ns_max && g.tsize == tsize && g.t0 == t0) {
+        if (g.dfl == dfl && g.nf == nf && g.ns == ns_max && g.tsize == tsize && g.t0 == t0 && g.variant == variant) {
+            if (before) CK(cudaEventRecord(before, E.st));
             CK(cudaGraphLaunch(g.exec, E.st));
             E.launches += g.launches;
             return;
@@ -749,6 +815,7 @@ static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsiz
     sg.ns = ns_max;
     sg.tsize = tsize;
     sg.t0 = t0;
+    sg.variant = variant;
     const long l0 = E.launches;
     CK(cudaStreamBeginCapture(E.st, cudaStreamCaptureModeThreadLocal));
     cudaGraph_t graph = nullptr;
@@ -769,6 +836,7 @@ static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsiz
         E.graphs.erase(E.graphs.begin());
     }
     E.graphs.push_back(sg);
+    if (before) CK(cudaEventRecord(before, E.st));
     CK(cudaGraphLaunch(sg.exec, E.st));
 }
 
@@ -805,12 +873,15 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int
                 E.launched();
             }
         };
-        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), t0, emit);
+        Engine::PlaneTune *timed = E.tune_now;
+        E.tune_now = nullptr;
+        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), t0, emit, PPC, timed ? timed->e0 : nullptr);
+        if (timed) CK(cudaEventRecord(timed->e1, E.st));
     };
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 32 && b == 32 && c == 32) {
         using N = std::integral_constant<int, 32>;
-        switch (sweep_planes(E, nf, 32, 4)) {
+        switch (sweep_planes(E, nf, 32, 4, (int)sizeof(T), ns_max - t0)) {
         case 4: run(N(), std::integral_constant<int, 4>()); break;
         case 2: run(N(), std::integral_constant<int, 2>()); break;
         default: run(N(), std::integral_constant<int, 1>()); break;
@@ -819,7 +890,7 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int
     }
     if (a == 16 && b == 16 && c == 16) {
         using N = std::integral_constant<int, 16>;
-        switch (sweep_planes(E, nf, 16, 8)) {
+        switch (sweep_planes(E, nf, 16, 8, (int)sizeof(T), ns_max - t0)) {
         case 8: run(N(), std::integral_constant<int, 8>()); break;
         case 4: run(N(), std::integral_constant<int, 4>()); break;
         case 2: run(N(), std::integral_constant<int, 2>()); break;
@@ -4495,5 +4566,16 @@ long pscfg_steps_per_density(const pscfg_engine *e)
 }
 
 long pscfg_launch_count(const pscfg_engine *e) { return e ? e->E.launches : 0; }
+
+int pscfg_sweep_planes(const pscfg_engine *e, int n_fields, int n_steps, int fp32)
+{
+    if (!e || e->E.dim != 3 || e->E.n[0] != e->E.n[1] || e->E.n[1] != e->E.n[2]) return 0;
+    const int n3 = e->E.n[2];
+    if (n3 != 16 && n3 != 32) return 0;
+    const long key = (((long)n3 * 16 + (fp32 ? 4 : 8)) * 100000 + n_fields) * 100000 + n_steps;
+    std::lock_guard<std::mutex> lk(g_planes_mu);
+    auto it = g_planes_best.find(key);
+    return it == g_planes_best.end() ? 0 : it->second;
+}
 
 }  // extern "C"

@@ -361,3 +361,19 @@ def test_rough_fields_all_kernel_paths(monkeypatch, dim, ngrid, crystal, cell, p
     assert rel_err(q[0, :1], q_ref) < 1e-12
     assert rel_err(rho[0], rho_ref) < 1e-12, ("density", rel_err(rho[0], rho_ref))
     e.close()
+
+
+def test_measured_planes_per_cta():
+    """The register sweep's planes per CTA are measured on the first sweeps
+    of each (grid, precision, field count, step count) -- one real sweep per
+    candidate -- and the choice never changes the densities."""
+    ss = [diblock(3, [32, 32, 32], "cubic", [3.9], fA=0.25 + 0.02 * i, chiN=20.0, ds=0.02) for i in range(3)]
+    w = np.stack([omega_guess(s, 40 + i, 2.0) for i, s in enumerate(ss)])
+    e = Engine(ss, FP64)
+    nsteps = e.steps_per_density // (2 * len(ss))
+    outs = [e.density(w)[0] for _ in range(5)]
+    p = e.sweep_planes(2 * len(ss), nsteps)
+    e.close()
+    assert p in (1, 2, 4), p
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
