@@ -162,18 +162,8 @@ struct Engine {
         long launches;
     };
     std::vector<SweepGraph> graphs;
-    // planes-per-CTA measurements of the register sweep in progress, per
-    // (grid, precision, field count, step count): one timed sweep per candidate
-    struct PlaneTune {
-        int cand[4] = {0, 0, 0, 0};
-        int ncand = 0;
-        int uses[4] = {0, 0, 0, 0};
-        float ms[4] = {0, 0, 0, 0};
-        int pending = -1;            // candidate whose timed sweep awaits its events
-        cudaEvent_t e0 = nullptr, e1 = nullptr;
-    };
-    std::map<long, PlaneTune> tune;
-    PlaneTune *tune_now = nullptr;   // set while a timed sweep is being enqueued
+    // events timing the trial sweeps of the planes-per-CTA choice
+    cudaEvent_t tune_e0 = nullptr, tune_e1 = nullptr;
     // optional CUDA-event timing of the phases (ms, accumulated)
     bool profiling = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -227,10 +217,8 @@ struct Engine {
 
     ~Engine()
     {
-        for (auto &t : tune) {
-            if (t.second.e0) cudaEventDestroy(t.second.e0);
-            if (t.second.e1) cudaEventDestroy(t.second.e1);
-        }
+        if (tune_e0) cudaEventDestroy(tune_e0);
+        if (tune_e1) cudaEventDestroy(tune_e1);
         if (amg_exec) cudaGraphExecDestroy(amg_exec);
         for (void *p : cap_blocks) cudaFree(p);
         if (st_up) cudaStreamDestroy(st_up);
@@ -733,13 +721,18 @@ static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
 // SMs share the work: at 32^3, 20 Anderson iterations of one BCC instance
 // sweep in 61 ms with one plane per CTA against 107 ms with four, while 64
 // instances are fastest with four (465 ms against 473 with two).
-// Planes per CTA of the register sweep (pmax, pmax/2, ..., 1), measured:
-// for each (grid, precision, field count, step count) every candidate runs
-// one real sweep (every choice gives identical results), its graph replay
-// timed with CUDA events on the engine stream (after any capture), and the
-// fastest is kept for the process (all engines).  PSCFG_PLANES forces a choice; inside a captured
-// Anderson iteration the decided choice, or until then the launch-size
-// rule (the largest count whose launch still has >= 512 CTAs), is used.
+// Planes per CTA of the register sweep (pmax, pmax/2, ..., 1), measured.
+// The first sweep of each (grid, precision, field count, step count) is
+// preceded by one trial sweep per candidate, timed with CUDA events on the
+// engine stream (a graph replay, after its capture); the fastest is kept
+// for the process (all engines) and the real sweep runs with it.  A trial
+// writes only the slices that the real sweep then writes again, so every
+// result comes from the chosen count -- which matters: the largest count's
+// column pass pairs the real columns kx = 0 and n/2 into one complex column
+// and rounds differently from the others.  PSCFG_PLANES forces a choice;
+// inside a captured Anderson iteration the decided choice, or until then
+// the launch-size rule (the largest count whose launch still has >= 512
+// CTAs), is used.
 static std::mutex g_planes_mu;
 static std::map<long, int> g_planes_best;
 
@@ -750,44 +743,46 @@ static int planes_rule(int nf, int n3, int pmax)
     return p;
 }
 
-static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, int nsteps)
+static long planes_key(int n3, int tsize, int nf, int nsteps)
 {
-    E.tune_now = nullptr;
+    return (((long)n3 * 16 + tsize) * 100000 + nf) * 100000 + nsteps;
+}
+
+// trial(p, e0, e1) enqueues one sweep with p planes per CTA, recording e0
+// just before its first launch and e1 after its last.
+template <typename Trial>
+static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, int nsteps, Trial trial)
+{
     if (E.planes > 0) {
         for (int p = pmax; p >= 1; p /= 2)
             if (E.planes == p) return p;
     }
-    const long key = (((long)n3 * 16 + tsize) * 100000 + nf) * 100000 + nsteps;
+    const long key = planes_key(n3, tsize, nf, nsteps);
     {
         std::lock_guard<std::mutex> lk(g_planes_mu);
         auto it = g_planes_best.find(key);
         if (it != g_planes_best.end()) return it->second;
     }
-    if (E.capturing || E.no_graphs) return planes_rule(nf, n3, pmax);
-    Engine::PlaneTune &T = E.tune[key];
-    if (T.ncand == 0) {
-        for (int p = pmax; p >= 1 && T.ncand < 4; p /= 2) T.cand[T.ncand++] = p;
-        CK(cudaEventCreate(&T.e0));
-        CK(cudaEventCreate(&T.e1));
+    if (E.capturing) return planes_rule(nf, n3, pmax);
+    if (!E.tune_e0) {
+        CK(cudaEventCreate(&E.tune_e0));
+        CK(cudaEventCreate(&E.tune_e1));
     }
-    if (T.pending >= 0) {
-        CK(cudaEventSynchronize(T.e1));
-        CK(cudaEventElapsedTime(&T.ms[T.pending], T.e0, T.e1));
-        T.pending = -1;
-    }
-    for (int i = 0; i < T.ncand; i++)
-        if (T.uses[i] < 1) {
-            T.uses[i] = 1;
-            T.pending = i;
-            E.tune_now = &T;
-            return T.cand[i];
+    int best = pmax;
+    float best_ms = 0;
+    for (int p = pmax; p >= 1; p /= 2) {
+        trial(p, E.tune_e0, E.tune_e1);
+        CK(cudaEventSynchronize(E.tune_e1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, E.tune_e0, E.tune_e1));
+        if (p == pmax || ms < best_ms) {
+            best = p;
+            best_ms = ms;
         }
-    int best = 0;
-    for (int i = 1; i < T.ncand; i++)
-        if (T.ms[i] < T.ms[best]) best = i;
+    }
     std::lock_guard<std::mutex> lk(g_planes_mu);
-    g_planes_best[key] = T.cand[best];
-    return T.cand[best];
+    auto ins = g_planes_best.emplace(key, best);   // another engine may have decided meanwhile
+    return ins.first->second;
 }
 
 // Runs emit() -- a fixed sequence of sweep launches whose jobs are read from
@@ -799,6 +794,7 @@ static void graph_sweep(Engine &E, const void *dfl, int nf, int ns_max, int tsiz
                         int variant = 0, cudaEvent_t before = nullptr)
 {
     if (E.no_graphs || E.capturing) {   // inside a captured Anderson iteration: its own nodes
+        if (before) CK(cudaEventRecord(before, E.st));
         emit();
         return;
     }
@@ -850,7 +846,7 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int
     // The sweep is a fixed sequence of 1 + 4 ns_max launches whose jobs are
     // read from the descriptors at dfl, so it is captured once into a CUDA
     // graph per (dfl, nf, ns_max) and replayed after each descriptor upload.
-    auto run = [&](auto n1c, auto ppcc) {
+    auto run = [&](auto n1c, auto ppcc, cudaEvent_t e0, cudaEvent_t e1) {
         constexpr int N = decltype(n1c)::value, PPC = decltype(ppcc)::value;
         constexpr int P = N * (N / 2 + 1);
         const size_t sm = sizeof(cx<T>) * PPC * P;
@@ -873,29 +869,33 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int
                 E.launched();
             }
         };
-        Engine::PlaneTune *timed = E.tune_now;
-        E.tune_now = nullptr;
-        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), t0, emit, PPC, timed ? timed->e0 : nullptr);
-        if (timed) CK(cudaEventRecord(timed->e1, E.st));
+        graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), t0, emit, PPC, e0);
+        if (e1) CK(cudaEventRecord(e1, E.st));
     };
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 32 && b == 32 && c == 32) {
         using N = std::integral_constant<int, 32>;
-        switch (sweep_planes(E, nf, 32, 4, (int)sizeof(T), ns_max - t0)) {
-        case 4: run(N(), std::integral_constant<int, 4>()); break;
-        case 2: run(N(), std::integral_constant<int, 2>()); break;
-        default: run(N(), std::integral_constant<int, 1>()); break;
-        }
+        auto go = [&](int p, cudaEvent_t e0, cudaEvent_t e1) {
+            switch (p) {
+            case 4: run(N(), std::integral_constant<int, 4>(), e0, e1); break;
+            case 2: run(N(), std::integral_constant<int, 2>(), e0, e1); break;
+            default: run(N(), std::integral_constant<int, 1>(), e0, e1); break;
+            }
+        };
+        go(sweep_planes(E, nf, 32, 4, (int)sizeof(T), ns_max - t0, go), nullptr, nullptr);
         return true;
     }
     if (a == 16 && b == 16 && c == 16) {
         using N = std::integral_constant<int, 16>;
-        switch (sweep_planes(E, nf, 16, 8, (int)sizeof(T), ns_max - t0)) {
-        case 8: run(N(), std::integral_constant<int, 8>()); break;
-        case 4: run(N(), std::integral_constant<int, 4>()); break;
-        case 2: run(N(), std::integral_constant<int, 2>()); break;
-        default: run(N(), std::integral_constant<int, 1>()); break;
-        }
+        auto go = [&](int p, cudaEvent_t e0, cudaEvent_t e1) {
+            switch (p) {
+            case 8: run(N(), std::integral_constant<int, 8>(), e0, e1); break;
+            case 4: run(N(), std::integral_constant<int, 4>(), e0, e1); break;
+            case 2: run(N(), std::integral_constant<int, 2>(), e0, e1); break;
+            default: run(N(), std::integral_constant<int, 1>(), e0, e1); break;
+            }
+        };
+        go(sweep_planes(E, nf, 16, 8, (int)sizeof(T), ns_max - t0, go), nullptr, nullptr);
         return true;
     }
     return false;
@@ -4572,7 +4572,7 @@ int pscfg_sweep_planes(const pscfg_engine *e, int n_fields, int n_steps, int fp3
     if (!e || e->E.dim != 3 || e->E.n[0] != e->E.n[1] || e->E.n[1] != e->E.n[2]) return 0;
     const int n3 = e->E.n[2];
     if (n3 != 16 && n3 != 32) return 0;
-    const long key = (((long)n3 * 16 + (fp32 ? 4 : 8)) * 100000 + n_fields) * 100000 + n_steps;
+    const long key = planes_key(n3, fp32 ? 4 : 8, n_fields, n_steps);
     std::lock_guard<std::mutex> lk(g_planes_mu);
     auto it = g_planes_best.find(key);
     return it == g_planes_best.end() ? 0 : it->second;
