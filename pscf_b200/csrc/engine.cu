@@ -214,6 +214,7 @@ struct Engine {
     char *cap_cur = nullptr;
     size_t cap_left = 0;
     cudaGraphExec_t amg_exec = nullptr;
+    std::vector<const double *> amg_G;   // per instance: its cell's G on the device (GeomJob of the run)
 
     ~Engine()
     {
@@ -911,7 +912,7 @@ static bool plane_kernels_apply(const Engine &E)
 
 // Position p of a forward four-step transform of length N (Split<N> of
 // fft_ct.cuh / kernels3p.cuh) -> frequency index.
-static int host_iperm(int N, int p)
+__host__ __device__ static inline int host_iperm(int N, int p)
 {
     int P = 1, Q = 1;
     switch (N) {
@@ -943,6 +944,45 @@ static void append_ek_factors(const Engine &E, const Cell &cell, double lap, std
         for (int xp = 0; xp <= M; xp++) out.push_back((T)expl(-c * g2(0, xp < M ? host_iperm(M, xp) : M)));
         for (int yp = 0; yp < n2; yp++) out.push_back((T)expl(-c * g2(1, host_iperm(n2, yp))));
         for (int zp = 0; zp < n3; zp++) out.push_back((T)expl(-c * g2(2, host_iperm(n3, zp))));
+    }
+}
+
+// The same factors computed on the device from a cell held there (the
+// graph-driven Anderson iteration updates the cell on the device): job j
+// writes 2 (N1/2+1+N2+N3) values from G (row-major 3 x 3, diagonal) and
+// lap.  grid = njobs, 256 threads.
+struct EkfJob {
+    const double *G;
+    double lap;
+    void *out;
+};
+
+template <typename T>
+static __global__ void k_ek_factors(const EkfJob *jobs, int n1, int n2, int n3)
+{
+    const EkfJob &J = jobs[blockIdx.x];
+    const int M = n1 / 2, L3 = M + 1 + n2 + n3;
+    T *out = (T *)J.out;
+    for (int i = threadIdx.x; i < 2 * L3; i += blockDim.x) {
+        const double c = J.lap / (i < L3 ? 6.0 : 12.0);
+        const int j = i % L3;
+        int axis, n, k;
+        if (j <= M) {
+            axis = 0;
+            n = n1;
+            k = j < M ? host_iperm(M, j) : M;
+        } else if (j < M + 1 + n2) {
+            axis = 1;
+            n = n2;
+            k = host_iperm(n2, j - M - 1);
+        } else {
+            axis = 2;
+            n = n3;
+            k = host_iperm(n3, j - M - 1 - n2);
+        }
+        const double kf = (k > n / 2) ? (double)(k - n) : (double)k;
+        const double g = J.G[axis * 3 + axis] * kf;
+        out[i] = (T)exp(-c * g * g);
     }
 }
 
@@ -1149,14 +1189,24 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
     if (fl.empty()) return;
     // separable k-space factors for the plane kernels when every cell of
     // the launch is orthogonal (written after the descriptors)
+    // (graph-driven iterations: from the cell on the device, k_ek_factors)
     std::vector<T> ekf;
+    std::vector<EkfJob> ekj;
     const int L3 = (int)(E.n[0] / 2 + 1) + E.n[1] + E.n[2];
-    if (plane_kernels_apply(E) && !E.amg) {   // graph-driven iterations: the cell lives on the device
+    if (plane_kernels_apply(E)) {
         bool ortho = true;
-        for (int i : act)
-            for (int a = 0; a < 3; a++)
-                for (int b2 = 0; b2 < 3; b2++)
-                    if (a != b2 && E.inst[i].cell.G[a][b2] != 0.0) ortho = false;
+        for (int i : act) {
+            if (E.amg) {
+                const int cs = E.inst[i].sys.crystal_system;
+                if ((cs != PSCFG_CUBIC && cs != PSCFG_TETRAGONAL && cs != PSCFG_ORTHORHOMBIC) ||
+                    i >= (int)E.amg_G.size() || !E.amg_G[i])
+                    ortho = false;
+            } else {
+                for (int a = 0; a < 3; a++)
+                    for (int b2 = 0; b2 < 3; b2++)
+                        if (a != b2 && E.inst[i].cell.G[a][b2] != 0.0) ortho = false;
+            }
+        }
         if (ortho) {
             for (int i : act) {
                 Inst &I = E.inst[i];
@@ -1164,7 +1214,12 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
                     for (int d = 0; d < 2; d++)
                         for (int b = 0; b < I.sys.n_block[c]; b++) {
                             const double kb = I.sys.kuhn[I.sys.block_monomer[c][b]];
-                            append_ek_factors<T>(E, I.cell, I.bds[c][b] * kb * kb, ekf);
+                            if (E.amg) {
+                                ekj.push_back(EkfJob{E.amg_G[i], I.bds[c][b] * kb * kb, nullptr});
+                                ekf.resize(ekf.size() + 2 * (size_t)L3, (T)0);
+                            } else {
+                                append_ek_factors<T>(E, I.cell, I.bds[c][b] * kb * kb, ekf);
+                            }
                         }
             }
         }
@@ -1173,12 +1228,21 @@ static void run_sweeps(Engine &E, const std::vector<int> &act)
     size_t off = ((tj.size() * sizeof(TableJob<T>) + 255) / 256) * 256;
     if (!ekf.empty()) {
         const size_t off_tab = off + ((fl.size() * sizeof(SweepField<T>) + 255) / 256) * 256;
-        E.desc(off_tab + ekf.size() * sizeof(T) + 256);   // capacity first: no reallocation below
-        dtj = E.upload(tj, 0);
+        const size_t off_ekj = off_tab + ((ekf.size() * sizeof(T) + 255) / 256) * 256;
+        if (!E.capturing) {   // capacity first: no reallocation below
+            E.desc(off_ekj + ekj.size() * sizeof(EkfJob) + 256);
+            dtj = E.upload(tj, 0);
+        }
         T *dtab = E.upload(ekf, off_tab);
         size_t k = 0;
         for (auto &f : fl)
             for (int b = 0; b < f.nblk; b++, k += 2 * (size_t)L3) f.ekf[b] = dtab + k;
+        if (!ekj.empty()) {
+            for (size_t j = 0; j < ekj.size(); j++) ekj[j].out = dtab + j * 2 * (size_t)L3;
+            EkfJob *dj = E.upload(ekj, off_ekj);
+            k_ek_factors<T><<<(unsigned)ekj.size(), 256, 0, E.st>>>(dj, E.n[0], E.n[1], E.n[2]);
+            E.launched();
+        }
     }
     SweepField<T> *dfl = E.upload(fl, off);
     {
@@ -2731,6 +2795,8 @@ static void amg_setup(Engine &E, AmRun &R, const std::vector<int> &act)
         g.kweight = I.kweight;
         g.wdg0 = I.kweight ? I.wdg0 : nullptr;
         g.gate = &R.g_st[act[k]].mixed;
+        E.amg_G.resize(E.inst.size(), nullptr);
+        E.amg_G[act[k]] = (const double *)((const char *)(R.g_geo + k) + offsetof(GeomJob, G));
         SymJob &y = sym[k];
         std::memset(&y, 0, sizeof(y));
         y.f = I.omega;

@@ -8,8 +8,8 @@ graph_check iterations.  Everything is compared with the host-driven
 iteration, which the oracle pins elsewhere.  The control kernels round as
 the host loop does (no multiply-add contraction, the same lambda ramp), so
 canonical runs on the k-space-table kernels give the host's iterates to the
-last bits; the grand ensemble (exp of mu on the device) and the grids whose
-host sweep uses separable k-space factors agree to roundoff."""
+last bits; the grand ensemble (exp of mu on the device) and the plane-kernel
+grids (separable k-space factors from the device cell) agree to roundoff."""
 import numpy as np
 import pytest
 
@@ -108,8 +108,9 @@ def test_fixed_iterations_match_host_blend(ensemble):
 
 
 def test_plane_kernel_grid_fixed_iterations():
-    """64^3 (the plane kernels; the graph uses the k-space tables where the
-    host-driven sweep uses separable factors)."""
+    """64^3 (the plane kernels; the graph computes their separable k-space
+    factors on the device from the device cell, the host-driven sweep on the
+    host in extended precision)."""
     s = diblock(3, [64, 64, 64], "cubic", [3.7], fA=0.4, chiN=16.0, ds=0.1)
     w0 = omega_guess(s, 3, 2.0)[None]
     kw = dict(error_max=1e-14, max_itr=3, domain=True)
