@@ -752,7 +752,7 @@ static long planes_key(int n3, int tsize, int nf, int nsteps)
 // trial(p, e0, e1) enqueues one sweep with p planes per CTA, recording e0
 // just before its first launch and e1 after its last.
 template <typename Trial>
-static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, int nsteps, Trial trial)
+static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, int nsteps, Trial trial, bool cluster = false)
 {
     if (E.planes > 0) {
         for (int p = pmax; p >= 1; p /= 2)
@@ -771,7 +771,7 @@ static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, int nste
     }
     int best = pmax;
     float best_ms = 0;
-    for (int p = pmax; p >= 1; p /= 2) {
+    for (int p = pmax; p >= (cluster ? 0 : 1); p = (p > 1 ? p / 2 : p - 1)) {
         trial(p, E.tune_e0, E.tune_e1);
         CK(cudaEventSynchronize(E.tune_e1));
         float ms = 0;
@@ -876,14 +876,30 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int
     const int a = E.n[0], b = E.n[1], c = E.n[2];
     if (a == 32 && b == 32 && c == 32) {
         using N = std::integral_constant<int, 32>;
+        // candidate 0: the one-launch cluster step (kernels3x.cuh), one
+        // launch per contour step instead of four
+        auto cluster = [&](cudaEvent_t e0, cudaEvent_t e1) {
+            const size_t sm = Cl32<T>::smem_bytes();
+            CK(allow_dyn_smem((const void *)k3x_step32<T>));
+            const PlaneGeom g = E.geom();
+            auto emit = [&]() {
+                for (int t = t0; t < ns_max; t++) {
+                    k3x_step32<T><<<dim3(8 * nf), 512, sm, E.st>>>(dfl, g, t);
+                    E.launched();
+                }
+            };
+            graph_sweep(E, dfl, nf, ns_max, (int)sizeof(T), t0, emit, 100, e0);
+            if (e1) CK(cudaEventRecord(e1, E.st));
+        };
         auto go = [&](int p, cudaEvent_t e0, cudaEvent_t e1) {
             switch (p) {
             case 4: run(N(), std::integral_constant<int, 4>(), e0, e1); break;
             case 2: run(N(), std::integral_constant<int, 2>(), e0, e1); break;
-            default: run(N(), std::integral_constant<int, 1>(), e0, e1); break;
+            case 1: run(N(), std::integral_constant<int, 1>(), e0, e1); break;
+            default: cluster(e0, e1); break;
             }
         };
-        go(sweep_planes(E, nf, 32, 4, (int)sizeof(T), ns_max - t0, go), nullptr, nullptr);
+        go(sweep_planes(E, nf, 32, 4, (int)sizeof(T), ns_max - t0, go, sizeof(T) == 8), nullptr, nullptr);
         return true;
     }
     if (a == 16 && b == 16 && c == 16) {
@@ -1267,7 +1283,10 @@ static void sweep_steps(Engine &E, const SweepField<T> *dfl, int nf, int t0, int
         size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)E.nr * sizeof(T);
         if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
         CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
-        int threads = (int)std::min<long>(256, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
+        // one CTA per field: a sweep of few fields is bound by the latency of
+        // its FFT phases, which more warps hide (64 x 64, one instance:
+        // 5.30 -> 4.28 ms per density with 512 threads instead of 256)
+        int threads = (int)std::min<long>(512, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
         k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, t0, t1);
         E.launched();
     } else {
@@ -4641,7 +4660,8 @@ int pscfg_sweep_planes(const pscfg_engine *e, int n_fields, int n_steps, int fp3
     const long key = planes_key(n3, fp32 ? 4 : 8, n_fields, n_steps);
     std::lock_guard<std::mutex> lk(g_planes_mu);
     auto it = g_planes_best.find(key);
-    return it == g_planes_best.end() ? 0 : it->second;
+    if (it == g_planes_best.end()) return 0;
+    return it->second > 0 ? it->second : -1;   // 0 in the cache: the cluster step
 }
 
 }  // extern "C"
