@@ -1279,13 +1279,22 @@ static void sweep_steps(Engine &E, const SweepField<T> *dfl, int nf, int t0, int
 {
     const PlaneGeom &g = E.geom();
     const int ns_max = t1;
+    if (E.dim == 2 && !E.no_fixed_kernels && E.n[0] == 64 && E.n[1] == 64) {
+        // fixed-shape whole-sweep kernel: tables and q in shared memory
+        const size_t sm = Sweep2P<T, 64, 64>::smem_bytes();
+        CK(allow_dyn_smem((const void *)k2p_sweep<T, 64, 64>));
+        k2p_sweep<T, 64, 64><<<nf, 256, sm, E.st>>>(dfl, t0, t1);
+        E.launched();
+        return;
+    }
     if (E.dim <= 2) {
         size_t sm = 2 * (size_t)g.n2 * g.LS * sizeof(cx<T>) + 2 * (size_t)E.nr * sizeof(T);
         if (sm > 227 * 1024) throw Err(PSCFG_EINVAL, "grid too large for the single-CTA plane step");
         CK(allow_dyn_smem((const void *)k_sweep_plane<T>));
         // one CTA per field: a sweep of few fields is bound by the latency of
-        // its FFT phases, which more warps hide (64 x 64, one instance:
-        // 5.30 -> 4.28 ms per density with 512 threads instead of 256)
+        // its FFT phases, which more warps hide (64 x 64 with this kernel,
+        // one instance: 5.30 -> 4.28 ms per density with 512 threads instead
+        // of 256; k2p_sweep above: 2.16 ms)
         int threads = (int)std::min<long>(512, std::max<long>(32, ((E.nr / 2 + 31) / 32) * 32));
         k_sweep_plane<T><<<nf, threads, sm, E.st>>>(dfl, g, t0, t1);
         E.launched();

@@ -556,4 +556,116 @@ __global__ void __launch_bounds__(256, 2) k3p_stress_z(const StressJob<T> *job, 
     }
 }
 
+// ---------------------------------------------------------------------
+// Whole 2-D sweep (dim = 2, the grid is one N1 x N2 plane) of one field per
+// CTA, for the small-batch case where a field's steps are latency bound:
+// the current block's tables (eo1, eo2 on the grid, ek1, ek2 on the half
+// spectrum [ky][kx]) and q, q1 stay in shared memory, and every transform
+// is PlaneP::forward / inverse in place (constant twiddles, conflict-free
+// line passes).  A step is the reference's step_exp
+// (src/step_mod.f90:146-176): q1 = eo1 F^-1[ek1 F[eo1 q]], two half steps
+// with eo2 / ek2, q <- (4 q2 - q1) / 3.  Optional per-step outputs as in
+// k_sweep_plane: f.q1, f.h_out (eo1 x first half step), f.q2_out.
+// grid = nfields, 256 threads.
+template <typename T, int N1, int N2>
+struct Sweep2P {
+    using PL = PlaneP<T, N1, N2>;
+    static constexpr int NP = PL::NP, PS = PL::PS, NH = PL::NH, NK = NH * N2;
+    static constexpr size_t smem_bytes() { return sizeof(cx<T>) * PS + sizeof(T) * (4 * NP + 2 * NK); }
+};
+
+template <typename T, int N1, int N2>
+__device__ __forceinline__ void k2p_mul(cx<T> *A, const T *ek)
+{
+    using PL = PlaneP<T, N1, N2>;
+    for (int i = threadIdx.x; i < PL::PS; i += blockDim.x) {
+        const int py = i / PL::NH, xp = i - py * PL::NH;
+        const T e = ek[PL::kx_of(xp) + PL::NH * iperm<N2>(py)];
+        A[i] = mk<T>(e * A[i].x, e * A[i].y);
+    }
+}
+
+template <typename T, int N1, int N2>
+__global__ void __launch_bounds__(256, 1) k2p_sweep(const SweepField<T> *fields, int t0, int t1)
+{
+    using K = Sweep2P<T, N1, N2>;
+    using PL = typename K::PL;
+    constexpr int NP = K::NP, NK = K::NK;
+    const SweepField<T> &f = fields[blockIdx.x];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cx<T> *A = (cx<T> *)smem_raw;
+    T *q = (T *)(A + K::PS);
+    T *q1 = q + NP;
+    T *eo1 = q1 + NP, *eo2 = eo1 + NP;
+    T *ek1 = eo2 + NP, *ek2 = ek1 + NK;
+    const T rn = (T)NP;
+    int blk, src, dst;
+    if (!step_slices(f, t0, blk, src, dst)) return;
+    {
+        const T *qs = src_slice(f, src, NP);
+        for (int i = threadIdx.x; i < NP; i += blockDim.x) q[i] = qs[i];
+    }
+    int cur = -1;
+    for (int t = t0; t < t1; t++) {
+        if (!step_slices(f, t, blk, src, dst)) break;
+        if (blk != cur) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < NP; i += blockDim.x) {
+                eo1[i] = f.eo1[blk][i];
+                eo2[i] = f.eo2[blk][i];
+            }
+            for (int i = threadIdx.x; i < NK; i += blockDim.x) {
+                ek1[i] = f.ek1[blk][i];
+                ek2[i] = f.ek2[blk][i];
+            }
+            cur = blk;
+        }
+        __syncthreads();
+        // full step
+        PL::pack(A, [&](int e) { return mk<T>(eo1[e] * q[e], eo1[e + 1] * q[e + 1]); });
+        PL::forward(A);
+        k2p_mul<T, N1, N2>(A, ek1);
+        PL::inverse(A);
+        PL::each_pair(A, [&](cx<T> &z, int e) {
+            const T a = eo1[e] * z.x / rn, b = eo1[e + 1] * z.y / rn;
+            q1[e] = a;
+            q1[e + 1] = b;
+            if (f.q1) {
+                f.q1[e] = a;
+                f.q1[e + 1] = b;
+            }
+        });
+        __syncthreads();
+        // two half steps
+        PL::pack(A, [&](int e) { return mk<T>(eo2[e] * q[e], eo2[e + 1] * q[e + 1]); });
+        PL::forward(A);
+        k2p_mul<T, N1, N2>(A, ek2);
+        PL::inverse(A);
+        PL::each_pair(A, [&](cx<T> &z, int e) {
+            const T a = eo1[e] * z.x / rn, b = eo1[e + 1] * z.y / rn;
+            if (f.h_out) {
+                f.h_out[e] = a;
+                f.h_out[e + 1] = b;
+            }
+            z = mk<T>(a, b);
+        });
+        PL::forward(A);
+        k2p_mul<T, N1, N2>(A, ek2);
+        PL::inverse(A);
+        T *out = dst_slice(f, dst, NP);
+        PL::each_pair(A, [&](cx<T> &z, int e) {
+            const T qa = eo2[e] * z.x / rn, qb = eo2[e + 1] * z.y / rn;
+            const T va = ((T)4 * qa - q1[e]) / (T)3, vb = ((T)4 * qb - q1[e + 1]) / (T)3;
+            q[e] = va;
+            q[e + 1] = vb;
+            out[e] = va;
+            out[e + 1] = vb;
+            if (f.q2_out) {
+                f.q2_out[e] = qa;
+                f.q2_out[e + 1] = qb;
+            }
+        });
+    }
+}
+
 }  // namespace pscfg

@@ -334,7 +334,8 @@ def test_large_plane_density_uses_line_passes():
     e.close()
 
 
-ROUGH_CASES = [(3, [64, 64, 64], "cubic", [3.7]), (3, [32, 32, 32], "cubic", [3.9]), (3, [16, 16, 16], "cubic", [3.9])]
+ROUGH_CASES = [(3, [64, 64, 64], "cubic", [3.7]), (3, [32, 32, 32], "cubic", [3.9]), (3, [16, 16, 16], "cubic", [3.9]),
+               (2, [64, 64], "hexagonal", [1.9])]
 
 
 @pytest.mark.parametrize("dim,ngrid,crystal,cell", ROUGH_CASES)
