@@ -72,20 +72,20 @@ __device__ __forceinline__ void zconv_cols(cx<T> *C, const T *__restrict__ ek, c
     stack_fft<32, 1, T, K::NCOL, K::NCOL, 0, 1, K::NCOL>(C, twz);
 }
 
+// One step (t) of field f by the cluster.  first: the cluster's first
+// step in this launch -- every CTA of the cluster must be running before
+// its shared memory is written by a peer, so each arrives on entry and
+// waits just before its first push.  Later steps need no such barrier: a
+// peer writes this CTA's column buffers only after the last cluster
+// barrier of the previous step, past which nothing reads them.
 template <typename T>
-__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(512, 1)
-    k3x_step32(const SweepField<T> *fields, PlaneGeom g, int t)
+__device__ __forceinline__ void cl32_step(cgx::cluster_group &cl, const SweepField<T> &f, const PlaneGeom &g,
+                                          int blk, int src, int dst, bool first)
 {
     using K = Cl32<T>;
     using PSk = PlaneStack<T, 32, 32, K::ZP>;
-    cgx::cluster_group cl = cgx::this_cluster();
     const int rank = (int)cl.block_rank();
-    const SweepField<T> &f = fields[blockIdx.x / K::CL];
-    int blk, src, dst;
-    if (!step_slices(f, t, blk, src, dst)) return;   // same for every CTA of the cluster
-    // every CTA of the cluster must be running before its shared memory is
-    // written by a peer: arrive now, wait just before the first push
-    asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
+    if (first) asm volatile("barrier.cluster.arrive.relaxed.aligned;\n" ::: "memory");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<T> *PA = (cx<T> *)smem_raw;
     cx<T> *PB = PA + K::ZP * K::PS;
@@ -106,7 +106,7 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(512, 1)
     PSk::pack(PB, [&](int e) { return eo2[e] * q[e]; });
     PSk::forward(PA, twM, twN2, twN1);
     PSk::forward(PB, twM, twN2, twN1);
-    asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+    if (first) asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
     push_planes<T>(cl, PA, CA, rank);
     push_planes<T>(cl, PB, CB, rank);
     cl.sync();
@@ -150,6 +150,34 @@ __global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(512, 1)
         const T q2 = eo2[e] * PSk::real_at(PB, e) / rn;
         out[e] = ((T)4 * q2 - Q1[e]) / (T)3;
         if (q2o) q2o[e] = q2;
+    }
+}
+
+
+template <typename T>
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(512, 1)
+    k3x_step32(const SweepField<T> *fields, PlaneGeom g, int t)
+{
+    cgx::cluster_group cl = cgx::this_cluster();
+    const SweepField<T> &f = fields[blockIdx.x / Cl32<T>::CL];
+    int blk, src, dst;
+    if (!step_slices(f, t, blk, src, dst)) return;   // same for every CTA of the cluster
+    cl32_step<T>(cl, f, g, blk, src, dst, true);
+}
+
+// Steps [t0, t1) of every field in one launch: a cluster walks its field's
+// contour, each CTA reading back the planes of q it wrote the step before.
+template <typename T>
+__global__ void __cluster_dims__(8, 1, 1) __launch_bounds__(512, 1)
+    k3x_sweep32(const SweepField<T> *fields, PlaneGeom g, int t0, int t1)
+{
+    cgx::cluster_group cl = cgx::this_cluster();
+    const SweepField<T> &f = fields[blockIdx.x / Cl32<T>::CL];
+    for (int t = t0; t < t1; t++) {
+        int blk, src, dst;
+        if (!step_slices(f, t, blk, src, dst)) break;   // same for every CTA of the cluster
+        cl32_step<T>(cl, f, g, blk, src, dst, t == t0);
+        __syncthreads();
     }
 }
 
