@@ -584,7 +584,7 @@ def c2_leg(args, rank, world, barrier, dev, local_rank):
            "roofline": roofline(wl.systems[0], prof, nsteps, peak, peak_kind, 8,
                                 "MDE step: k3r_final_fwd + k3s_zconv x2 + k3r_inv_mid (kernels3c.cuh, 32^3)"),
            "sweep_steps_per_s_fp64": nsteps / (prof["sweep_ms"] / 1e3),
-           "planes_per_cta": e.sweep_planes(2 * len(wl.systems), e.steps_per_density // (2 * len(wl.systems)))}
+           "planes_per_cta": e.sweep_planes(2 * len(wl.systems))}
     if not args.no_solve:
         out.update(solve_legs(e, wl, stream, barrier, dev, world))
     e.close()

@@ -364,12 +364,13 @@ long pscfg_steps_per_density(const pscfg_engine *e);
 long pscfg_launch_count(const pscfg_engine *e);
 
 /* Planes per CTA that the 3-D register sweep of this engine's grid uses for
- * a sweep of n_fields fields over n_steps steps in FP64 (fp32 != 0: FP32),
- * as measured by the engine (one timed trial sweep per candidate before the
- * first real sweep, the fastest kept for the process); -1 when the
- * one-launch thread-block-cluster step (32^3, FP64) was the fastest; 0
- * while undecided or for grids without the register sweep (16^3, 32^3). */
-int pscfg_sweep_planes(const pscfg_engine *e, int n_fields, int n_steps, int fp32);
+ * a sweep of n_fields fields in FP64 (fp32 != 0: FP32), as measured by the
+ * engine (one timed trial sweep per candidate before the first real sweep
+ * of each class of field counts -- up to the same power of two -- the
+ * fastest kept for the process); -1 when the thread-block-cluster sweep
+ * (32^3, FP64) was the fastest; 0 while undecided or for grids without the
+ * register sweep (16^3, 32^3). */
+int pscfg_sweep_planes(const pscfg_engine *e, int n_fields, int fp32);
 
 #ifdef __cplusplus
 }

@@ -723,7 +723,7 @@ static void step3r(Engine &E, const SweepField<T> *dfl, int nf, int t)
 // sweep in 61 ms with one plane per CTA against 107 ms with four, while 64
 // instances are fastest with four (465 ms against 473 with two).
 // Planes per CTA of the register sweep (pmax, pmax/2, ..., 1), measured.
-// The first sweep of each (grid, precision, field count, step count) is
+// The first sweep of each (grid, precision, field-count class) is
 // preceded by one trial sweep per candidate, timed with CUDA events on the
 // engine stream (a graph replay, after its capture); the fastest is kept
 // for the process (all engines) and the real sweep runs with it.  A trial
@@ -744,22 +744,26 @@ static int planes_rule(int nf, int n3, int pmax)
     return p;
 }
 
-static long planes_key(int n3, int tsize, int nf, int nsteps)
+// the choice is shared by field counts up to the same power of two, so that
+// a batch whose running instances dwindle measures a handful of times
+static long planes_key(int n3, int tsize, int nf)
 {
-    return (((long)n3 * 16 + tsize) * 100000 + nf) * 100000 + nsteps;
+    long b = 1;
+    while (b < nf) b *= 2;
+    return ((long)n3 * 16 + tsize) * 100000 + b;
 }
 
 // trial(p, e0, e1) enqueues one sweep with p planes per CTA, recording e0
 // just before its first launch and e1 after its last.
 template <typename Trial>
-static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, int nsteps, Trial trial, bool cluster = false)
+static int sweep_planes(Engine &E, int nf, int n3, int pmax, int tsize, Trial trial, bool cluster = false)
 {
     if (E.planes > 0) {
         for (int p = pmax; p >= 1; p /= 2)
             if (E.planes == p) return p;
     }
     if (E.planes < 0 && cluster) return 0;   // PSCFG_PLANES=-1: the cluster sweep
-    const long key = planes_key(n3, tsize, nf, nsteps);
+    const long key = planes_key(n3, tsize, nf);
     {
         std::lock_guard<std::mutex> lk(g_planes_mu);
         auto it = g_planes_best.find(key);
@@ -899,7 +903,7 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int
             default: cluster(e0, e1); break;
             }
         };
-        go(sweep_planes(E, nf, 32, 4, (int)sizeof(T), ns_max - t0, go, sizeof(T) == 8), nullptr, nullptr);
+        go(sweep_planes(E, nf, 32, 4, (int)sizeof(T), go, sizeof(T) == 8), nullptr, nullptr);
         return true;
     }
     if (a == 16 && b == 16 && c == 16) {
@@ -912,7 +916,7 @@ static bool sweep3r(Engine &E, const SweepField<T> *dfl, int nf, int ns_max, int
             default: run(N(), std::integral_constant<int, 1>(), e0, e1); break;
             }
         };
-        go(sweep_planes(E, nf, 16, 8, (int)sizeof(T), ns_max - t0, go), nullptr, nullptr);
+        go(sweep_planes(E, nf, 16, 8, (int)sizeof(T), go), nullptr, nullptr);
         return true;
     }
     return false;
@@ -4661,12 +4665,12 @@ long pscfg_steps_per_density(const pscfg_engine *e)
 
 long pscfg_launch_count(const pscfg_engine *e) { return e ? e->E.launches : 0; }
 
-int pscfg_sweep_planes(const pscfg_engine *e, int n_fields, int n_steps, int fp32)
+int pscfg_sweep_planes(const pscfg_engine *e, int n_fields, int fp32)
 {
     if (!e || e->E.dim != 3 || e->E.n[0] != e->E.n[1] || e->E.n[1] != e->E.n[2]) return 0;
     const int n3 = e->E.n[2];
     if (n3 != 16 && n3 != 32) return 0;
-    const long key = planes_key(n3, fp32 ? 4 : 8, n_fields, n_steps);
+    const long key = planes_key(n3, fp32 ? 4 : 8, n_fields);
     std::lock_guard<std::mutex> lk(g_planes_mu);
     auto it = g_planes_best.find(key);
     if (it == g_planes_best.end()) return 0;

@@ -125,7 +125,7 @@ SIGNATURES = {
     "pscfg_density_adjoint_device": (C.c_int, [_vp, _vp, _dp, _vp]),
     "pscfg_steps_per_density": (C.c_long, [_vp]),
     "pscfg_launch_count": (C.c_long, [_vp]),
-    "pscfg_sweep_planes": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
+    "pscfg_sweep_planes": (C.c_int, [_vp, C.c_int, C.c_int]),
 }
 
 _lib = None
@@ -433,7 +433,7 @@ class Engine:
     def launch_count(self) -> int:
         return int(self.lib.pscfg_launch_count(self._h))
 
-    def sweep_planes(self, n_fields: int, n_steps: int, fp32: bool = False) -> int:
-        """Planes per CTA the measured tuner chose for the 3-D register sweep
-        (0 while undecided)."""
-        return int(self.lib.pscfg_sweep_planes(self._h, n_fields, n_steps, 1 if fp32 else 0))
+    def sweep_planes(self, n_fields: int, fp32: bool = False) -> int:
+        """Planes per CTA the measured choice gives the 3-D register sweep of
+        n_fields fields (-1: the cluster sweep; 0 while undecided)."""
+        return int(self.lib.pscfg_sweep_planes(self._h, n_fields, 1 if fp32 else 0))

@@ -366,15 +366,14 @@ def test_rough_fields_all_kernel_paths(monkeypatch, dim, ngrid, crystal, cell, p
 
 def test_measured_planes_per_cta():
     """The register sweep's planes per CTA are measured before the first
-    sweep of each (grid, precision, field count, step count) -- one timed
+    sweep of each (grid, precision, class of field counts) -- one timed
     trial sweep per candidate -- and every density comes from the chosen
     count: repeated calls are bit-identical."""
     ss = [diblock(3, [32, 32, 32], "cubic", [3.9], fA=0.25 + 0.02 * i, chiN=20.0, ds=0.02) for i in range(3)]
     w = np.stack([omega_guess(s, 40 + i, 2.0) for i, s in enumerate(ss)])
     e = Engine(ss, FP64)
-    nsteps = e.steps_per_density // (2 * len(ss))
     outs = [e.density(w)[0] for _ in range(5)]
-    p = e.sweep_planes(2 * len(ss), nsteps)
+    p = e.sweep_planes(2 * len(ss))
     e.close()
     assert p in (1, 2, 4, -1), p                                     # -1: the cluster step
     for o in outs[1:]:
