@@ -16,6 +16,7 @@ pytestmark = pytest.mark.gpu
 CASES = [
     (1, [32], "lamellar", [1.7], 0.005),
     (2, [24, 24], "hexagonal", [1.9], 0.01),
+    (2, [64, 64], "hexagonal", [1.9], 0.01),
     (3, [16, 16, 16], "cubic", [3.9], 0.01),
     (3, [32, 32, 32], "cubic", [3.9], 0.01),
     (3, [64, 64, 64], "cubic", [3.7], 0.005),

@@ -100,8 +100,12 @@ def test_batched_uneven_instances_fp64():
         assert abs(f[i] - fr) < 1e-11
 
 
-def test_density_fp32_close():
-    s = diblock(3, [16, 16, 16], "cubic", [3.9], fA=0.3)
+@pytest.mark.parametrize("dim,ngrid,crystal,cell", [(3, [16, 16, 16], "cubic", [3.9]),
+                                                   (2, [64, 64], "hexagonal", [1.9])])
+def test_density_fp32_close(dim, ngrid, crystal, cell):
+    """FP32 propagation (FP64 sums) against the FP64 oracle; 64 x 64 runs the
+    whole-sweep 2-D kernel in single precision."""
+    s = diblock(dim, ngrid, crystal, cell, fA=0.3)
     w = omega_guess(s, 3, 2.0)
     o = O.Oracle(s)
     rho_ref, q_ref = o.density(w)
