@@ -652,6 +652,14 @@ static void create_engine(Engine &E, const pscfg_system *sys, int n_inst, int pr
 // Density
 // ---------------------------------------------------------------------
 static int red_ctas(long n) { return (int)std::min<long>(std::max<long>((n + 255) / 256, 1), 64); }
+// CTAs per job of a batched reduction over n points with njobs jobs: 64 per
+// job for a batch, up to 4 per SM when a few jobs (one large instance) would
+// otherwise leave most SMs idle and the loads without parallelism
+static int red_ctas(long n, int njobs)
+{
+    const long cap = std::max<long>(64, 592 / std::max(njobs, 1));
+    return (int)std::min<long>(std::max<long>((n + 255) / 256, 1), cap);
+}
 
 // One 3-D MDE step of every field with compile-time-shaped kernels.
 template <typename T, int N1, int N2, int N3, int PPC>
@@ -1347,7 +1355,7 @@ static void run_contour(Engine &E, const std::vector<int> &act)
             qout.push_back(I.Qdev + c);
         }
     }
-    const int nct = red_ctas(E.nr);
+    const int nct = red_ctas(E.nr, (int)qp.size());
     size_t off = 0;
     if (!qp.empty()) {
         const T **dqp = (const T **)E.upload(qp, 0);
@@ -2136,7 +2144,7 @@ static void fe_spectral(Engine &E, const std::vector<int> &which, double *hout, 
         CK(cudaMalloc(&E.fe_spec, per * chunk));
         E.fe_spec_bytes = per * chunk;
     }
-    const int nct = red_ctas(E.nk);
+    const int nct = red_ctas(E.nk, (int)std::min<size_t>(chunk, which.size()));
     for (size_t c0 = 0; c0 < which.size(); c0 += chunk) {
         const int cn = (int)std::min<size_t>(chunk, which.size() - c0);
         std::vector<const double *> src;
@@ -2232,7 +2240,7 @@ static void free_energy_all(Engine &E, const std::vector<int> &act, std::vector<
             fj.push_back(j);
         }
         FieldJob *dj = E.upload(fj, 0);
-        const int nct = red_ctas(E.nr);
+        const int nct = red_ctas(E.nr, (int)fj.size());
         double *part = E.part((size_t)nct * fj.size());
         k_fe_partial<<<dim3(nct, (unsigned)fj.size()), 256, 0, E.st>>>(dj, E.nr, part);
         E.launched();
@@ -2460,7 +2468,6 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
     const long fl = (long)E.M * E.nr;
     const int ninst = (int)E.inst.size();
     const double large = 100.0;
-    const int nct = red_ctas(E.nr);
     std::vector<AmState> &st = R.st;
     std::vector<double> hsmall;
     int remaining = 0;
@@ -2471,6 +2478,7 @@ static int am_iterate(Engine &E, AmRun &R, int iters)
         remaining = (int)act.size();
         if (act.empty()) break;
         const int na = (int)act.size();
+        const int nct = red_ctas(E.nr, na);
         for (int i : act) st[i].itr++;
 
         // density, stress, free-energy terms and the Anderson sums are all
@@ -2862,7 +2870,7 @@ static void amg_iteration(Engine &E, AmRun &R, const std::vector<int> &act)
     const int na = (int)act.size();
     const int S = prm.n_hist + 1;
     const long fl = (long)E.M * E.nr;
-    const int nct = red_ctas(E.nr);
+    const int nct = red_ctas(E.nr, na);
     const double large = 100.0;
     const unsigned g1 = (unsigned)((na + 127) / 128);
     density_all(E, act, false);
