@@ -1795,7 +1795,7 @@ static void density_finish(Engine &E, const std::vector<int> &act);
 // region of the descriptor scratch).
 static void copy_list(Engine &E, const std::vector<CopyJob> &jobs, long maxn)
 {
-    const unsigned gx = (unsigned)std::max<long>(1, std::min<long>((maxn + 255) / 256, 64));
+    const unsigned gx = (unsigned)red_ctas(maxn, (int)std::min<size_t>(jobs.size(), 65535));
     for (size_t j0 = 0; j0 < jobs.size(); j0 += 65535) {
         const size_t cnt = std::min<size_t>(65535, jobs.size() - j0);
         std::vector<CopyJob> part(jobs.begin() + j0, jobs.begin() + j0 + cnt);
@@ -2921,7 +2921,7 @@ static void amg_iteration(Engine &E, AmRun &R, const std::vector<int> &act)
         k_symmetrize<<<grid, 128, 0, E.st>>>(R.g_sym, E.nr);
         E.launched();
     }
-    const unsigned gx = (unsigned)std::max<long>(1, std::min<long>((fl + 255) / 256, 64));
+    const unsigned gx = (unsigned)red_ctas(fl, na);
     k_copy_list<<<dim3(gx, na), 256, 0, E.st>>>(R.g_hc);
     E.launched();
     if (prm.domain) {
