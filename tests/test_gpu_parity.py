@@ -405,3 +405,33 @@ def test_cluster_sweep_matches_oracle(monkeypatch):
     rho2, _ = e.density(np.stack([w, w]))
     e.close()
     assert rel_err(rho2, rho) < 1e-13
+
+
+@pytest.mark.parametrize("dim,ngrid,crystal,cell", [(2, [12, 12], "square", [1.8]),
+                                                   (3, [16, 16, 16], "cubic", [2.2])])
+def test_system_at_the_limits(dim, ngrid, crystal, cell):
+    """Every array bound of the C ABI at its maximum (include/pscf_gpu.h:
+    4 monomers, 4 chains, an 8-block chain, 4 solvents): density, Q, Q_s,
+    stress, free energy and mu against the oracle."""
+    from pscf_b200.system import Chain, Solvent, System
+    chi = np.array([[0, 12.0, 18.0, 9.0], [12.0, 0, 14.0, 20.0], [18.0, 14.0, 0, 11.0], [9.0, 20.0, 11.0, 0]])
+    chains = [Chain([0, 1, 2, 3, 0, 1, 2, 3], [0.15, 0.1, 0.2, 0.1, 0.1, 0.15, 0.1, 0.1], phi=0.5),
+              Chain([1], [0.4], phi=0.15), Chain([2, 3], [0.3, 0.3], phi=0.15), Chain([3, 0, 2], [0.2, 0.3, 0.25], phi=0.1)]
+    solvents = [Solvent(monomer=m, size=0.05 + 0.05 * m, phi=0.025) for m in range(4)]
+    s = System(dim=dim, ngrid=ngrid, crystal_system=crystal, cell_param=cell, kuhn=[1.0, 1.1, 0.9, 1.2], chi=chi,
+               chains=chains, solvents=solvents, ds=0.02)
+    w = omega_guess(s, 23, 1.5)
+    o = O.Oracle(s)
+    rho_ref, q_ref = o.density(w)
+    st_ref = o.stress()
+    f_ref, p_ref = o.free_energy(w, rho_ref)
+    mu_ref, _ = o.mu_phi()
+    e = Engine([s], FP64)
+    rho, q = e.density(w[None])
+    assert rel_err(rho[0], rho_ref) < 1e-12
+    assert rel_err(q[0, :len(q_ref)], q_ref) < 1e-12
+    np.testing.assert_allclose(e.scf_stress()[0, :1], st_ref, rtol=1e-10, atol=1e-12)
+    f, p, mu = e.free_energy()
+    assert abs(f[0] - f_ref) < 1e-11 and abs(p[0] - p_ref) < 1e-11
+    np.testing.assert_allclose(mu[0, :4], mu_ref[:4], rtol=1e-12)
+    e.close()
