@@ -435,3 +435,28 @@ def test_system_at_the_limits(dim, ngrid, crystal, cell):
     assert abs(f[0] - f_ref) < 1e-11 and abs(p[0] - p_ref) < 1e-11
     np.testing.assert_allclose(mu[0, :4], mu_ref[:4], rtol=1e-12)
     e.close()
+
+
+def test_batch_with_a_solvent_only_instance():
+    """Ragged batch: an instance without chains (two solvents) next to a
+    diblock + solvent instance in one engine; densities, stress and free
+    energy against the oracle (the chainless instance has no propagators,
+    no stress and no sweep fields)."""
+    from pscf_b200.system import Chain, Solvent, System
+    kw = dict(dim=2, ngrid=[12, 12], crystal_system="square", cell_param=[1.8], kuhn=[1.0, 1.0],
+              chi=[[0, 2.0], [2.0, 0]], ds=0.02)
+    a = System(chains=[], solvents=[Solvent(0, 1.0, phi=0.6), Solvent(1, 0.5, phi=0.4)], **kw)
+    b = System(chains=[Chain([0, 1], [0.4, 0.6], phi=0.8)], solvents=[Solvent(1, 0.3, phi=0.2)], **kw)
+    ws = [omega_guess(a, 3, 0.5), omega_guess(b, 4, 1.0)]
+    e = Engine([a, b], FP64)
+    rho, q = e.density(np.stack(ws))
+    st = e.scf_stress()
+    f, p, _ = e.free_energy()
+    for i, s in enumerate((a, b)):
+        o = O.Oracle(s)
+        rho_ref, q_ref = o.density(ws[i])
+        assert rel_err(rho[i], rho_ref) < 1e-12, i
+        f_ref, p_ref = o.free_energy(ws[i], rho_ref)
+        assert abs(f[i] - f_ref) < 1e-11 and abs(p[i] - p_ref) < 1e-11, i
+        np.testing.assert_allclose(st[i, :1], o.stress(), rtol=1e-10, atol=1e-13)
+    e.close()
