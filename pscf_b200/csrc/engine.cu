@@ -2814,6 +2814,7 @@ static void amg_setup(Engine &E, AmRun &R, const std::vector<int> &act)
     for (size_t k = 0; k < pos_plain.size(); k++) tidx[pos_plain[k]] = (int)k;
     for (size_t k = 0; k < pos_w.size(); k++) tidx[pos_w[k]] = (int)(pos_plain.size() + k);
     R.g_maxorb = 0;
+    E.amg_G.assign(E.inst.size(), nullptr);
     for (int k = 0; k < na; k++) {
         Inst &I = E.inst[act[k]];
         std::memset(&aj[k], 0, sizeof(AmJob));
@@ -2835,7 +2836,6 @@ static void amg_setup(Engine &E, AmRun &R, const std::vector<int> &act)
         g.kweight = I.kweight;
         g.wdg0 = I.kweight ? I.wdg0 : nullptr;
         g.gate = &R.g_st[act[k]].mixed;
-        E.amg_G.resize(E.inst.size(), nullptr);
         E.amg_G[act[k]] = (const double *)((const char *)(R.g_geo + k) + offsetof(GeomJob, G));
         SymJob &y = sym[k];
         std::memset(&y, 0, sizeof(y));
