@@ -36,6 +36,7 @@ class Increments:
     symmetric matrix."""
     kuhn: Optional[Sequence[float]] = None
     chi: Optional[np.ndarray] = None
+    temperature: Optional[float] = None     # interaction_type 'chi_T': d(temperature)
     block_length: Optional[Sequence[Sequence[float]]] = None
     phi_chain: Optional[Sequence[float]] = None
     mu_chain: Optional[Sequence[float]] = None
@@ -52,7 +53,12 @@ def increment_parameters(system: System, inc: Increments, step: float, domain: b
     s = copy.deepcopy(system)
     if inc.kuhn is not None:
         s.kuhn = [k + step * d for k, d in zip(s.kuhn, inc.kuhn)]
-    if inc.chi is not None:
+    if s.temperature is not None:
+        # chi_T: the temperature moves and chi follows (chi_A / T + chi_B)
+        if inc.temperature is not None:
+            s.temperature = s.temperature + step * inc.temperature
+        s.chi = s.chi_A / s.temperature + s.chi_B
+    elif inc.chi is not None:
         s.chi = s.chi + step * np.asarray(inc.chi, dtype=np.float64)
     for j, c in enumerate(s.chains):
         if inc.block_length is not None:
@@ -188,8 +194,12 @@ def write_out(path: str, system: System, group_name: str, result: Dict, iterate:
             L += [_lab("mu_chain")] + [_real(c.mu) for c in s.chains]
         if s.solvents:
             L += [_lab("mu_solvent")] + [_real(v.mu) for v in s.solvents]
-    L += ["", _lab("INTERACTION"), _lab("interaction_type"), _str("chi"), _lab("chi")]
-    L += ["".join(_real(s.chi[k, j]) for j in range(k)) for k in range(1, s.n_monomer)]
+    lower = lambda m: ["".join(_real(m[k, j]) for j in range(k)) for k in range(1, s.n_monomer)]
+    if s.temperature is None:
+        L += ["", _lab("INTERACTION"), _lab("interaction_type"), _str("chi"), _lab("chi")] + lower(s.chi)
+    else:
+        L += ["", _lab("INTERACTION"), _lab("interaction_type"), _str("chi_T"), _lab("chi_A")] + lower(s.chi_A)
+        L += [_lab("chi_B")] + lower(s.chi_B) + [_lab("temperature"), _real(s.temperature)]
     L += ["", _lab("UNIT_CELL"), _lab("dim"), _int(s.dim), _lab("crystal_system"), _str(s.crystal_system),
           _lab("N_cell_param"), _int(len(s.cell_param)), _lab("cell_param"),
           "".join(_real(c) for c in s.cell_param)]
@@ -220,6 +230,8 @@ def write_out(path: str, system: System, group_name: str, result: Dict, iterate:
         if s.solvents:
             L += [_lab("phi_solvent")] + [_real(v.phi) for v in s.solvents]
     L += [_lab("stress"), "".join(_real(x) for x in r["stress"][:len(s.cell_param)])]
+    if s.temperature is not None:                       # chi printed when it follows T
+        L += [_lab("chi")] + lower(s.chi)
     st = stats
     L += ["", _lab("STATISTICS"), _lab("N_star"), _int(st["n_star"]), _lab("final_error"),
           _real(st["final_error"]), _lab("iterations"), _int(st["iterations"]), _lab("basis_time"),

@@ -187,8 +187,17 @@ class System:
     ds: float
     solvents: List[Solvent] = dataclasses.field(default_factory=list)
     ensemble: int = 0
+    # interaction_type 'chi_T' (src/chemistry_mod.f90): chi = chi_A / T + chi_B,
+    # with chi computed from these when temperature is set
+    chi_A: Optional[np.ndarray] = None
+    chi_B: Optional[np.ndarray] = None
+    temperature: Optional[float] = None
 
     def __post_init__(self):
+        if self.temperature is not None:
+            self.chi_A = np.asarray(self.chi_A, dtype=np.float64)
+            self.chi_B = np.asarray(self.chi_B, dtype=np.float64)
+            self.chi = self.chi_A / float(self.temperature) + self.chi_B
         self.chi = np.asarray(self.chi, dtype=np.float64)
         self.cell_param = [float(c) for c in self.cell_param]
         if not (1 <= self.dim <= 3):

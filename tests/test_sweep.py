@@ -160,3 +160,29 @@ def test_sweep_schedule_outputs_and_backtracking(tmp_path):
     pts = S.run_sweep(s0, np.zeros((2, 16)), inc, 3.0, flaky, domain=False)
     assert [round(c[0], 8) for c in calls] == [0.40, 0.399, 0.39, 0.38, 0.385, 0.38, 0.375, 0.37]
     assert [round(p.s, 6) for p in pts] == [0.0, 1.0, 2.0, 3.0]
+
+
+def test_temperature_interaction_sweep_and_summary(tmp_path):
+    """interaction_type 'chi_T' (chi = chi_A / T + chi_B): a temperature
+    increment moves chi with it (increment_parameters,
+    src/sweep_mod.f90:418-421), and the summary prints chi_A, chi_B and the
+    temperature under INTERACTION and the resulting chi under THERMO
+    (output_interaction, src/chemistry_mod.f90:1274-1326; output_summary,
+    src/pscf.fp.f90:1157-1159)."""
+    chi_A = np.array([[0.0, 3000.0], [3000.0, 0.0]])
+    chi_B = np.array([[0.0, -2.0], [-2.0, 0.0]])
+    s = System(dim=1, ngrid=[16], crystal_system="lamellar", cell_param=[1.7], kuhn=[1.0, 1.0], chi=np.zeros((2, 2)),
+               chains=[Chain([0, 1], [0.5, 0.5])], ds=0.01, chi_A=chi_A, chi_B=chi_B, temperature=200.0)
+    assert abs(s.chi[0, 1] - (3000.0 / 200.0 - 2.0)) < 1e-14
+    t = S.increment_parameters(s, S.Increments(temperature=-10.0), 0.5, domain=True)
+    assert t.temperature == 195.0 and abs(t.chi[0, 1] - (3000.0 / 195.0 - 2.0)) < 1e-13
+    assert s.temperature == 200.0
+    res = dict(f_helmholtz=2.0, pressure=3.0, stress=[1e-12], mu_chain=[4.0])
+    it = dict(max_itr=10, error_max=1e-8, domain=True, itr_algo="AM", N_hist=20)
+    st = dict(n_star=9, final_error=1e-9, iterations=5)
+    S.write_out(str(tmp_path / "t.out"), t, "-1", res, it, st)
+    lines = open(tmp_path / "t.out").read().splitlines()
+    d = S.read_out(str(tmp_path / "t.out"))
+    assert d["interaction_type"] == ["chi_T"] and d["chi_A"] == [3000.0] and d["chi_B"] == [-2.0]
+    assert d["temperature"] == [195.0] and abs(d["chi"][0] - t.chi[1, 0]) < 1e-9
+    assert lines.index("chi                 ") > lines.index("THERMO              ")
