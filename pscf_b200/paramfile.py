@@ -1,0 +1,272 @@
+"""The reference's parameter files, read and run on the engine.
+
+A parameter file (doc/user-man/param.rst; read by the main program,
+src/pscf.fp.f90:200-720) is a version line and a sequence of sections, each
+a name on its own line followed by `label` / value lines in the io_mod
+layout -- the same layout as the first part of an output summary:
+
+  MONOMERS, CHAINS, SOLVENTS, COMPOSITION, INTERACTION, UNIT_CELL,
+  DISCRETIZATION, BASIS  -- the system;
+  ITERATE                -- solve from a basis-format omega file;
+  SWEEP                  -- continuation to s_max with d_<name> increments,
+                            ended by end_increments;
+  FIELD_TO_RGRID, RGRID_TO_FIELD, RHO_TO_OMEGA -- field conversions;
+  FINISH.
+
+read_param parses a file into its sections; system_of builds the System;
+run_param executes the commands in order with the engine (Anderson mixing,
+or Newton with the batched Jacobian for itr_algo 'NR'), writing the same
+files as the reference: <output_prefix>out / omega / rho for ITERATE,
+<output_prefix>0., 1., ... for a SWEEP.  RESPONSE, RESCALE, KGRID_TO_RGRID,
+OUTPUT_WAVES and OUTPUT_GROUP are not run here (pscf_b200.response covers
+the response calculation from Python).
+"""
+from __future__ import annotations
+
+import os
+import time
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+from .system import Chain, Solvent, System
+
+SYSTEM_SECTIONS = ("MONOMERS", "CHAINS", "SOLVENTS", "COMPOSITION", "INTERACTION", "UNIT_CELL", "DISCRETIZATION",
+                   "BASIS")
+COMMANDS = ("ITERATE", "SWEEP", "RESPONSE", "FIELD_TO_RGRID", "RGRID_TO_FIELD", "KGRID_TO_RGRID", "RHO_TO_OMEGA",
+            "RESCALE", "OUTPUT_WAVES", "OUTPUT_GROUP", "FINISH")
+
+
+def _values(line: str):
+    """The values of a data line, or None for a label line."""
+    t = line.strip()
+    toks = t.split()
+    try:
+        return [float(x.replace("D", "E").replace("d", "e")) for x in toks]
+    except ValueError:
+        pass
+    if t.startswith("'") or t in ("T", "F"):
+        return [t.strip("'")]
+    return None
+
+
+def read_param(path: str) -> List[Tuple[str, Dict[str, List]]]:
+    """Sections of a parameter file in file order: (name, {label: values});
+    parsing stops at FINISH."""
+    lines = open(path).read().splitlines()
+    out: List[Tuple[str, Dict[str, List]]] = []
+    cur = None
+    key = None
+    for raw in lines[1:]:
+        t = raw.strip()
+        if not t:
+            continue
+        if t in SYSTEM_SECTIONS or t in COMMANDS:
+            cur = (t, {})
+            out.append(cur)
+            key = None
+            if t == "FINISH":
+                break
+            continue
+        if t == "end_increments":
+            key = None
+            continue
+        vals = _values(t)
+        if vals is None:
+            key = t
+            if cur is None:
+                raise ValueError(f"{path}: {t!r} before the first section")
+            cur[1][key] = []
+        elif key is not None:
+            cur[1][key] += vals
+        else:
+            raise ValueError(f"{path}: values {t!r} without a label")
+    return out
+
+
+def _sections(param) -> Dict[str, Dict[str, List]]:
+    d: Dict[str, Dict[str, List]] = {}
+    for name, body in param:
+        if name in SYSTEM_SECTIONS:
+            d.setdefault(name, {}).update(body)
+    return d
+
+
+def _lower(vals, M):
+    m = np.zeros((M, M))
+    k = 0
+    for a in range(1, M):
+        for b in range(a):
+            m[a, b] = m[b, a] = vals[k]
+            k += 1
+    return m
+
+
+def system_of(param) -> Tuple[System, str]:
+    """(System, group name) of the system sections (monomer indices made
+    0-based)."""
+    d = _sections(param)
+    mon, ch, comp, inter = d["MONOMERS"], d.get("CHAINS", {}), d["COMPOSITION"], d["INTERACTION"]
+    cell, disc = d["UNIT_CELL"], d["DISCRETIZATION"]
+    M = int(mon["N_monomer"][0])
+    ens = int(comp["ensemble"][0])
+    chains = []
+    nch = int(ch.get("N_chain", [0])[0])
+    if nch:
+        nblk = [int(x) for x in ch["N_block"]]
+        bm = [int(x) - 1 for x in ch["block_monomer"]]
+        bl = ch["block_length"]
+        k = 0
+        for j in range(nch):
+            c = Chain(bm[k:k + nblk[j]], bl[k:k + nblk[j]])
+            if ens == 0:
+                c.phi = comp["phi_chain"][j]
+            else:
+                c.mu = comp["mu_chain"][j]
+            chains.append(c)
+            k += nblk[j]
+    solvents = []
+    sv = d.get("SOLVENTS", {})
+    for j in range(int(sv.get("N_solvent", [0])[0])):
+        v = Solvent(monomer=int(sv["solvent_monomer"][j]) - 1, size=sv["solvent_size"][j])
+        if ens == 0:
+            v.phi = comp["phi_solvent"][j]
+        else:
+            v.mu = comp["mu_solvent"][j]
+        solvents.append(v)
+    kw = {}
+    itype = inter["interaction_type"][0]
+    if itype == "chi":
+        chi = _lower(inter["chi"], M)
+    elif itype == "chi_T":
+        kw = dict(chi_A=_lower(inter["chi_A"], M), chi_B=_lower(inter["chi_B"], M),
+                  temperature=inter["temperature"][0])
+        chi = np.zeros((M, M))
+    else:
+        raise ValueError(f"interaction_type {itype!r}")
+    dim = int(cell["dim"][0])
+    s = System(dim=dim, ngrid=[int(x) for x in disc["ngrid"]], crystal_system=cell["crystal_system"][0],
+               cell_param=cell["cell_param"], kuhn=mon["kuhn"], chi=chi, chains=chains, ds=disc["chain_step"][0],
+               solvents=solvents, ensemble=ens, **kw)
+    return s, d.get("BASIS", {}).get("group_name", [""])[0]
+
+
+def increments_of(body: Dict[str, List], system: System):
+    """(s_max, Increments) of a SWEEP section."""
+    from .sweep import Increments
+    M = system.n_monomer
+    inc = Increments()
+    for key, vals in body.items():
+        if key == "s_max":
+            continue
+        if not key.startswith("d_"):
+            raise ValueError(f"SWEEP: unknown entry {key!r}")
+        name = key[2:]
+        if name == "chi":
+            inc.chi = _lower(vals, M)
+        elif name == "block_length":
+            rows, k = [], 0
+            for c in system.chains:
+                n = len(c.block_length)
+                rows.append(list(vals[k:k + n]))
+                k += n
+            inc.block_length = rows
+        elif name in ("temperature",):
+            inc.temperature = vals[0]
+        elif name in ("kuhn", "phi_chain", "mu_chain", "phi_solvent", "mu_solvent", "solvent_size", "cell_param"):
+            setattr(inc, name, list(vals))
+        else:
+            raise ValueError(f"SWEEP: no increments of {name!r}")
+    return body["s_max"][0], inc
+
+
+def _iterate_params(body):
+    it = dict(input_filename=body["input_filename"][0], output_prefix=body["output_prefix"][0],
+              max_itr=int(body["max_itr"][0]), error_max=body["error_max"][0], domain=body["domain"][0] == "T",
+              itr_algo=body["itr_algo"][0])
+    if it["itr_algo"] == "NR":
+        it["N_cut"] = int(body.get("N_cut", [0])[0])
+    elif it["itr_algo"] == "AM":
+        it["N_hist"] = int(body.get("N_hist", [20])[0])
+    else:
+        raise ValueError(f"itr_algo {it['itr_algo']!r}")
+    return it
+
+
+def _solver(it, group):
+    from .sweep import am_solver, nr_solver
+    if it["itr_algo"] == "AM":
+        return am_solver(group or None, error_max=it["error_max"], max_itr=it["max_itr"], n_hist=it["N_hist"],
+                         domain=it["domain"])
+    return nr_solver(group, n_cut=it["N_cut"] or None, error_max=it["error_max"], max_itr=it["max_itr"],
+                     domain=it["domain"])
+
+
+def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
+    """Run the commands of a parameter file; file names are relative to
+    workdir (default: the file's directory).  Returns the last system, the
+    converged fields and results (ITERATE) and the sweep points (SWEEP)."""
+    from . import field_io as F
+    from .basis import StarBasis
+    from .sweep import run_sweep, write_out
+    param = read_param(path)
+    wd = workdir or os.path.dirname(os.path.abspath(path))
+    at = lambda name: name if os.path.isabs(name) else os.path.join(wd, name)
+    system, group = system_of(param)
+    state: Dict = {"system": system}
+    names = [n for n, _ in param]
+    for k, (name, body) in enumerate(param):
+        if name in SYSTEM_SECTIONS:
+            continue
+        if name == "FINISH":
+            break
+        if name == "ITERATE":
+            it = _iterate_params(body)
+            _, w0 = F.read_field(at(it["input_filename"]), system, group)
+            t0 = time.perf_counter()
+            w, rho, r = _solver(it, group)(system, w0)
+            dt = time.perf_counter() - t0
+            if it["domain"]:
+                system.cell_param = list(r["cell_param"])
+            nxt = names[k + 1] if k + 1 < len(names) else ""
+            prefix = at(it["output_prefix"]) + ("0." if nxt == "SWEEP" else "")
+            d = os.path.dirname(prefix)
+            if d:
+                os.makedirs(d, exist_ok=True)
+            n_star = len(F.FieldBasis(group, system).stars) if group else 0
+            stats = dict(n_star=n_star, final_error=r["error"], iterations=r["itr"], basis_time=0.0, scf_time=dt)
+            write_out(prefix + "out", system, group, r, it, stats)
+            if group:
+                F.write_field(prefix + "omega", w, system, group)
+                F.write_field(prefix + "rho", rho, system, group)
+            log(f"ITERATE: {'converged' if r['converged'] else 'not converged'} after {r['itr']} iterations")
+            state.update(iterate=it, omega=w, rho=rho, result=r, n_star=n_star)
+        elif name == "SWEEP":
+            if "result" not in state or not state["result"]["converged"]:
+                raise RuntimeError("SWEEP needs a converged ITERATE before it")
+            it = state["iterate"]
+            s_max, inc = increments_of(body, system)
+            pts = run_sweep(system, state["omega"], inc, s_max, _solver(it, group), it["domain"],
+                            out_prefix=at(it["output_prefix"]), group_name=group or None, iterate=it,
+                            n_star=state["n_star"], log=log,
+                            start=(state["omega"], state["rho"], state["result"]))
+            state["sweep"] = pts
+            system = pts[-1].system
+        elif name in ("FIELD_TO_RGRID", "RGRID_TO_FIELD", "RHO_TO_OMEGA"):
+            src, dst = at(body["input_filename"][0]), at(body["output_filename"][0])
+            if name == "FIELD_TO_RGRID":
+                _, f = F.read_field(src, system, group)
+                F.write_rgrid(dst, f, system, group)
+            elif name == "RGRID_TO_FIELD":
+                _, _, f = F.read_rgrid(src)
+                b = StarBasis(group, system.ngrid)
+                f = np.stack([b.to_grid(b.to_basis(x)) for x in f])      # onto the group's fields
+                F.write_field(dst, f, system, group)
+            else:
+                # omega_a = sum_b chi_ab rho_b: the pressure field set to zero
+                _, rho = F.read_field(src, system, group)
+                F.write_field(dst, system.chi @ rho, system, group)
+        else:
+            raise NotImplementedError(f"parameter-file command {name} is not run by this driver")
+    state["system"] = system
+    return state

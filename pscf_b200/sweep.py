@@ -321,12 +321,14 @@ class SweepPoint:
 def run_sweep(system: System, omega: np.ndarray, inc: Increments, s_max: float, solve: Callable,
               domain: bool, out_prefix: Optional[str] = None, group_name: Optional[str] = None,
               iterate: Optional[Dict] = None, n_star: int = 0, min_step: float = 1.0 / 16.0,
-              log: Callable[[str], None] = lambda msg: None) -> List[SweepPoint]:
+              log: Callable[[str], None] = lambda msg: None, start=None) -> List[SweepPoint]:
     """ITERATE at s = 0, then SWEEP to s_max (src/pscf.fp.f90:557-700).
     Returns the converged points at integer s (s = 0 first); with
     out_prefix, writes <prefix><j>.out (and <prefix><j>.omega / .rho in the
-    basis format when group_name is given) for each of them.  Raises
-    RuntimeError when a point fails at the smallest unit step or at s = 0."""
+    basis format when group_name is given) for each of them.  start:
+    (omega, rho, result) of an already converged s = 0 point, which is then
+    neither solved again nor written.  Raises RuntimeError when a point
+    fails at the smallest unit step or at s = 0."""
     def emit(j, pt):
         if not out_prefix:
             return
@@ -346,14 +348,15 @@ def run_sweep(system: System, omega: np.ndarray, inc: Increments, s_max: float, 
     # writes them, default-real (single precision) literals
     f01, f09 = float(np.float32(0.1)), float(np.float32(0.9))
     t0 = time.perf_counter()
-    w, rho, r = solve(system, omega)
+    w, rho, r = solve(system, omega) if start is None else start
     if not r["converged"]:
         raise RuntimeError("the first point (s = 0) did not converge")
     sys0 = copy.deepcopy(system)
     if domain:
         sys0.cell_param = list(r["cell_param"])
     points = [SweepPoint(0.0, sys0, w, rho, r, time.perf_counter() - t0)]
-    emit(0, points[0])
+    if start is None:
+        emit(0, points[0])
     hist = History()
     hist.update(0.0, w, sys0.cell_param, domain)
     cur = sys0
