@@ -7,6 +7,9 @@ layout -- the same layout as the first part of an output summary:
 
   MONOMERS, CHAINS, SOLVENTS, COMPOSITION, INTERACTION, UNIT_CELL,
   DISCRETIZATION, BASIS  -- the system;
+  RESCALE                -- read an omega file and change the monomer
+                            reference volume (the next ITERATE starts
+                            from that field);
   ITERATE                -- solve from a basis-format omega file;
   SWEEP                  -- continuation to s_max with d_<name> increments,
                             ended by end_increments;
@@ -17,8 +20,8 @@ read_param parses a file into its sections; system_of builds the System;
 run_param executes the commands in order with the engine (Anderson mixing,
 or Newton with the batched Jacobian for itr_algo 'NR'), writing the same
 files as the reference: <output_prefix>out / omega / rho for ITERATE,
-<output_prefix>0., 1., ... for a SWEEP.  RESPONSE, RESCALE, KGRID_TO_RGRID,
-OUTPUT_WAVES and OUTPUT_GROUP are not run here (pscf_b200.response covers
+<output_prefix>0., 1., ... for a SWEEP.  RESPONSE, KGRID_TO_RGRID, OUTPUT_WAVES
+and OUTPUT_GROUP are not run here (pscf_b200.response covers
 the response calculation from Python).
 """
 from __future__ import annotations
@@ -53,7 +56,12 @@ def _values(line: str):
 def read_param(path: str) -> List[Tuple[str, Dict[str, List]]]:
     """Sections of a parameter file in file order: (name, {label: values});
     parsing stops at FINISH."""
-    lines = open(path).read().splitlines()
+    return read_param_text(open(path).read(), path)
+
+
+def read_param_text(text: str, path: str = "<text>") -> List[Tuple[str, Dict[str, List]]]:
+    """read_param of the file's text."""
+    lines = text.splitlines()
     out: List[Tuple[str, Dict[str, List]]] = []
     cur = None
     key = None
@@ -180,8 +188,31 @@ def increments_of(body: Dict[str, List], system: System):
     return body["s_max"][0], inc
 
 
+def rescale_vref(system: System, scale: float) -> System:
+    """The same system with the monomer reference volume v -> v / scale
+    (rescale_vref, src/chemistry_mod.f90:1344-1361): kuhn / sqrt(scale),
+    chi (or chi_A and chi_B) / scale, block lengths and solvent sizes
+    x scale.  The caller divides omega by scale."""
+    import copy
+    s = copy.deepcopy(system)
+    s.kuhn = [k / np.sqrt(scale) for k in s.kuhn]
+    if s.temperature is not None:
+        s.chi_A = s.chi_A / scale
+        s.chi_B = s.chi_B / scale
+        s.chi = s.chi_A / float(s.temperature) + s.chi_B
+    else:
+        s.chi = np.asarray(s.chi, dtype=np.float64) / scale
+    for c in s.chains:
+        c.block_length = [L * scale for L in c.block_length]
+    for v in s.solvents:
+        v.size = v.size * scale
+    return s
+
+
 def _iterate_params(body):
-    it = dict(input_filename=body["input_filename"][0], output_prefix=body["output_prefix"][0],
+    # an ITERATE after RESCALE has no input_filename: it starts from the rescaled field
+    it = dict(input_filename=body["input_filename"][0] if "input_filename" in body else None,
+              output_prefix=body["output_prefix"][0],
               max_itr=int(body["max_itr"][0]), error_max=body["error_max"][0], domain=body["domain"][0] == "T",
               itr_algo=body["itr_algo"][0])
     if it["itr_algo"] == "NR":
@@ -220,9 +251,23 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
             continue
         if name == "FINISH":
             break
+        if name == "RESCALE":
+            # src/pscf.fp.f90:414-455: read omega, change v, then omega / scale
+            lam = body["vref_scale"][0]
+            _, w = F.read_field(at(body["input_filename"][0]), system, group)
+            system = rescale_vref(system, lam)
+            state["omega_in"] = w / lam
+            state["omega_file"] = body["input_filename"][0]
+            continue
         if name == "ITERATE":
             it = _iterate_params(body)
-            _, w0 = F.read_field(at(it["input_filename"]), system, group)
+            if it["input_filename"] is None:
+                if "omega_in" not in state:
+                    raise ValueError("ITERATE without input_filename needs a RESCALE before it")
+                w0 = state.pop("omega_in")
+                it["input_filename"] = state["omega_file"]
+            else:
+                _, w0 = F.read_field(at(it["input_filename"]), system, group)
             t0 = time.perf_counter()
             w, rho, r = _solver(it, group)(system, w0)
             dt = time.perf_counter() - t0

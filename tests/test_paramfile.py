@@ -133,14 +133,7 @@ def test_three_monomer_file_with_sweep(tmp_path):
     assert it["itr_algo"] == "AM" and it["N_hist"] == 10 and it["domain"] is False
 
 
-def test_field_conversion_commands(tmp_path):
-    """FIELD_TO_RGRID, RGRID_TO_FIELD and RHO_TO_OMEGA on the reference's
-    own rho file (group -1, 40 points): the grid file holds the field, the
-    round trip restores every coefficient, and omega = chi rho."""
-    import shutil
-    h = F._read_header(open(os.path.join(HERE, "golden", "fieldfile_rho.txt")).read().splitlines())[0]
-    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "rho")
-    text = f""" format  1  0
+_TWO_MONOMER = """ format  1  0
 
 MONOMERS
 N_monomer
@@ -178,7 +171,7 @@ crystal_system
 N_cell_param
                    1
 cell_param
-{h["cell_param"][0]:20.10E}
+@CELL@
 
 DISCRETIZATION
 ngrid
@@ -190,7 +183,17 @@ BASIS
 group_name
                 '-1'
 
-FIELD_TO_RGRID
+"""
+
+
+def test_field_conversion_commands(tmp_path):
+    """FIELD_TO_RGRID, RGRID_TO_FIELD and RHO_TO_OMEGA on the reference's
+    own rho file (group -1, 40 points): the grid file holds the field, the
+    round trip restores every coefficient, and omega = chi rho."""
+    import shutil
+    h = F._read_header(open(os.path.join(HERE, "golden", "fieldfile_rho.txt")).read().splitlines())[0]
+    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "rho")
+    text = _TWO_MONOMER.replace("@CELL@", f'{h["cell_param"][0]:20.10E}') + """FIELD_TO_RGRID
 input_filename
                'rho'
 output_filename
@@ -222,4 +225,58 @@ FINISH
     np.testing.assert_allclose(w, s.chi @ rho, atol=1e-9)
     with pytest.raises(NotImplementedError):
         (tmp_path / "p2").write_text(text.replace("FIELD_TO_RGRID", "OUTPUT_WAVES", 1))
+        P.run_param(str(tmp_path / "p2"))
+
+
+def test_rescale_reference_volume(tmp_path, monkeypatch):
+    """RESCALE (src/pscf.fp.f90:414-455, rescale_vref
+    src/chemistry_mod.f90:1344-1361): v -> v / lambda divides kuhn by
+    sqrt(lambda) and chi and omega by lambda and multiplies block lengths and
+    solvent sizes by lambda, so chi N, omega N and b N^(1/2) stay; the
+    ITERATE after it has no input_filename and starts from omega / lambda."""
+    import shutil
+    from pscf_b200.system import Solvent
+    base = PARAM.split("ITERATE")[0]
+    s0, group = P.system_of(P.read_param_text(base + "FINISH\n"))
+    s0.solvents = [Solvent(monomer=2, size=0.2, phi=0.0)]
+    lam = 2.0
+    s1 = P.rescale_vref(s0, lam)
+    for c0, c1 in zip(s0.chains, s1.chains):
+        np.testing.assert_allclose(np.sum(c1.block_length) * s1.chi, np.sum(c0.block_length) * s0.chi)
+        np.testing.assert_allclose(np.sqrt(np.sum(c1.block_length)) * np.array(s1.kuhn),
+                                   np.sqrt(np.sum(c0.block_length)) * np.array(s0.kuhn))
+    assert s1.solvents[0].size == 0.4 and s0.solvents[0].size == 0.2       # the input is not modified
+    it = P._iterate_params(dict(output_prefix=["out/"], max_itr=[10.0], error_max=[1e-8], domain=["F"],
+                                itr_algo=["AM"], N_hist=[5.0]))
+    assert it["input_filename"] is None
+    # a file with RESCALE + ITERATE, run with a stand-in solver
+    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "in.omega")
+    h = F._read_header(open(tmp_path / "in.omega").read().splitlines())[0]
+    cell = f"{h['cell_param'][0]:20.10E}"
+    text = (_TWO_MONOMER.replace("@CELL@", cell) + "RESCALE\ninput_filename\n          'in.omega'\nvref_scale\n"
+            "    4.0000000000E+00\n\nITERATE\noutput_prefix\n              'out/'\nmax_itr\n"
+            "                 100\nerror_max\n    1.0000000000E-08\ndomain\n                   F\n"
+            "itr_algo\n                'AM'\nN_hist\n                  10\n\nFINISH\n")
+    (tmp_path / "param").write_text(text)
+    seen = {}
+
+    def fake_solver(it, group):
+        def solve(system, w0):
+            seen.update(system=system, w0=w0, it=it)
+            r = dict(converged=True, itr=1, error=1e-9, f_helmholtz=1.0, pressure=2.0, stress=[0.0],
+                     mu_chain=[3.0], cell_param=list(system.cell_param))
+            return w0, w0, r
+        return solve
+    monkeypatch.setattr(P, "_solver", fake_solver)
+    st = P.run_param(str(tmp_path / "param"))
+    s = seen["system"]
+    assert s.chains[0].block_length == [0.56 * 4.0, 0.44 * 4.0] and s.kuhn == [0.5, 0.5]
+    assert abs(s.chi[0, 1] - 15.0 / 4.0) < 1e-15 and seen["it"]["input_filename"] == "in.omega"
+    _, w = F.read_field(str(tmp_path / "in.omega"), s)
+    np.testing.assert_array_equal(seen["w0"], w / 4.0)
+    d = __import__("pscf_b200.sweep", fromlist=["read_out"]).read_out(str(tmp_path / "out" / "out"))
+    assert d["block_length"] == [2.24, 1.76] and d["input_filename"] == ["in.omega"]
+    (tmp_path / "p2").write_text(text.replace("RESCALE\ninput_filename\n          'in.omega'\nvref_scale\n"
+                                              "    4.0000000000E+00\n\n", ""))
+    with pytest.raises(ValueError):
         P.run_param(str(tmp_path / "p2"))
