@@ -194,7 +194,13 @@ class FieldBasis:
     def to_coeffs(self, field: np.ndarray) -> np.ndarray:
         """Reference basis coefficients [n_star] of a grid field
         (kgrid_to_basis)."""
-        F = _spectrum(np.asarray(field, dtype=np.float64), self.n)
+        return self.spectrum_to_coeffs(_spectrum(np.asarray(field, dtype=np.float64), self.n))
+
+    def spectrum_to_coeffs(self, F: np.ndarray) -> np.ndarray:
+        """Reference basis coefficients [n_star] of Fourier components F(G)
+        over the full grid (flat, x fastest): each star's coefficient is
+        read from its own wave alone (kgrid_to_basis,
+        src/grid_basis_mod.f90:146-200)."""
         out = np.zeros(len(self.stars))
         r2 = np.sqrt(2.0)
         for k, st in enumerate(self.stars):
@@ -223,11 +229,21 @@ def write_field(path: str, fields: np.ndarray, system, group_name: str) -> None:
     """Basis-format file of grid fields [n_monomer][nr] (output_field)."""
     fb = FieldBasis(group_name, system)
     fields = np.asarray(fields, dtype=np.float64).reshape(-1, system.nr)
-    coeffs = np.stack([fb.to_coeffs(f) for f in fields])          # [M][n_star]
+    write_coeffs(path, np.stack([fb.to_coeffs(f) for f in fields]), system, group_name, fb)
+
+
+def write_coeffs(path: str, coeffs: np.ndarray, system, group_name: str, fb: "FieldBasis" = None) -> None:
+    """Basis-format file of coefficients [n_monomer][n] of the first n stars
+    of the group's basis (output_field with N_basis_out = n,
+    src/field_io_mod.f90:101-135)."""
+    fb = fb or FieldBasis(group_name, system)
+    coeffs = np.atleast_2d(np.asarray(coeffs, dtype=np.float64))
+    if coeffs.shape[1] > len(fb.stars):
+        raise ValueError(f"{coeffs.shape[1]} coefficients for a basis of {len(fb.stars)} stars")
     cell = {"dim": system.dim, "crystal_system": system.crystal_system, "cell_param": system.cell_param}
-    out = _header(cell, group_name, len(fields))
-    out += [_label("N_star"), f"{len(fb.stars):>20d}"]
-    for s in range(len(fb.stars)):
+    out = _header(cell, group_name, len(coeffs))
+    out += [_label("N_star"), f"{coeffs.shape[1]:>20d}"]
+    for s in range(coeffs.shape[1]):
         line = "".join(f"{a:20.12E}" for a in coeffs[:, s]) + "    "
         line += "".join(f"{g:4d}" for g in fb.first_bz[s]) + f"{fb.count[s]:6d}"
         out.append(line)
@@ -274,6 +290,65 @@ def write_rgrid(path: str, fields: np.ndarray, system, group_name: str) -> None:
         out.append("".join(f"{fields[m, r]:18.9f}" for m in range(len(fields))) + "    ")
     with open(path, "w") as fh:
         fh.write("\n".join(out) + "\n")
+
+
+def write_kgrid(path: str, fields: np.ndarray, system, group_name: str) -> None:
+    """Wave-grid file of grid fields [n_monomer][nr]: the grid-format header,
+    then the Fourier components F(G) = (1/N) sum_r f(r) exp(-iG.r) on the
+    half grid 0 <= G1 <= n1/2, G3 fastest and G1 slowest, one line of
+    n_monomer complex values '(re,im)' per wave -- the file that
+    KGRID_TO_RGRID reads (src/pscf.fp.f90:813-888)."""
+    fields = np.asarray(fields, dtype=np.float64).reshape(-1, system.nr)
+    n = list(system.n)
+    spec = [_spectrum(f, n).reshape(n[2], n[1], n[0]) for f in fields]
+    cell = {"dim": system.dim, "crystal_system": system.crystal_system, "cell_param": system.cell_param}
+    out = _header(cell, group_name, len(fields))
+    out += [_label("ngrid"), "".join(f"{g:20d}" for g in system.ngrid)]
+    for i1 in range(n[0] // 2 + 1):
+        for i2 in range(n[1]):
+            for i3 in range(n[2]):
+                out.append("  ".join(f"({z[i3, i2, i1].real:.16E},{z[i3, i2, i1].imag:.16E})" for z in spec))
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+
+
+def read_kgrid(path: str, system) -> Tuple[Dict, np.ndarray]:
+    """(header, Fourier components [n_monomer][nr] over the full grid, flat
+    x fastest) of a wave-grid file (KGRID_TO_RGRID,
+    src/pscf.fp.f90:813-888).  The file holds the half grid
+    0 <= G1 <= n1/2 with G3 fastest, n_monomer complex values per wave in
+    list-directed form ('(re,im)', or two plain numbers); the other half
+    is F(-G) = conj F(G).  A grid that differs from the system's raises
+    ValueError, as the reference stops there."""
+    import re
+    lines = open(path).read().splitlines()
+    h, i = _read_header(lines)
+    if lines[i].split()[0] != "ngrid":
+        raise ValueError(f"{path}: expected 'ngrid', got {lines[i]!r}")
+    g = [int(x) for x in lines[i + 1].split()]
+    if g[:system.dim] != list(system.ngrid)[:system.dim]:
+        raise ValueError(f"{path}: inconsistent grid {g} in the wave-grid file (system grid {list(system.ngrid)})")
+    M = h["N_monomer"]
+    n = list(system.n)
+    n1h = n[0] // 2 + 1
+    text = "\n".join(lines[i + 2:]).replace("D", "E").replace("d", "e")
+    pairs = re.findall(r"\(\s*([^,()\s]+)\s*,\s*([^,()\s]+)\s*\)", text)
+    if pairs:
+        vals = np.array([complex(float(a), float(b)) for a, b in pairs])
+    else:
+        v = np.array([float(x) for x in text.split()])
+        vals = v[0::2] + 1j * v[1::2]
+    need = n1h * n[1] * n[2] * M
+    if len(vals) < need:
+        raise ValueError(f"{path}: {len(vals)} values, {need} expected")
+    half = vals[:need].reshape(n1h, n[1], n[2], M)                     # [G1][G2][G3][monomer]
+    out = np.zeros((M, n[2], n[1], n[0]), dtype=complex)
+    out[:, :, :, :n1h] = half.transpose(3, 2, 1, 0)
+    for x in range(n1h, n[0]):
+        # F(x, y, z) = conj F(-x, -y, -z), with -x in the half grid
+        src = out[:, :, :, (-x) % n[0]]
+        out[:, :, :, x] = np.conj(src[:, (-np.arange(n[2])) % n[2]][:, :, (-np.arange(n[1])) % n[1]])
+    return h, out.reshape(M, -1)
 
 
 def read_rgrid(path: str) -> Tuple[Dict, List[int], np.ndarray]:

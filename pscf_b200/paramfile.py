@@ -13,16 +13,19 @@ layout -- the same layout as the first part of an output summary:
   ITERATE                -- solve from a basis-format omega file;
   SWEEP                  -- continuation to s_max with d_<name> increments,
                             ended by end_increments;
-  FIELD_TO_RGRID, RGRID_TO_FIELD, RHO_TO_OMEGA -- field conversions;
+  RESPONSE               -- eigenvalues and eigenvectors of the linear
+                            response of the converged state along a line
+                            of k points;
+  FIELD_TO_RGRID, RGRID_TO_FIELD, KGRID_TO_RGRID, RHO_TO_OMEGA
+                         -- field conversions;
   FINISH.
 
 read_param parses a file into its sections; system_of builds the System;
 run_param executes the commands in order with the engine (Anderson mixing,
 or Newton with the batched Jacobian for itr_algo 'NR'), writing the same
 files as the reference: <output_prefix>out / omega / rho for ITERATE,
-<output_prefix>0., 1., ... for a SWEEP.  RESPONSE, KGRID_TO_RGRID, OUTPUT_WAVES
-and OUTPUT_GROUP are not run here (pscf_b200.response covers
-the response calculation from Python).
+<output_prefix>0., 1., ... for a SWEEP, <output_prefix>j.eval and
+j.evec.k for RESPONSE.  OUTPUT_WAVES and OUTPUT_GROUP are not run here.
 """
 from __future__ import annotations
 
@@ -224,6 +227,76 @@ def _iterate_params(body):
     return it
 
 
+def response_params(body: Dict[str, List], dim: int) -> Dict:
+    """The RESPONSE section, read in the order response_startup and
+    response_sweep read it (src/response_mod.f90:182, 329-342): k_group,
+    kdim, kvec0 (kdim values), nkstep, dkvec (kdim values, present only
+    when nkstep > 0), n_eigval_out, n_eigvec_out, n_basis_out.  The labels
+    are comments there and are not checked here either."""
+    vals = [v for vs in body.values() for v in vs]
+    pos = [0]
+
+    def take(n=1):
+        if pos[0] + n > len(vals):
+            raise ValueError("RESPONSE: section ends early")
+        out = vals[pos[0]:pos[0] + n]
+        pos[0] += n
+        return out
+    k_group = str(take()[0])
+    if dim == 1 and k_group.strip() == "P 1":
+        k_group = "1"
+    kdim = int(take()[0])
+    if kdim not in (dim, dim + 1):
+        raise ValueError(f"RESPONSE: kdim must equal dim or dim+1, got {kdim}")
+    kvec0 = [float(x) for x in take(kdim)]
+    nkstep = int(take()[0])
+    dkvec = [float(x) for x in take(kdim)] if nkstep > 0 else [0.0] * kdim
+    n_eigval_out, n_eigvec_out, n_basis_out = (int(x) for x in take(3))
+    return dict(k_group=k_group, kdim=kdim, kvec0=kvec0, nkstep=nkstep, dkvec=dkvec, n_eigval_out=n_eigval_out,
+                n_eigvec_out=n_eigvec_out, n_basis_out=n_basis_out)
+
+
+def _fortran_e(v: float, w: int = 20, d: int = 9) -> str:
+    """Fortran Ew.d: 0.ddd...E+xx, right-justified in w columns (a
+    three-digit exponent drops the E)."""
+    v = float(v)
+    if v == 0.0:
+        body = "0." + "0" * d + "E+00"
+    else:
+        m, e = f"{abs(v):.{d - 1}E}".split("E")
+        e = int(e) + 1
+        digits = m.replace(".", "")
+        ex = f"E{'+' if e >= 0 else '-'}{abs(e):02d}" if abs(e) < 100 else f"{'+' if e >= 0 else '-'}{abs(e):03d}"
+        body = ("-" if v < 0 else "") + "0." + digits + ex
+    return f"{body:>{w}}"
+
+
+def write_eval(path: str, kvec: List[float], n_basis: int, evals) -> None:
+    """Eigenvalue file of one k point (calc_drho_domega_full,
+    src/response_mod.f90:597-605): q_vec (three components), N_basis, an
+    empty line, then one 'eval  k' line per eigenvalue (E20.9, I5)."""
+    k3 = list(kvec) + [0.0] * (3 - len(kvec))
+    out = [f"{'q_vec   =':<20}" + "".join(f"{x:20.10E}" for x in k3[:3]),
+           f"{'N_basis =':<20}" + f"{n_basis:20d}", ""]
+    out += [_fortran_e(x) + "  " + f"{k:5d}" for k, x in enumerate(evals, 1)]
+    with open(path, "w") as fh:
+        fh.write("\n".join(out) + "\n")
+
+
+def _response_sweep(system: System, omega, rp: Dict):
+    """The response at every k point of the sweep, on the engine (fp64):
+    the ideal-gas propagation of the converged state and the incompressible
+    response (pscf_b200.response)."""
+    from .engine import FP64, Engine
+    from .response import response_sweep
+    e = Engine([system], FP64)
+    try:
+        e.density(np.asarray(omega, dtype=np.float64).reshape(1, system.n_monomer, system.nr))
+        return response_sweep(e, 0, rp["kvec0"], rp["dkvec"], rp["nkstep"], rp["k_group"], rp["n_eigval_out"])
+    finally:
+        e.close()
+
+
 def _solver(it, group):
     from .sweep import am_solver, nr_solver
     if it["itr_algo"] == "AM":
@@ -251,6 +324,10 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
             continue
         if name == "FINISH":
             break
+        # set by ITERATE, kept by SWEEP, cleared by every other command (iterate_flag, src/pscf.fp.f90)
+        iterate_flag = state.get("iterate_flag", False)
+        if name not in ("ITERATE", "SWEEP"):
+            state["iterate_flag"] = False
         if name == "RESCALE":
             # src/pscf.fp.f90:414-455: read omega, change v, then omega / scale
             lam = body["vref_scale"][0]
@@ -285,7 +362,7 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
                 F.write_field(prefix + "omega", w, system, group)
                 F.write_field(prefix + "rho", rho, system, group)
             log(f"ITERATE: {'converged' if r['converged'] else 'not converged'} after {r['itr']} iterations")
-            state.update(iterate=it, omega=w, rho=rho, result=r, n_star=n_star)
+            state.update(iterate=it, omega=w, rho=rho, result=r, n_star=n_star, iterate_flag=True)
         elif name == "SWEEP":
             if "result" not in state or not state["result"]["converged"]:
                 raise RuntimeError("SWEEP needs a converged ITERATE before it")
@@ -297,9 +374,33 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
                             start=(state["omega"], state["rho"], state["result"]))
             state["sweep"] = pts
             system = pts[-1].system
-        elif name in ("FIELD_TO_RGRID", "RGRID_TO_FIELD", "RHO_TO_OMEGA"):
+            state["omega"] = pts[-1].omega
+        elif name == "RESPONSE":
+            # src/pscf.fp.f90:707-723 and response_sweep, src/response_mod.f90:309-389
+            if not iterate_flag:
+                raise RuntimeError("RESPONSE needs an ITERATE before it")
+            rp = response_params(body, system.dim)
+            pts = _response_sweep(system, state["omega"], rp)
+            prefix = at(state["iterate"]["output_prefix"])
+            d = os.path.dirname(prefix)
+            if d:
+                os.makedirs(d, exist_ok=True)
+            for j, pt in enumerate(pts):
+                write_eval(f"{prefix}{j}.eval", pt["kvec"], pt["n_basis"], pt["eval"])
+                nb = min(rp["n_basis_out"], pt["n_basis"])
+                for k in range(min(rp["n_eigvec_out"], len(pt["eval"]))):
+                    v = pt["evec"][:nb, k]
+                    F.write_coeffs(f"{prefix}{j}.evec.{k + 1}", np.stack([v, -v]), system, rp["k_group"])
+            log(f"RESPONSE: {len(pts)} k points")
+            state["response"] = pts
+        elif name in ("FIELD_TO_RGRID", "RGRID_TO_FIELD", "KGRID_TO_RGRID", "RHO_TO_OMEGA"):
             src, dst = at(body["input_filename"][0]), at(body["output_filename"][0])
-            if name == "FIELD_TO_RGRID":
+            if name == "KGRID_TO_RGRID":
+                # wave grid -> basis coefficients -> coordinate grid (src/pscf.fp.f90:813-888)
+                _, spec = F.read_kgrid(src, system)
+                fb = F.FieldBasis(group, system)
+                F.write_rgrid(dst, np.stack([fb.to_grid(fb.spectrum_to_coeffs(z)) for z in spec]), system, group)
+            elif name == "FIELD_TO_RGRID":
                 _, f = F.read_field(src, system, group)
                 F.write_rgrid(dst, f, system, group)
             elif name == "RGRID_TO_FIELD":

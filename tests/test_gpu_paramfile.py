@@ -112,3 +112,45 @@ def test_iterate_and_sweep_from_a_parameter_file(tmp_path):
     assert abs(last.system.cell_param[0] - r[0]["cell_param"][0]) < 1e-6
     d2 = S.read_out(str(tmp_path / "out" / "2.out"))
     assert abs(d2["f_Helmholtz"][0] - r[0]["f_helmholtz"]) < 1e-8
+
+
+RESPONSE = """RESPONSE
+k_group
+                 '1'
+kdim
+                   1
+kvec
+    1.0000000000E-01
+nkstep
+                   1
+dkvec
+    2.0000000000E-01
+n_eigval_out
+                   4
+n_eigvec_out
+                   1
+n_basis_out
+                   4
+
+FINISH
+"""
+
+
+def test_iterate_and_response_from_a_parameter_file(tmp_path):
+    """ITERATE then RESPONSE (src/pscf.fp.f90:707-723) on the engine: the
+    eigenvalues in <prefix>0.eval and 1.eval equal the oracle's response
+    of the converged state at k = 0.1 and 0.3."""
+    from tests.test_paramfile import _oracle_response_sweep
+    s = diblock(1, [32], "lamellar", [1.5], fA=0.5, chiN=15.0)
+    F.write_field(str(tmp_path / "in.omega"), lamellar_guess(s), s, "-1")
+    (tmp_path / "param").write_text(TEXT.split("SWEEP\n")[0] + RESPONSE)
+    st = P.run_param(str(tmp_path / "param"))
+    assert st["result"]["converged"] and len(st["response"]) == 2
+    want = _oracle_response_sweep(st["system"], st["omega"],
+                                  dict(k_group="1", kvec0=[0.1], dkvec=[0.2], nkstep=1, n_eigval_out=4))
+    for j, pt in enumerate(want):
+        lines = open(tmp_path / "out" / f"{j}.eval").read().splitlines()
+        ev = [float(x.split()[0]) for x in lines[3:]]
+        np.testing.assert_allclose(ev, pt["eval"], rtol=1e-8)
+        np.testing.assert_allclose(st["response"][j]["eval"], pt["eval"], rtol=1e-9)
+        assert (tmp_path / "out" / f"{j}.evec.1").exists()

@@ -280,3 +280,136 @@ def test_rescale_reference_volume(tmp_path, monkeypatch):
                                               "    4.0000000000E+00\n\n", ""))
     with pytest.raises(ValueError):
         P.run_param(str(tmp_path / "p2"))
+
+
+def test_kgrid_to_rgrid(tmp_path):
+    """KGRID_TO_RGRID (src/pscf.fp.f90:813-888): a wave-grid file of the
+    reference's rho (Fortran list-directed '(re , im)' values) gives the
+    same coordinate grid as FIELD_TO_RGRID of the basis file; each star's
+    coefficient comes from its own wave (kgrid_to_basis), so a change at
+    another wave of the star does not move it; a wrong grid raises."""
+    import shutil
+    h = F._read_header(open(os.path.join(HERE, "golden", "fieldfile_rho.txt")).read().splitlines())[0]
+    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "rho")
+    sys_text = _TWO_MONOMER.replace("@CELL@", f'{h["cell_param"][0]:20.10E}')
+    (tmp_path / "p0").write_text(sys_text + "FINISH\n")
+    s, group = P.system_of(P.read_param(str(tmp_path / "p0")))
+    _, rho = F.read_field(str(tmp_path / "rho"), s)
+    F.write_kgrid(str(tmp_path / "rho.kg"), rho, s, group)
+    # the Fortran list-directed form of the same values
+    lines = open(tmp_path / "rho.kg").read().splitlines()
+    nh = len(lines) - (s.n[0] // 2 + 1)
+    fort = lines[:nh] + [ln.replace("(", "(  ").replace(",", "     ,  ").replace(")", "     )").replace("E", "D")
+                         for ln in lines[nh:]]
+    (tmp_path / "rho.kgf").write_text("\n".join(fort) + "\n")
+    text = sys_text + ("KGRID_TO_RGRID\ninput_filename\n             'rho.kgf'\noutput_filename\n"
+                       "              'a.rg'\n\nFIELD_TO_RGRID\ninput_filename\n               'rho'\n"
+                       "output_filename\n              'b.rg'\n\nFINISH\n")
+    (tmp_path / "param").write_text(text)
+    P.run_param(str(tmp_path / "param"))
+    assert open(tmp_path / "a.rg").read() == open(tmp_path / "b.rg").read()
+    _, spec = F.read_kgrid(str(tmp_path / "rho.kg"), s)
+    fb = F.FieldBasis(group, s)
+    c0 = fb.spectrum_to_coeffs(spec[0])
+    st = next(x for x in fb.stars if len(x["idx"]) > 1)
+    other = next(int(k) for k in st["idx"] if int(k) != st["wave"])
+    bumped = spec[0].copy()
+    bumped[other] += 0.5
+    np.testing.assert_array_equal(fb.spectrum_to_coeffs(bumped), c0)
+    s2, _ = P.system_of(P.read_param_text(sys_text.replace("                  40\n", "                  20\n")
+                                          + "FINISH\n"))
+    with pytest.raises(ValueError):
+        F.read_kgrid(str(tmp_path / "rho.kg"), s2)
+
+
+def _oracle_response_sweep(system, omega, rp):
+    """response_sweep of pscf_b200.response with the oracle in place of the
+    engine (the CPU stand-in for _response_sweep)."""
+    from oracle import response as R
+    from pscf_b200.response import perturbation_basis
+    basis = perturbation_basis(rp["k_group"], system.ngrid)
+    resp = R.Response(system, np.asarray(omega).reshape(system.n_monomer, system.nr))
+    G = system.unit_cell()[0]
+    out, k = [], np.array(rp["kvec0"], dtype=float)
+    for _ in range(rp["nkstep"] + 1):
+        kt = R.transverse_ksq(system.dim, G, k)
+        smm, spm, spp = resp.drho_domega_id(k[:system.dim], kt, basis)[:3]
+        ev, V = R.drho_domega_full(smm, spm, spp, float(system.chi[0, 1]), rp["n_eigval_out"])
+        out.append({"kvec": k.copy(), "eval": ev, "evec": V, "n_basis": len(basis)})
+        k = k + np.asarray(rp["dkvec"])
+    return out
+
+
+def test_fortran_e_format():
+    assert P._fortran_e(1.0) == "     0.100000000E+01"
+    assert P._fortran_e(-0.5) == "    -0.500000000E+00"
+    assert P._fortran_e(0.0) == "     0.000000000E+00"
+    assert P._fortran_e(9.9999999999) == "     0.100000000E+02"
+    assert P._fortran_e(-1.234567891e-5) == "    -0.123456789E-04"
+    assert P._fortran_e(1e-101) == "     0.100000000-100"
+
+
+def test_response_command(tmp_path, monkeypatch):
+    """RESPONSE (src/pscf.fp.f90:707-723; response_sweep and
+    calc_drho_domega_full, src/response_mod.f90:309-389, 497-652): the
+    section is read in the reference's order (no dkvec when nkstep = 0),
+    needs an ITERATE (or SWEEP) just before it, and writes
+    <prefix>j.eval (q_vec, N_basis, E20.9 eigenvalues) and
+    <prefix>j.evec.k (the eigenvector's first n_basis_out coefficients,
+    +v / -v for the two monomers) per k point.  The engine's response is
+    stood in for by the oracle here; the GPU test runs the engine."""
+    import shutil
+    from oracle import response as R
+    from pscf_b200.sweep import read_out
+    rp = P.response_params({"k_group": ["1"], "kdim": [1.0], "kvec0": [0.0], "nkstep": [0.0],
+                            "n_eigval_out": [4.0], "n_eigvec_out": [1.0], "n_basis_out": [3.0]}, 1)
+    assert rp["dkvec"] == [0.0] and rp["n_basis_out"] == 3
+    assert P.response_params({"a": ["P 1"], "b": [2.0], "c": [0.1, 0.2], "d": [1.0], "e": [0.0, 0.1],
+                              "f": [1.0, 1.0, 1.0]}, 1)["k_group"] == "1"
+    with pytest.raises(ValueError):
+        P.response_params({"k_group": ["1"], "kdim": [3.0]}, 1)
+    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "in.omega")
+    h = F._read_header(open(tmp_path / "in.omega").read().splitlines())[0]
+    sys_text = _TWO_MONOMER.replace("@CELL@", f'{h["cell_param"][0]:20.10E}')
+    iterate = ("ITERATE\ninput_filename\n          'in.omega'\noutput_prefix\n              'out/'\nmax_itr\n"
+               "                 100\nerror_max\n    1.0000000000E-08\ndomain\n                   F\n"
+               "itr_algo\n                'AM'\nN_hist\n                  10\n\n")
+    response = ("RESPONSE\nk_group\n                 '1'\nkdim\n                   1\nkvec\n"
+                "    1.0000000000E-01\nnkstep\n                   1\ndkvec\n    2.0000000000E-01\n"
+                "n_eigval_out\n                   5\nn_eigvec_out\n                   2\nn_basis_out\n"
+                "                   6\n\n")
+
+    def fake_solver(it, group):
+        def solve(system, w0):
+            r = dict(converged=True, itr=1, error=1e-9, f_helmholtz=1.0, pressure=2.0, stress=[0.0],
+                     mu_chain=[3.0], cell_param=list(system.cell_param))
+            return w0, w0, r
+        return solve
+    monkeypatch.setattr(P, "_solver", fake_solver)
+    monkeypatch.setattr(P, "_response_sweep", _oracle_response_sweep)
+    (tmp_path / "param").write_text(sys_text + iterate + response + "FINISH\n")
+    st = P.run_param(str(tmp_path / "param"))
+    s = st["system"]
+    _, w = F.read_field(str(tmp_path / "in.omega"), s)
+    want = _oracle_response_sweep(s, w, dict(k_group="1", kvec0=[0.1], dkvec=[0.2], nkstep=1, n_eigval_out=5))
+    for j, pt in enumerate(want):
+        lines = open(tmp_path / "out" / f"{j}.eval").read().splitlines()
+        assert lines[0].startswith("q_vec   =") and abs(float(lines[0].split()[2]) - (0.1 + 0.2 * j)) < 1e-12
+        assert lines[1].split()[-1] == "40" and lines[2] == ""
+        ev = [float(x.split()[0]) for x in lines[3:]]
+        assert [int(x.split()[1]) for x in lines[3:]] == list(range(1, 6))
+        np.testing.assert_allclose(ev, pt["eval"], rtol=1e-8)
+        for k in (1, 2):
+            el = open(tmp_path / "out" / f"{j}.evec.{k}").read().splitlines()
+            i = el.index(next(x for x in el if x.startswith("N_star")))
+            assert int(el[i + 1]) == 6
+            rows = [[float(v) for v in x.split()[:2]] for x in el[i + 2:i + 8]]
+            np.testing.assert_allclose([r[0] for r in rows], pt["evec"][:6, k - 1], rtol=1e-11, atol=1e-13)
+            assert all(r[1] == -r[0] for r in rows)
+        assert not os.path.exists(tmp_path / "out" / f"{j}.evec.3")
+    # RESPONSE must follow ITERATE (or SWEEP) directly
+    conv = "RHO_TO_OMEGA\ninput_filename\n          'in.omega'\noutput_filename\n          'w2'\n\n"
+    for text in (sys_text + response, sys_text + iterate + conv + response):
+        (tmp_path / "p2").write_text(text + "FINISH\n")
+        with pytest.raises(RuntimeError):
+            P.run_param(str(tmp_path / "p2"))
