@@ -151,6 +151,8 @@ def test_iterate_and_response_from_a_parameter_file(tmp_path):
     for j, pt in enumerate(want):
         lines = open(tmp_path / "out" / f"{j}.eval").read().splitlines()
         ev = [float(x.split()[0]) for x in lines[3:]]
-        np.testing.assert_allclose(ev, pt["eval"], rtol=1e-8)
-        np.testing.assert_allclose(st["response"][j]["eval"], pt["eval"], rtol=1e-9)
+        # absolute as well as relative: the lowest eigenvalue of an ordered phase
+        # at small k lies near the translation mode's zero
+        np.testing.assert_allclose(ev, pt["eval"], rtol=1e-7, atol=1e-7)
+        np.testing.assert_allclose(st["response"][j]["eval"], pt["eval"], rtol=1e-7, atol=1e-7)
         assert (tmp_path / "out" / f"{j}.evec.1").exists()
