@@ -308,9 +308,9 @@ int pscfg_propagate(pscfg_engine *e, int inst, const double *omega_m, double b, 
  * 512 n3 bytes each.  Other grids are rejected with PSCFG_EINVAL, before
  * any GPU work is queued, and a message from pscfg_last_error(NULL).  The
  * first call on a device does a one-time set-up with that device current:
- * it looks up the array's device address (cudaGetSymbolAddress) and uploads
- * the codelet constants; make that first call before any stream capture.
- * A call queues kernel launches only (no host-device copies).  All calls
+ * it looks up the array's device address (cudaGetSymbolAddress) and copies
+ * the codelet constants to the device (cudaMemcpyToSymbol).  After that a
+ * call queues kernel launches only (no host-device copies).  All calls
  * on a device share the array: calls whose GPU work overlaps (other host
  * threads, or streams with no ordering between them) race on it.  Each
  * call writes every scratch entry it reads, so nothing carries over from
