@@ -107,3 +107,32 @@ def test_basis_file_without_inversion(tmp_path, group, dim, ngrid, crystal, cell
         a = np.zeros(len(fb.stars))
         a[k] = 1.0
         np.testing.assert_allclose(fb.to_coeffs(fb.to_grid(a)), a, atol=1e-12)
+
+
+@pytest.mark.parametrize("group,dim,ngrid,crystal,cell", [
+    ("P 1", 3, [6, 5, 4], "orthorhombic", [1.0, 1.5, 2.0]),
+    ("I 41 3 2", 3, [8, 8, 8], "cubic", [3.7]),
+    ("p 6 m m", 2, [9, 9], "hexagonal", [1.9]),
+])
+def test_wave_grid_file(tmp_path, group, dim, ngrid, crystal, cell):
+    """Wave-grid files (read by KGRID_TO_RGRID, src/pscf.fp.f90:813-888):
+    the half grid G1 <= n1/2 with G3 fastest; the reader fills the other
+    half from F(-G) = conj F(G), so a general real field's full spectrum
+    comes back; a group's field read through its basis is unchanged."""
+    s = diblock(dim, ngrid, crystal, cell)
+    w = omega_guess(s, 7, 2.0)
+    p = tmp_path / "k"
+    F.write_kgrid(str(p), w, s, group)
+    n = list(s.n)
+    lines = _lines(str(p))
+    assert lines[13].split()[0] == "ngrid" and len(lines) == 15 + (n[0] // 2 + 1) * n[1] * n[2]
+    _, spec = F.read_kgrid(str(p), s)
+    for m in range(2):
+        full = np.fft.fftn(w[m].reshape(n[2], n[1], n[0])).ravel() / s.nr
+        np.testing.assert_allclose(spec[m], full, rtol=0, atol=1e-15 * max(1.0, np.max(np.abs(full))))
+    ws = np.stack([G.symmetrize(w[m], group, ngrid) for m in range(2)])
+    F.write_kgrid(str(p), ws, s, group)
+    _, spec = F.read_kgrid(str(p), s)
+    fb = F.FieldBasis(group, s)
+    back = np.stack([fb.to_grid(fb.spectrum_to_coeffs(z)) for z in spec])
+    assert np.max(np.abs(back - ws)) < 1e-12 * max(1.0, np.max(np.abs(ws)))
