@@ -413,3 +413,41 @@ def test_response_command(tmp_path, monkeypatch):
         (tmp_path / "p2").write_text(text + "FINISH\n")
         with pytest.raises(RuntimeError):
             P.run_param(str(tmp_path / "p2"))
+
+
+def test_response_after_sweep_uses_the_last_point(tmp_path, monkeypatch):
+    """SWEEP leaves iterate_flag set (src/pscf.fp.f90:557-700), so a RESPONSE
+    after it runs on the sweep's last system and field."""
+    import shutil
+    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "in.omega")
+    h = F._read_header(open(tmp_path / "in.omega").read().splitlines())[0]
+    sys_text = _TWO_MONOMER.replace("@CELL@", f'{h["cell_param"][0]:20.10E}')
+    iterate = ("ITERATE\ninput_filename\n          'in.omega'\noutput_prefix\n              'out/'\nmax_itr\n"
+               "                 100\nerror_max\n    1.0000000000E-08\ndomain\n                   F\n"
+               "itr_algo\n                'AM'\nN_hist\n                  10\n\n")
+    sweep = "SWEEP\ns_max\n    1.0000000000E+00\nd_chi\n    2.0000000000E+00\nend_increments\n\n"
+    response = ("RESPONSE\nk_group\n                 '1'\nkdim\n                   1\nkvec\n"
+                "    2.0000000000E-01\nnkstep\n                   0\nn_eigval_out\n                   3\n"
+                "n_eigvec_out\n                   0\nn_basis_out\n                   0\n\n")
+    seen = []
+
+    def fake_solver(it, group):
+        def solve(system, w0):
+            seen.append(float(system.chi[0, 1]))
+            r = dict(converged=True, itr=1, error=1e-9, f_helmholtz=1.0, pressure=2.0, stress=[0.0],
+                     mu_chain=[3.0], cell_param=list(system.cell_param))
+            return w0 * (1.0 + 0.01 * len(seen)), w0, r
+        return solve
+    got = {}
+
+    def response_on_oracle(system, omega, rp):
+        got.update(chi=float(system.chi[0, 1]), omega=np.array(omega))
+        return _oracle_response_sweep(system, omega, rp)
+    monkeypatch.setattr(P, "_solver", fake_solver)
+    monkeypatch.setattr(P, "_response_sweep", response_on_oracle)
+    (tmp_path / "param").write_text(sys_text + iterate + sweep + response + "FINISH\n")
+    st = P.run_param(str(tmp_path / "param"))
+    assert abs(got["chi"] - 17.0) < 1e-6 and abs(seen[-1] - 17.0) < 1e-6
+    np.testing.assert_array_equal(got["omega"], st["sweep"][-1].omega)
+    assert (tmp_path / "out" / "0.eval").exists() and not (tmp_path / "out" / "0.evec.1").exists()
+    assert (tmp_path / "out" / "1.out").exists()
