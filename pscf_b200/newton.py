@@ -28,7 +28,7 @@ in tests, on the CPU oracle.
 from __future__ import annotations
 
 import math
-from typing import Optional, Sequence
+from typing import Optional
 
 import numpy as np
 

@@ -82,7 +82,7 @@ def rel_err(a, b):
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-from pscf_b200.guess import BCC_SITES, HEX_SITES, site_density, omega_from_density  # noqa: E402
+from pscf_b200.guess import BCC_SITES, site_density, omega_from_density  # noqa: E402
 
 
 def sphere_guess(system, fA, sites=BCC_SITES, width=0.08, chiN=None):

@@ -2,8 +2,6 @@
 import os
 import socket
 
-import numpy as np
-import pytest
 import torch.multiprocessing as mp
 
 from pscf_b200.parallel import shard

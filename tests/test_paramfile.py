@@ -235,6 +235,7 @@ def test_rescale_reference_volume(tmp_path, monkeypatch):
     solvent sizes by lambda, so chi N, omega N and b N^(1/2) stay; the
     ITERATE after it has no input_filename and starts from omega / lambda."""
     import shutil
+    from pscf_b200.sweep import read_out
     from pscf_b200.system import Solvent
     base = PARAM.split("ITERATE")[0]
     s0, group = P.system_of(P.read_param_text(base + "FINISH\n"))
@@ -274,7 +275,7 @@ def test_rescale_reference_volume(tmp_path, monkeypatch):
     assert abs(s.chi[0, 1] - 15.0 / 4.0) < 1e-15 and seen["it"]["input_filename"] == "in.omega"
     _, w = F.read_field(str(tmp_path / "in.omega"), s)
     np.testing.assert_array_equal(seen["w0"], w / 4.0)
-    d = __import__("pscf_b200.sweep", fromlist=["read_out"]).read_out(str(tmp_path / "out" / "out"))
+    d = read_out(str(tmp_path / "out" / "out"))
     assert d["block_length"] == [2.24, 1.76] and d["input_filename"] == ["in.omega"]
     (tmp_path / "p2").write_text(text.replace("RESCALE\ninput_filename\n          'in.omega'\nvref_scale\n"
                                               "    4.0000000000E+00\n\n", ""))
@@ -359,8 +360,6 @@ def test_response_command(tmp_path, monkeypatch):
     +v / -v for the two monomers) per k point.  The engine's response is
     stood in for by the oracle here; the GPU test runs the engine."""
     import shutil
-    from oracle import response as R
-    from pscf_b200.sweep import read_out
     rp = P.response_params({"k_group": ["1"], "kdim": [1.0], "kvec0": [0.0], "nkstep": [0.0],
                             "n_eigval_out": [4.0], "n_eigvec_out": [1.0], "n_basis_out": [3.0]}, 1)
     assert rp["dkvec"] == [0.0] and rp["n_basis_out"] == 3
