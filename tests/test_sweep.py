@@ -1,7 +1,7 @@
 """Sweep driver and output summary files (pscf_b200.sweep), on the CPU.
 
 The summary writer is pinned to two of the reference's own output files
-(tests/golden/sweep_0.out, lamellar.out, copied by make_outfile_fixture.py):
+(tests/golden/sweep/0.out, lamellar.out, copied by make_outfile_fixture.py):
 written from the values they hold, they come back byte for byte.  The
 sweep's step schedule, continuation and backtracking (src/pscf.fp.f90:557-700,
 src/sweep_mod.f90:407-600) are checked with a stand-in solver."""
@@ -48,7 +48,7 @@ def _from_out(path):
     return s, d["group_name"][0], res, it, st, d
 
 
-@pytest.mark.parametrize("name", ["sweep_0.out", "lamellar.out"])
+@pytest.mark.parametrize("name", ["sweep/0.out", "lamellar.out"])
 def test_output_summary_reproduces_reference_files(tmp_path, name):
     src = os.path.join(HERE, "golden", name)
     s, group, res, it, st, d = _from_out(src)
@@ -186,3 +186,39 @@ def test_temperature_interaction_sweep_and_summary(tmp_path):
     assert d["interaction_type"] == ["chi_T"] and d["chi_A"] == [3000.0] and d["chi_B"] == [-2.0]
     assert d["temperature"] == [195.0] and abs(d["chi"][0] - t.chi[1, 0]) < 1e-9
     assert lines.index("chi                 ") > lines.index("THERMO              ")
+
+
+def test_sweep_reproduces_the_reference_sweep_files(tmp_path, monkeypatch):
+    """The reference's own sweep (tools/python/tests/sweep/out/0.out ...
+    11.out: BCC 20^3, block length 0.39 -> 0.28 in steps of -0.01, cell
+    relaxed at every point), replayed with a stand-in solver that returns
+    each point's own results: every file comes back line for line but for
+    the two timings.  This pins the step schedule (the single-precision
+    first steps: 0.38000000022, ...), the parameters written, f_homo and
+    the layout against the reference's own output."""
+    ref = [_from_out(os.path.join(HERE, "golden", "sweep", f"{j}.out")) for j in range(12)]
+    s0, group, _, it, st0, _ = ref[0]
+    by_length = {round(r[0].chains[0].block_length[0], 9): r for r in ref}
+
+    def solve(system, omega):
+        got = by_length.get(round(system.chains[0].block_length[0], 9))
+        if got is None:                        # s = 0.1: not written
+            return omega, omega, dict(converged=True, itr=1, error=1e-9, f_helmholtz=0.0, pressure=0.0,
+                                      stress=[0.0], mu_chain=[0.0], cell_param=list(system.cell_param))
+        s, _, res, _, st, _ = got
+        r = dict(res, converged=True, itr=st["iterations"], error=st["final_error"], cell_param=list(s.cell_param))
+        return omega, omega, r
+    from pscf_b200 import field_io
+    monkeypatch.setattr(field_io, "write_field", lambda *a, **k: None)
+    pts = S.run_sweep(s0, np.zeros((2, s0.nr)), S.Increments(block_length=[[-0.01, 0.01]]), 11.0, solve,
+                      domain=True, out_prefix=str(tmp_path / "out") + "/", group_name=group, iterate=it,
+                      n_star=st0["n_star"])
+    assert len(pts) == 12
+    for j in range(12):
+        want = open(os.path.join(HERE, "golden", "sweep", f"{j}.out")).read().splitlines()
+        got = open(tmp_path / "out" / f"{j}.out").read().splitlines()
+        assert len(got) == len(want)
+        skip = {want.index(x) + 1 for x in want if x.strip() in ("basis_time", "scf_time")}
+        for k, (a, b) in enumerate(zip(got, want)):
+            if k not in skip:
+                assert a == b, (j, k, a, b)
