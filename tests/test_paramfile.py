@@ -247,6 +247,14 @@ def test_rescale_reference_volume(tmp_path, monkeypatch):
         np.testing.assert_allclose(np.sqrt(np.sum(c1.block_length)) * np.array(s1.kuhn),
                                    np.sqrt(np.sum(c0.block_length)) * np.array(s0.kuhn))
     assert s1.solvents[0].size == 0.4 and s0.solvents[0].size == 0.2       # the input is not modified
+    # interaction_type 'chi_T': chi_A and chi_B scale, the temperature stays
+    from pscf_b200.system import Chain, System
+    t0 = System(dim=1, ngrid=[16], crystal_system="lamellar", cell_param=[1.7], kuhn=[1.0, 1.0],
+                chi=np.zeros((2, 2)), chains=[Chain([0, 1], [0.5, 0.5])], ds=0.01,
+                chi_A=[[0.0, 3000.0], [3000.0, 0.0]], chi_B=[[0.0, -2.0], [-2.0, 0.0]], temperature=200.0)
+    t1 = P.rescale_vref(t0, 4.0)
+    assert t1.temperature == 200.0 and t1.chi_A[0, 1] == 750.0 and t1.chi_B[0, 1] == -0.5
+    assert abs(t1.chi[0, 1] - t0.chi[0, 1] / 4.0) < 1e-15 and t1.chains[0].block_length == [2.0, 2.0]
     it = P._iterate_params(dict(output_prefix=["out/"], max_itr=[10.0], error_max=[1e-8], domain=["F"],
                                 itr_algo=["AM"], N_hist=[5.0]))
     assert it["input_filename"] is None
