@@ -31,6 +31,7 @@ FFT.
 """
 from __future__ import annotations
 
+from collections import OrderedDict
 from typing import Dict, List, Sequence, Tuple
 
 import numpy as np
@@ -106,6 +107,37 @@ def _spectrum(field: np.ndarray, n: Sequence[int]) -> np.ndarray:
     return (np.fft.fftn(field.reshape(n[2], n[1], n[0])) / nr).ravel()
 
 
+_STAR_BASES: "OrderedDict[Tuple, StarBasis]" = OrderedDict()
+_FIELD_BASES: "OrderedDict[Tuple, FieldBasis]" = OrderedDict()
+
+
+def _cached(cache: OrderedDict, key: Tuple, make, keep: int):
+    obj = cache.pop(key, None)
+    if obj is None:
+        obj = make()
+    cache[key] = obj
+    while len(cache) > keep:
+        cache.popitem(last=False)
+    return obj
+
+
+def star_basis(group_name: str, ngrid: Sequence[int]) -> StarBasis:
+    """StarBasis(group_name, ngrid) for the file conventions, kept for the
+    last few (group, grid) pairs: it does not depend on the cell, so the
+    points of a sweep share it."""
+    key = (group_name, tuple(int(x) for x in ngrid))
+    return _cached(_STAR_BASES, key, lambda: StarBasis(group_name, ngrid), 4)
+
+
+def field_basis(group_name: str, system) -> "FieldBasis":
+    """FieldBasis(group_name, system), kept for the last two (group, grid,
+    cell) triples (a field file's omega and rho are written with the same
+    one)."""
+    key = (group_name, system.dim, tuple(int(x) for x in system.ngrid), system.crystal_system,
+           tuple(float(c) for c in system.cell_param))
+    return _cached(_FIELD_BASES, key, lambda: FieldBasis(group_name, system), 2)
+
+
 class FieldBasis:
     """Star basis of a group on a grid with the reference's file
     conventions (star waves, coefficient phases and normalisation, the
@@ -119,9 +151,13 @@ class FieldBasis:
         self.dim = system.dim
         self.n = list(system.n)
         self.nr = system.nr
-        self.basis = StarBasis(group_name, system.ngrid)
+        self.basis = star_basis(group_name, system.ngrid)
         self.Gb = make_unit_cell(system.dim, system.crystal_system, system.cell_param)[0]
         b = self.basis
+        # first-zone forms of every orbit's waves, in one pass over all of them
+        self._bz_off = np.concatenate([[0], np.cumsum([len(i) for i in b.orbit_idx])])
+        all_idx = np.concatenate([np.asarray(i) for i in b.orbit_idx])
+        self._bz_all = _g_to_bz(_grid_waves(all_idx, self.n), self.n, self.Gb, self.dim)
         self.stars: List[Dict] = []
         done = set()
         for s in range(b.n_star):
@@ -147,7 +183,7 @@ class FieldBasis:
     def _sorted(self, o):
         """Waves of star o in G_lt order (largest first), their first-zone forms."""
         idx = np.asarray(self.basis.orbit_idx[o])
-        bz = _g_to_bz(_grid_waves(idx, self.n), self.n, self.Gb, self.dim)
+        bz = self._bz_all[self._bz_off[o]:self._bz_off[o + 1]]
         order = sorted(range(len(idx)), key=lambda j: tuple(bz[j][:self.dim]), reverse=True)
         return idx, bz, order
 
@@ -227,7 +263,7 @@ class FieldBasis:
 
 def write_field(path: str, fields: np.ndarray, system, group_name: str) -> None:
     """Basis-format file of grid fields [n_monomer][nr] (output_field)."""
-    fb = FieldBasis(group_name, system)
+    fb = field_basis(group_name, system)
     fields = np.asarray(fields, dtype=np.float64).reshape(-1, system.nr)
     write_coeffs(path, np.stack([fb.to_coeffs(f) for f in fields]), system, group_name, fb)
 
@@ -236,7 +272,7 @@ def write_coeffs(path: str, coeffs: np.ndarray, system, group_name: str, fb: "Fi
     """Basis-format file of coefficients [n_monomer][n] of the first n stars
     of the group's basis (output_field with N_basis_out = n,
     src/field_io_mod.f90:101-135)."""
-    fb = fb or FieldBasis(group_name, system)
+    fb = fb or field_basis(group_name, system)
     coeffs = np.atleast_2d(np.asarray(coeffs, dtype=np.float64))
     if coeffs.shape[1] > len(fb.stars):
         raise ValueError(f"{coeffs.shape[1]} coefficients for a basis of {len(fb.stars)} stars")
@@ -261,7 +297,7 @@ def read_field(path: str, system, group_name: str = None) -> Tuple[Dict, np.ndar
     assert lines[i].split()[0] == "N_star"
     nstar = int(lines[i + 1].split()[0])
     M = h["N_monomer"]
-    fb = FieldBasis(group_name or h["group_name"], system)
+    fb = field_basis(group_name or h["group_name"], system)
     coeffs = np.zeros((M, len(fb.stars)))
     n = np.array(system.n)
     for line in lines[i + 2:i + 2 + nstar]:

@@ -311,7 +311,6 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
     workdir (default: the file's directory).  Returns the last system, the
     converged fields and results (ITERATE) and the sweep points (SWEEP)."""
     from . import field_io as F
-    from .basis import StarBasis
     from .sweep import run_sweep, write_out
     param = read_param(path)
     wd = workdir or os.path.dirname(os.path.abspath(path))
@@ -355,7 +354,7 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
             d = os.path.dirname(prefix)
             if d:
                 os.makedirs(d, exist_ok=True)
-            n_star = len(F.FieldBasis(group, system).stars) if group else 0
+            n_star = len(F.field_basis(group, system).stars) if group else 0
             stats = dict(n_star=n_star, final_error=r["error"], iterations=r["itr"], basis_time=0.0, scf_time=dt)
             write_out(prefix + "out", system, group, r, it, stats)
             if group:
@@ -398,14 +397,14 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
             if name == "KGRID_TO_RGRID":
                 # wave grid -> basis coefficients -> coordinate grid (src/pscf.fp.f90:813-888)
                 _, spec = F.read_kgrid(src, system)
-                fb = F.FieldBasis(group, system)
+                fb = F.field_basis(group, system)
                 F.write_rgrid(dst, np.stack([fb.to_grid(fb.spectrum_to_coeffs(z)) for z in spec]), system, group)
             elif name == "FIELD_TO_RGRID":
                 _, f = F.read_field(src, system, group)
                 F.write_rgrid(dst, f, system, group)
             elif name == "RGRID_TO_FIELD":
                 _, _, f = F.read_rgrid(src)
-                b = StarBasis(group, system.ngrid)
+                b = F.star_basis(group, system.ngrid)
                 f = np.stack([b.to_grid(b.to_basis(x)) for x in f])      # onto the group's fields
                 F.write_field(dst, f, system, group)
             else:
