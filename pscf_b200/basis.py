@@ -58,36 +58,60 @@ class StarBasis:
         order = np.lexsort((np.arange(self.nr), np.round(gsq, 10)))
         nvec = np.array(n)
         flat = lambda g: g[..., 0] + n[0] * (g[..., 1] + n[1] * g[..., 2])
-        # stars: wave indices, normalised projection coefficients, |G|^2
-        visited = np.zeros(self.nr, dtype=bool)
+        # orbits of the point operations g -> M^T g (mod n), each led by its
+        # member that comes first in `order` (a walk through `order` that
+        # skips waves already seen meets the same leaders in the same order)
+        rank = np.empty(self.nr, dtype=np.int64)
+        rank[order] = np.arange(self.nr)
+        lead_rank = np.empty(self.nr, dtype=np.int64)
+        # images M^T g of a block of waves as one exact small-integer product
+        Mt = np.asarray(M, dtype=np.float64).transpose(1, 0, 2).reshape(3, nops * 3)     # [j, (k, i)]
+
+        nvec32 = nvec.astype(np.int32)
+
+        def images(g):
+            return np.rint(g.astype(np.float64) @ Mt).astype(np.int32).reshape(len(g), nops, 3) % nvec32
+        chunk = max(1, (1 << 22) // nops)
+        for c0 in range(0, self.nr, chunk):
+            keys = flat(images(G[c0:c0 + chunk]))                                      # [waves, ops]
+            lead_rank[c0:c0 + chunk] = rank[keys].min(axis=1)
+        lead_ranks, orbit_id = np.unique(lead_rank, return_inverse=True)
+        leads = order[lead_ranks]
+        # projection coefficients phi(M^T g0) += exp(2 pi i g0.t / n) / |g|,
+        # summed over the operations in their order
+        coef_all = np.zeros(self.nr, dtype=complex)
+        for c0 in range(0, len(leads), chunk):
+            g0 = G[leads[c0:c0 + chunk]]                                              # [leaders, 3]
+            keys = flat(images(g0))
+            ph = np.exp(2j * np.pi * (t[None, :, :] * g0[:, None, :] / nvec[None, None, :]).sum(axis=2))
+            np.add.at(coef_all, keys.ravel(), ph.ravel())
+        coef_all /= nops
+        # stars: wave indices (ascending), normalised coefficients, |G|^2 of
+        # the leader; stars whose projection vanishes are dropped
+        by_orbit = np.lexsort((np.arange(self.nr), orbit_id))
+        starts = np.searchsorted(orbit_id[by_orbit], np.arange(len(leads) + 1))
         orb_idx, orb_coef, orb_gsq = [], [], []
-        orbit_of = {}
-        for w in order:
-            if visited[w]:
-                continue
-            g0 = G[w]
-            imgs = np.einsum("kji,j->ki", M, g0) % nvec                   # M^T g0
-            ph = np.exp(2j * np.pi * (t * g0[None, :] / nvec[None, :]).sum(axis=1))
-            keys = flat(imgs)
-            uniq, inv = np.unique(keys, return_inverse=True)
-            coef = np.zeros(len(uniq), dtype=complex)
-            np.add.at(coef, inv, ph)
-            coef /= nops
-            visited[uniq] = True
+        orbit_of = np.full(self.nr, -1, dtype=np.int64)
+        pos_in_orbit = np.empty(self.nr, dtype=np.int64)
+        pos_in_orbit[by_orbit] = np.arange(self.nr) - starts[orbit_id[by_orbit]]
+        neg_of = flat((-G) % nvec)                                           # flat index of -G
+        # a sequential sum of the non-negative |c|^2 is within 1e-12 (relative)
+        # of the pairwise np.sum below, so it settles every orbit away from
+        # the cancellation threshold; the others get the exact test
+        seq = np.add.reduceat(np.abs(coef_all[by_orbit]) ** 2, starts[:-1])
+        for o in np.nonzero(seq >= 1e-20 * (1.0 - 1e-12))[0]:
+            uniq = by_orbit[starts[o]:starts[o + 1]]
+            coef = coef_all[uniq]
             nrm = np.sum(np.abs(coef) ** 2)
             if nrm < 1e-20:
                 continue                                                     # cancelled star
-            for k in uniq:
-                orbit_of[int(k)] = len(orb_idx)
+            orbit_of[uniq] = len(orb_idx)
             orb_idx.append(uniq)
             orb_coef.append(coef / np.sqrt(nrm))
-            orb_gsq.append(float(gsq[w]))
+            orb_gsq.append(float(gsq[leads[o]]))
         # inverse partner of every star (itself when closed under inversion)
-        partner = []
-        for idx in orb_idx:
-            g = np.stack([idx % n[0], (idx // n[0]) % n[1], idx // (n[0] * n[1])], axis=1)
-            neg = flat((-g) % nvec)
-            partner.append(orbit_of[int(neg[0])])
+        partner = [int(x) for x in orbit_of[neg_of[np.array([idx[0] for idx in orb_idx], dtype=np.int64)]]] \
+            if orb_idx else []
         self.orbit_idx, self.orbit_coef, self.orbit_partner = orb_idx, orb_coef, partner
         # real basis functions
         self.star_idx: List[np.ndarray] = []
@@ -99,9 +123,7 @@ class StarBasis:
             p = partner[o]
             if p == o:
                 # phi(-G) = +- conj phi(G): real (cosine-like) or i x real
-                g = np.stack([idx % n[0], (idx // n[0]) % n[1], idx // (n[0] * n[1])], axis=1)
-                pos = {int(k): i for i, k in enumerate(idx)}
-                j = np.array([pos[int(k)] for k in flat((-g) % nvec)])
+                j = pos_in_orbit[neg_of[idx]]
                 odd = np.sum(np.abs(c + np.conj(c[j])) ** 2) < np.sum(np.abs(c - np.conj(c[j])) ** 2)
                 self.star_idx.append(idx)
                 self.star_coef.append(-1j * c if odd else c)
@@ -110,9 +132,7 @@ class StarBasis:
                 self.star_orbit.append(o)
             elif p > o:
                 # the pair (o, p): conj phi on the inverse waves of p
-                g = np.stack([idx % n[0], (idx // n[0]) % n[1], idx // (n[0] * n[1])], axis=1)
-                neg = flat((-g) % nvec)
-                both = np.concatenate([idx, neg])
+                both = np.concatenate([idx, neg_of[idx]])
                 r2 = np.sqrt(2.0)
                 self.star_idx += [both, both]
                 self.star_coef += [np.concatenate([c, np.conj(c)]) / r2,
