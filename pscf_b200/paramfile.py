@@ -219,7 +219,9 @@ def _iterate_params(body):
               max_itr=int(body["max_itr"][0]), error_max=body["error_max"][0], domain=body["domain"][0] == "T",
               itr_algo=body["itr_algo"][0])
     if it["itr_algo"] == "NR":
-        it["N_cut"] = int(body.get("N_cut", [0])[0])
+        if "N_cut" not in body:
+            raise ValueError("ITERATE: itr_algo 'NR' needs N_cut")
+        it["N_cut"] = int(body["N_cut"][0])
     elif it["itr_algo"] == "AM":
         it["N_hist"] = int(body.get("N_hist", [20])[0])
     else:
@@ -302,7 +304,9 @@ def _solver(it, group):
     if it["itr_algo"] == "AM":
         return am_solver(group or None, error_max=it["error_max"], max_itr=it["max_itr"], n_hist=it["N_hist"],
                          domain=it["domain"])
-    return nr_solver(group, n_cut=it["N_cut"] or None, error_max=it["error_max"], max_itr=it["max_itr"],
+    # N_cut = 0: no differenced columns, the Debye response alone
+    # (N_corner = 0, iterate_NR_startup, src/iterate_mod.fp.f90:200-225)
+    return nr_solver(group, n_cut=it["N_cut"], error_max=it["error_max"], max_itr=it["max_itr"],
                      domain=it["domain"])
 
 

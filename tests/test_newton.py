@@ -101,3 +101,30 @@ def test_debye_correlation_limits():
     np.testing.assert_allclose(c[:, :, 0], [[0.09, 0.21], [0.21, 0.49]], rtol=1e-14)
     x = 0.3 * 1e6 / 6.0
     assert abs(c[0, 0, 1] - 0.09 * 2.0 * (x - 1.0) / x ** 2) < 1e-15
+
+
+def test_newton_n_cut_zero_uses_the_debye_response_alone():
+    """N_cut = 0 (N_corner = 0 in iterate_NR_startup,
+    src/iterate_mod.fp.f90:200-225): no column is differenced, the Jacobian
+    is the homogeneous melt's Debye response, and from the lamellar guess
+    at chi N = 15 Newton settles on the disordered solution (uniform rho,
+    F = the Flory-Huggins free energy), itself a solution of the SCF
+    equations."""
+    from pscf_b200.sweep import free_energy_fh
+    g = GOLD["lamellar_outfile"]
+    s = diblock(1, [32], "lamellar", [g["cell_param"][0]], fA=0.5, chiN=g["chi"][0])
+    basis = StarBasis("-1", [32])
+    prov = OracleProvider(s, "-1")
+    batches = []
+    inner = prov.__call__
+
+    def counting(oms, cells=None, want_stress=False):
+        batches.append(len(oms))
+        return inner(oms, cells, want_stress)
+    w, rho, r = iterate_nr(counting, basis, s, lamellar_guess(s), error_max=1e-11, max_itr=100, n_cut=0)
+    assert r["converged"] and set(batches) <= {0, 1}
+    assert np.ptp(rho, axis=1).max() < 1e-10
+    o = prov.o
+    rr, q = o.density(w)
+    f, p = o.free_energy(w, rr)
+    assert abs(f - free_energy_fh(s)) < 1e-9

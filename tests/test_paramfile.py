@@ -458,3 +458,19 @@ def test_response_after_sweep_uses_the_last_point(tmp_path, monkeypatch):
     np.testing.assert_array_equal(got["omega"], st["sweep"][-1].omega)
     assert (tmp_path / "out" / "0.eval").exists() and not (tmp_path / "out" / "0.evec.1").exists()
     assert (tmp_path / "out" / "1.out").exists()
+
+
+def test_nr_n_cut_is_passed_through(monkeypatch):
+    """ITERATE with itr_algo 'NR' reads N_cut as the reference does (it is
+    required there) and hands it to the solver unchanged, 0 included."""
+    from pscf_b200 import sweep as S
+    seen = {}
+    monkeypatch.setattr(S, "nr_solver", lambda group, **kw: seen.update(kw) or (lambda system, w: None))
+    for n_cut in (0, 17):
+        it = P._iterate_params(dict(input_filename=["in.omega"], output_prefix=["out/"], max_itr=[20.0],
+                                    error_max=[1e-8], domain=["T"], itr_algo=["NR"], N_cut=[float(n_cut)]))
+        P._solver(it, "-1")
+        assert seen["n_cut"] == n_cut and seen["domain"] is True
+    with pytest.raises(ValueError):
+        P._iterate_params(dict(input_filename=["in.omega"], output_prefix=["out/"], max_itr=[20.0],
+                               error_max=[1e-8], domain=["T"], itr_algo=["NR"]))
