@@ -10,7 +10,9 @@ layout -- the same layout as the first part of an output summary:
   RESCALE                -- read an omega file and change the monomer
                             reference volume (the next ITERATE starts
                             from that field);
-  ITERATE                -- solve from a basis-format omega file;
+  ITERATE                -- solve from a basis-format omega file, or,
+                            without input_filename, from the current omega
+                            (RESCALE's, or the last ITERATE's or SWEEP's);
   SWEEP                  -- continuation to s_max with d_<name> increments,
                             ended by end_increments;
   RESPONSE               -- eigenvalues and eigenvectors of the linear
@@ -327,27 +329,33 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
             continue
         if name == "FINISH":
             break
-        # set by ITERATE, kept by SWEEP, cleared by every other command (iterate_flag, src/pscf.fp.f90)
+        # iterate_flag: set by ITERATE, kept by SWEEP, cleared by every other
+        # command; omega_flag (a current omega exists): set by ITERATE and
+        # RESCALE, kept by SWEEP and RESPONSE, cleared by the conversions and
+        # listings (src/pscf.fp.f90:174-175, 414-1017)
         iterate_flag = state.get("iterate_flag", False)
         if name not in ("ITERATE", "SWEEP"):
             state["iterate_flag"] = False
+        if name not in ("ITERATE", "SWEEP", "RESPONSE", "RESCALE"):
+            state["omega_flag"] = False
         if name == "RESCALE":
             # src/pscf.fp.f90:414-455: read omega, change v, then omega / scale
             lam = body["vref_scale"][0]
             _, w = F.read_field(at(body["input_filename"][0]), system, group)
             system = rescale_vref(system, lam)
-            state["omega_in"] = w / lam
-            state["omega_file"] = body["input_filename"][0]
+            state.update(omega_cur=w / lam, omega_file=body["input_filename"][0], omega_flag=True)
             continue
         if name == "ITERATE":
             it = _iterate_params(body)
             if it["input_filename"] is None:
-                if "omega_in" not in state:
-                    raise ValueError("ITERATE without input_filename needs a RESCALE before it")
-                w0 = state.pop("omega_in")
+                # the reference reads input_filename only while no omega is current
+                if not state.get("omega_flag"):
+                    raise ValueError("ITERATE without input_filename needs an omega from RESCALE or an ITERATE before it")
+                w0 = state["omega_cur"]
                 it["input_filename"] = state["omega_file"]
             else:
                 _, w0 = F.read_field(at(it["input_filename"]), system, group)
+                state["omega_file"] = it["input_filename"]
             t0 = time.perf_counter()
             w, rho, r = _solver(it, group)(system, w0)
             dt = time.perf_counter() - t0
@@ -365,7 +373,8 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
                 F.write_field(prefix + "omega", w, system, group)
                 F.write_field(prefix + "rho", rho, system, group)
             log(f"ITERATE: {'converged' if r['converged'] else 'not converged'} after {r['itr']} iterations")
-            state.update(iterate=it, omega=w, rho=rho, result=r, n_star=n_star, iterate_flag=True)
+            state.update(iterate=it, omega=w, rho=rho, result=r, n_star=n_star, iterate_flag=True, omega_cur=w,
+                         omega_flag=True)
         elif name == "SWEEP":
             if "result" not in state or not state["result"]["converged"]:
                 raise RuntimeError("SWEEP needs a converged ITERATE before it")
@@ -377,7 +386,7 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
                             start=(state["omega"], state["rho"], state["result"]))
             state["sweep"] = pts
             system = pts[-1].system
-            state["omega"] = pts[-1].omega
+            state["omega"] = state["omega_cur"] = pts[-1].omega
         elif name == "RESPONSE":
             # src/pscf.fp.f90:707-723 and response_sweep, src/response_mod.f90:309-389
             if not iterate_flag:

@@ -474,3 +474,37 @@ def test_nr_n_cut_is_passed_through(monkeypatch):
     with pytest.raises(ValueError):
         P._iterate_params(dict(input_filename=["in.omega"], output_prefix=["out/"], max_itr=[20.0],
                                error_max=[1e-8], domain=["T"], itr_algo=["NR"]))
+
+
+def test_second_iterate_starts_from_the_current_omega(tmp_path, monkeypatch):
+    """omega_flag (src/pscf.fp.f90:479-487): once an ITERATE has run, the
+    next one reads no input_filename and starts from the current omega; a
+    conversion command in between clears it."""
+    import shutil
+    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "in.omega")
+    h = F._read_header(open(tmp_path / "in.omega").read().splitlines())[0]
+    sys_text = _TWO_MONOMER.replace("@CELL@", f'{h["cell_param"][0]:20.10E}')
+    tail = ("output_prefix\n              'out/'\nmax_itr\n                 100\nerror_max\n    1.0000000000E-08\n"
+            "domain\n                   F\nitr_algo\n                'AM'\nN_hist\n                  10\n\n")
+    first = "ITERATE\ninput_filename\n          'in.omega'\n" + tail
+    again = "ITERATE\n" + tail
+    starts = []
+
+    def fake_solver(it, group):
+        def solve(system, w0):
+            starts.append(np.array(w0))
+            r = dict(converged=True, itr=1, error=1e-9, f_helmholtz=1.0, pressure=2.0, stress=[0.0],
+                     mu_chain=[3.0], cell_param=list(system.cell_param))
+            return w0 + 1.0, w0, r
+        return solve
+    monkeypatch.setattr(P, "_solver", fake_solver)
+    (tmp_path / "param").write_text(sys_text + first + again + "FINISH\n")
+    P.run_param(str(tmp_path / "param"))
+    np.testing.assert_array_equal(starts[1], starts[0] + 1.0)
+    from pscf_b200.sweep import read_out
+    d = read_out(str(tmp_path / "out" / "out"))
+    assert d["input_filename"] == ["in.omega"]
+    conv = "FIELD_TO_RGRID\ninput_filename\n          'in.omega'\noutput_filename\n          'x.rg'\n\n"
+    (tmp_path / "p2").write_text(sys_text + first + conv + again + "FINISH\n")
+    with pytest.raises(ValueError):
+        P.run_param(str(tmp_path / "p2"))
