@@ -42,7 +42,7 @@ from .system import Chain, Solvent, System
 SYSTEM_SECTIONS = ("MONOMERS", "CHAINS", "SOLVENTS", "COMPOSITION", "INTERACTION", "UNIT_CELL", "DISCRETIZATION",
                    "BASIS")
 COMMANDS = ("ITERATE", "SWEEP", "RESPONSE", "FIELD_TO_RGRID", "RGRID_TO_FIELD", "KGRID_TO_RGRID", "RHO_TO_OMEGA",
-            "RESCALE", "OUTPUT_WAVES", "OUTPUT_GROUP", "FINISH")
+            "RESCALE", "OUTPUT_WAVES", "OUTPUT_GROUP", "OUTPUT_GROUP_CPP", "WRITE_GROUPS", "FINISH")
 
 
 def _values(line: str):

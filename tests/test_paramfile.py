@@ -223,9 +223,10 @@ FINISH
     assert np.max(np.abs(back - rho)) < 5e-9
     _, w = F.read_field(str(tmp_path / "omega"), s)
     np.testing.assert_allclose(w, s.chi @ rho, atol=1e-9)
-    with pytest.raises(NotImplementedError):
-        (tmp_path / "p2").write_text(text.replace("FIELD_TO_RGRID", "OUTPUT_WAVES", 1))
-        P.run_param(str(tmp_path / "p2"))
+    for listing in ("OUTPUT_WAVES", "OUTPUT_GROUP", "OUTPUT_GROUP_CPP", "WRITE_GROUPS"):
+        (tmp_path / "p2").write_text(text.replace("FIELD_TO_RGRID", listing, 1))
+        with pytest.raises(NotImplementedError):
+            P.run_param(str(tmp_path / "p2"))
 
 
 def test_rescale_reference_volume(tmp_path, monkeypatch):
