@@ -71,3 +71,35 @@ def test_solve_sharded_gloo_matches_serial():
     for r in range(2):
         assert [x["f"] for x in outs[r]] == [x["f"] for x in serial]
         assert all(x["converged"] for x in outs[r])
+
+
+def _reduce_worker(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    import bench
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        # per-rank seconds (max over ranks) and MDE steps (sum over ranks)
+        q.put((rank, bench.reduce_max_sum([0.5 + rank, 1000 * (rank + 1)], ["max", "sum"], "cpu", world)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_reduction_over_ranks_gloo():
+    """The bench's whole-job figures over ranks: the time is the slowest
+    rank's, the work the sum of all ranks' (world size 2, gloo)."""
+    import bench
+    assert bench.reduce_max_sum([1.5, 7], ["max", "sum"], "cpu", 1) == [1.5, 7.0]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_reduce_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    outs = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert outs[0] == outs[1] == [1.5, 3000.0]
