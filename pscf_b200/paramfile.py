@@ -301,6 +301,37 @@ def _response_sweep(system: System, omega, rp: Dict):
         e.close()
 
 
+def _decompose(system: System, group: str, omega, f_total: float) -> Dict:
+    """f_component and overlap of a solution for the DECOMPOSE section
+    (sweep.divide_energy): one density of omega on the engine (fp64), the
+    chains' propagators at their first and last junctions, and the
+    reference-convention coefficients of omega and rho."""
+    from . import field_io as F
+    from .engine import FP64, Engine
+    from .sweep import divide_energy
+    from .system import chain_grid
+    M, nr = system.n_monomer, system.nr
+    w = np.asarray(omega, dtype=np.float64).reshape(M, nr)
+    e = Engine([system], FP64)
+    try:
+        rho, q = e.density(w.reshape(1, M, nr))
+        junctions = []
+        for c, chain in enumerate(system.chains):
+            qf, qr = e.propagators(0, c)
+            bgn, _ = chain_grid(chain.block_length, system.ds)
+            if qf.shape[0] != bgn[-1] + 1:
+                raise RuntimeError(f"chain {c}: {qf.shape[0]} stored slices, {bgn[-1] + 1} expected")
+            h, t = bgn[1], bgn[len(chain.block_length) - 1]
+            junctions.append((qf[h], qr[h], qf[t], qr[t]))
+    finally:
+        e.close()
+    fb = F.field_basis(group, system)
+    omega_c = np.stack([fb.to_coeffs(x) for x in w])
+    rho_c = np.stack([fb.to_coeffs(x) for x in rho[0]])
+    fc, ov = divide_energy(system, omega_c, rho_c, q[0, :len(system.chains)], junctions, f_total)
+    return dict(f_component=fc, overlap=ov)
+
+
 def _solver(it, group):
     from .sweep import am_solver, nr_solver
     if it["itr_algo"] == "AM":
@@ -368,7 +399,8 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
                 os.makedirs(d, exist_ok=True)
             n_star = len(F.field_basis(group, system).stars) if group else 0
             stats = dict(n_star=n_star, final_error=r["error"], iterations=r["itr"], basis_time=0.0, scf_time=dt)
-            write_out(prefix + "out", system, group, r, it, stats)
+            dec = _decompose(system, group, w, r["f_helmholtz"]) if group and system.chains else {}
+            write_out(prefix + "out", system, group, dict(r, **dec), it, stats)
             if group:
                 F.write_field(prefix + "omega", w, system, group)
                 F.write_field(prefix + "rho", rho, system, group)
@@ -383,7 +415,9 @@ def run_param(path: str, workdir: str = None, log=lambda msg: None) -> Dict:
             pts = run_sweep(system, state["omega"], inc, s_max, _solver(it, group), it["domain"],
                             out_prefix=at(it["output_prefix"]), group_name=group or None, iterate=it,
                             n_star=state["n_star"], log=log,
-                            start=(state["omega"], state["rho"], state["result"]))
+                            start=(state["omega"], state["rho"], state["result"]),
+                            decompose=(lambda s_, w_, r_: _decompose(s_, group, w_, r_["f_helmholtz"]))
+                            if group and system.chains else None)
             state["sweep"] = pts
             system = pts[-1].system
             state["omega"] = state["omega_cur"] = pts[-1].omega

@@ -163,9 +163,56 @@ def _str(v: str) -> str:
     return f"{chr(39) + v + chr(39):>20}"
 
 
+def divide_energy(system: System, omega_c: np.ndarray, rho_c: np.ndarray, Q: Sequence[float], junctions,
+                  f_total: float):
+    """Components of the free energy per monomer and the overlap integrals
+    of a solution (divide_energy, src/scf_mod.fp.f90:588-709):
+
+      overlap(a, b) = sum over stars rho_a rho_b,
+      f_enthalpy    = sum_{a<b} chi_ab overlap(a, b),
+      f_head        = -<qf qr log qf / Q> phi / N at the chain's first
+                      junction (block_bgn(2)) - (omega . rho of its first
+                      block's monomer) phi,
+      f_tail        = the same with log qr at its last junction
+                      (block_bgn(N_block)) and the last block's monomer,
+      f_excess      = f_Helmholtz + sum phi / N - the three above,
+
+    summed over chains, the averages over the grid points where qf and qr
+    are both positive.  omega_c, rho_c: basis coefficients [M][n_star] in
+    the reference's convention; Q: the chains' partition functions;
+    junctions: per chain (qf, qr at the first junction, qf, qr at the last)
+    as grid arrays.  Returns (f_component [4], overlap [M][M])."""
+    M = system.n_monomer
+    ov = np.zeros((M, M))
+    enthalpy = 0.0
+    for a in range(M):
+        for b in range(a + 1, M):
+            ov[a, b] = ov[b, a] = float(np.dot(rho_c[a], rho_c[b]))
+            enthalpy += float(system.chi[a, b]) * ov[a, b]
+    fhead = ftail = 0.0
+    nr = None
+    for c, q, (qfh, qrh, qft, qrt) in zip(system.chains, Q, junctions):
+        w = c.phi / sum(c.block_length)
+        nr = len(qfh)
+        m = (qfh > 0.0) & (qrh > 0.0)
+        fhead -= float(np.sum(qfh[m] * qrh[m] / q * np.log(qfh[m]))) * w
+        m = (qft > 0.0) & (qrt > 0.0)
+        ftail -= float(np.sum(qft[m] * qrt[m] / q * np.log(qrt[m]))) * w
+    if nr:
+        fhead /= nr
+        ftail /= nr
+    for c in system.chains:
+        b0, b1 = c.block_monomer[0], c.block_monomer[-1]
+        fhead -= float(np.dot(omega_c[b0], rho_c[b0])) * c.phi
+        ftail -= float(np.dot(omega_c[b1], rho_c[b1])) * c.phi
+    fjct = f_total + sum(c.phi / sum(c.block_length) for c in system.chains) - enthalpy - fhead - ftail
+    return np.array([enthalpy, fhead, ftail, fjct]), ov
+
+
 def write_out(path: str, system: System, group_name: str, result: Dict, iterate: Dict, stats: Dict) -> None:
     """The reference's output summary file: the input-file sections of the
-    system, FINISH, then THERMO and STATISTICS.  result: f_helmholtz,
+    system, FINISH, then THERMO, DECOMPOSE (when the result carries
+    f_component and overlap, from divide_energy) and STATISTICS.  result: f_helmholtz,
     pressure, stress, mu_chain and, when present, mu_solvent (canonical;
     the grand ensemble prints the systems' phi);
     iterate: input_filename, output_prefix, max_itr, error_max, domain,
@@ -232,6 +279,14 @@ def write_out(path: str, system: System, group_name: str, result: Dict, iterate:
     L += [_lab("stress"), "".join(_real(x) for x in r["stress"][:len(s.cell_param)])]
     if s.temperature is not None:                       # chi printed when it follows T
         L += [_lab("chi")] + lower(s.chi)
+    if "f_component" in r and "overlap" in r:
+        # DECOMPOSE (output_summary, src/pscf.fp.f90:1162-1174)
+        ov, fc = r["overlap"], r["f_component"]
+        L += ["", _lab("DECOMPOSE"), _lab("overlap_AB"), _real(ov[0][1])]
+        if s.n_monomer == 3:
+            L += [_lab("overlap_BC"), _real(ov[1][2]), _lab("overlap_CA"), _real(ov[2][0])]
+        L += [_lab("f_enthalpy"), _real(fc[0]), _lab("f_head"), _real(fc[1]), _lab("f_tail"), _real(fc[2]),
+              _lab("f_excess"), _real(fc[3])]
     st = stats
     L += ["", _lab("STATISTICS"), _lab("N_star"), _int(st["n_star"]), _lab("final_error"),
           _real(st["final_error"]), _lab("iterations"), _int(st["iterations"]), _lab("basis_time"),
@@ -321,14 +376,17 @@ class SweepPoint:
 def run_sweep(system: System, omega: np.ndarray, inc: Increments, s_max: float, solve: Callable,
               domain: bool, out_prefix: Optional[str] = None, group_name: Optional[str] = None,
               iterate: Optional[Dict] = None, n_star: int = 0, min_step: float = 1.0 / 16.0,
-              log: Callable[[str], None] = lambda msg: None, start=None) -> List[SweepPoint]:
+              log: Callable[[str], None] = lambda msg: None, start=None,
+              decompose: Optional[Callable] = None) -> List[SweepPoint]:
     """ITERATE at s = 0, then SWEEP to s_max (src/pscf.fp.f90:557-700).
     Returns the converged points at integer s (s = 0 first); with
     out_prefix, writes <prefix><j>.out (and <prefix><j>.omega / .rho in the
     basis format when group_name is given) for each of them.  start:
     (omega, rho, result) of an already converged s = 0 point, which is then
     neither solved again nor written.  Raises RuntimeError when a point
-    fails at the smallest unit step or at s = 0."""
+    fails at the smallest unit step or at s = 0.  decompose(system, omega,
+    result) -> dict(f_component, overlap), when given, adds the DECOMPOSE
+    section to every file written."""
     def emit(j, pt):
         if not out_prefix:
             return
@@ -336,6 +394,8 @@ def run_sweep(system: System, omega: np.ndarray, inc: Increments, s_max: float, 
         if d:
             os.makedirs(d, exist_ok=True)
         r = pt.result
+        if decompose is not None:
+            r = dict(r, **decompose(pt.system, pt.omega, r))
         stats = dict(n_star=n_star, final_error=r["error"], iterations=r["itr"], basis_time=0.0,
                      scf_time=pt.seconds)
         write_out(f"{out_prefix}{j}.out", pt.system, group_name or "", r, iterate or {}, stats)

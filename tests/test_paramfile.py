@@ -14,6 +14,32 @@ from pscf_b200 import paramfile as P
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
+def _oracle_decompose(system, group, omega, f_total):
+    """_decompose with the oracle's density and propagators in place of the
+    engine's (the CPU stand-in)."""
+    from oracle import oracle as O
+    from pscf_b200.sweep import divide_energy
+    from pscf_b200.system import chain_grid
+    w = np.asarray(omega, dtype=np.float64).reshape(system.n_monomer, system.nr)
+    o = O.Oracle(system)
+    rho, q = o.density(w)
+    junctions = []
+    for c, chain in enumerate(system.chains):
+        qf, qr = o.propagators(c)
+        bgn, _ = chain_grid(chain.block_length, system.ds)
+        h, t = bgn[1], bgn[len(chain.block_length) - 1]
+        junctions.append((qf[h], qr[h], qf[t], qr[t]))
+    fb = F.field_basis(group, system)
+    fc, ov = divide_energy(system, np.stack([fb.to_coeffs(x) for x in w]), np.stack([fb.to_coeffs(x) for x in rho]),
+                           q, junctions, f_total)
+    return dict(f_component=fc, overlap=ov)
+
+
+@pytest.fixture(autouse=True)
+def _decompose_on_the_oracle(monkeypatch):
+    monkeypatch.setattr(P, "_decompose", _oracle_decompose)
+
+
 def test_reference_file_system_and_iterate():
     param = P.read_param(os.path.join(HERE, "golden", "lamellar.out"))
     assert [n for n, _ in param][-2:] == ["ITERATE", "FINISH"]
@@ -509,3 +535,63 @@ def test_second_iterate_starts_from_the_current_omega(tmp_path, monkeypatch):
     (tmp_path / "p2").write_text(sys_text + first + conv + again + "FINISH\n")
     with pytest.raises(ValueError):
         P.run_param(str(tmp_path / "p2"))
+
+
+def test_divide_energy_uniform_fields():
+    """divide_energy (src/scf_mod.fp.f90:588-709) on uniform fields a, b
+    of a diblock f_A, N = 1: q is exp(-a s) along the A block, so at the
+    junction qf qr / Q = 1 and f_head = -log qf - a f_A = 0, f_tail = 0;
+    overlap_AB = f_A f_B; f_excess = f_total + 1 - chi f_A f_B."""
+    from oracle import oracle as O
+    from pscf_b200.sweep import divide_energy
+    from pscf_b200.system import Chain, System, chain_grid
+    s = System(dim=1, ngrid=[16], crystal_system="lamellar", cell_param=[1.7], kuhn=[1.0, 1.0],
+               chi=[[0.0, 14.0], [14.0, 0.0]], chains=[Chain([0, 1], [0.4, 0.6], phi=1.0)], ds=0.01)
+    w = np.stack([np.full(16, 2.0), np.full(16, -0.5)])
+    o = O.Oracle(s)
+    rho, q = o.density(w)
+    qf, qr = o.propagators(0)
+    h = chain_grid([0.4, 0.6], 0.01)[0][1]
+    fb = F.FieldBasis("-1", s)
+    fc, ov = divide_energy(s, np.stack([fb.to_coeffs(x) for x in w]), np.stack([fb.to_coeffs(x) for x in rho]), q,
+                           [(qf[h], qr[h], qf[h], qr[h])], 3.0)
+    assert abs(fc[1]) < 1e-12 and abs(fc[2]) < 1e-12
+    assert abs(ov[0, 1] - 0.4 * 0.6) < 1e-12 and abs(fc[0] - 14.0 * 0.24) < 1e-11
+    assert abs(fc[3] - (3.0 + 1.0 - 14.0 * 0.24)) < 1e-11
+
+
+def test_decompose_section_in_iterate_and_sweep_files(tmp_path, monkeypatch):
+    """The summary of the current reference writes DECOMPOSE between THERMO
+    and STATISTICS (output_summary, src/pscf.fp.f90:1162-1174): overlap_AB,
+    f_enthalpy, f_head, f_tail, f_excess, for the ITERATE file and every
+    sweep point."""
+    import shutil
+    from pscf_b200.sweep import read_out
+    shutil.copy(os.path.join(HERE, "golden", "fieldfile_rho.txt"), tmp_path / "in.omega")
+    h = F._read_header(open(tmp_path / "in.omega").read().splitlines())[0]
+    sys_text = _TWO_MONOMER.replace("@CELL@", f'{h["cell_param"][0]:20.10E}')
+    iterate = ("ITERATE\ninput_filename\n          'in.omega'\noutput_prefix\n              'out/'\nmax_itr\n"
+               "                 100\nerror_max\n    1.0000000000E-08\ndomain\n                   F\n"
+               "itr_algo\n                'AM'\nN_hist\n                  10\n\n")
+    sweep = "SWEEP\ns_max\n    1.0000000000E+00\nd_chi\n    2.0000000000E+00\nend_increments\n\n"
+
+    def fake_solver(it, group):
+        def solve(system, w0):
+            r = dict(converged=True, itr=1, error=1e-9, f_helmholtz=1.25, pressure=2.0, stress=[0.0],
+                     mu_chain=[3.0], cell_param=list(system.cell_param))
+            return w0, w0, r
+        return solve
+    monkeypatch.setattr(P, "_solver", fake_solver)
+    (tmp_path / "param").write_text(sys_text + iterate + sweep + "FINISH\n")
+    st = P.run_param(str(tmp_path / "param"))
+    for j in (0, 1):
+        lines = open(tmp_path / "out" / f"{j}.out").read().splitlines()
+        i = lines.index("DECOMPOSE           ")
+        assert lines[i - 1] == "" and lines.index("STATISTICS          ") > i > lines.index("THERMO              ")
+        assert [x.strip() for x in lines[i + 1:i + 11:2]] == ["overlap_AB", "f_enthalpy", "f_head", "f_tail", "f_excess"]
+        d = read_out(str(tmp_path / "out" / f"{j}.out"))
+        pt = st["sweep"][j]
+        want = _oracle_decompose(pt.system, "-1", pt.omega, 1.25)
+        assert abs(d["overlap_AB"][0] - want["overlap"][0, 1]) < 1e-9 * max(1.0, abs(want["overlap"][0, 1]))
+        np.testing.assert_allclose([d[k][0] for k in ("f_enthalpy", "f_head", "f_tail", "f_excess")],
+                                   want["f_component"], rtol=1e-9, atol=1e-10)
