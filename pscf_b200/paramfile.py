@@ -308,13 +308,14 @@ def _decompose(system: System, group: str, omega, f_total: float) -> Dict:
     reference-convention coefficients of omega and rho."""
     from . import field_io as F
     from .engine import FP64, Engine
-    from .sweep import divide_energy
+    from .sweep import divide_energy, grand_phi
     from .system import chain_grid
     M, nr = system.n_monomer, system.nr
     w = np.asarray(omega, dtype=np.float64).reshape(M, nr)
     e = Engine([system], FP64)
     try:
         rho, q = e.density(w.reshape(1, M, nr))
+        system = grand_phi(system, dict(q=q[0, :len(system.chains)], q_solvent=e.q_solvent[0, :len(system.solvents)]))
         junctions = []
         for c, chain in enumerate(system.chains):
             qf, qr = e.propagators(0, c)

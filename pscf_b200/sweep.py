@@ -163,6 +163,21 @@ def _str(v: str) -> str:
     return f"{chr(39) + v + chr(39):>20}"
 
 
+def grand_phi(system: System, result: Dict) -> System:
+    """The system with the volume fractions of a grand-canonical solution,
+    phi = Q exp(mu) for chains (mu_phi_chain, src/scf_mod.fp.f90:768-785)
+    and solvents (solvent_density, :251-295), from the result's q and
+    q_solvent; a canonical system is returned as it is."""
+    if system.ensemble != 1:
+        return system
+    s = copy.deepcopy(system)
+    for c, q in zip(s.chains, result.get("q", [])):
+        c.phi = float(q) * float(np.exp(c.mu))
+    for v, q in zip(s.solvents, result.get("q_solvent", [])):
+        v.phi = float(q) * float(np.exp(v.mu))
+    return s
+
+
 def divide_energy(system: System, omega_c: np.ndarray, rho_c: np.ndarray, Q: Sequence[float], junctions,
                   f_total: float):
     """Components of the free energy per monomer and the overlap integrals
@@ -212,9 +227,10 @@ def divide_energy(system: System, omega_c: np.ndarray, rho_c: np.ndarray, Q: Seq
 def write_out(path: str, system: System, group_name: str, result: Dict, iterate: Dict, stats: Dict) -> None:
     """The reference's output summary file: the input-file sections of the
     system, FINISH, then THERMO, DECOMPOSE (when the result carries
-    f_component and overlap, from divide_energy) and STATISTICS.  result: f_helmholtz,
-    pressure, stress, mu_chain and, when present, mu_solvent (canonical;
-    the grand ensemble prints the systems' phi);
+    f_component and overlap, from divide_energy) and STATISTICS.  result:
+    f_helmholtz, pressure, stress, mu_chain and, when present, mu_solvent
+    (canonical); the grand ensemble prints phi = Q exp(mu) from the
+    result's q (and q_solvent), and f_homo of those phi;
     iterate: input_filename, output_prefix, max_itr, error_max, domain,
     itr_algo and N_cut or N_hist; stats: n_star, final_error, iterations,
     basis_time, scf_time."""
@@ -264,8 +280,9 @@ def write_out(path: str, system: System, group_name: str, result: Dict, iterate:
         L += [_lab("N_hist"), _int(it["N_hist"])]
     L += ["", _lab("FINISH")]
     r = result
+    sp = grand_phi(s, r)                                # phi of the solution in the grand ensemble
     L += ["", _lab("THERMO"), _lab("f_Helmholtz"), _real(r["f_helmholtz"]), _lab("f_homo"),
-          _real(free_energy_fh(s)), _lab("pressure"), _real(r["pressure"])]
+          _real(free_energy_fh(sp)), _lab("pressure"), _real(r["pressure"])]
     if s.ensemble == 0:
         if s.chains:
             L += [_lab("mu_chain")] + [_real(m) for m in r["mu_chain"][:len(s.chains)]]
@@ -273,9 +290,9 @@ def write_out(path: str, system: System, group_name: str, result: Dict, iterate:
             L += [_lab("mu_solvent")] + [_real(m) for m in r["mu_solvent"][:len(s.solvents)]]
     else:
         if s.chains:
-            L += [_lab("phi_chain")] + [_real(c.phi) for c in s.chains]
+            L += [_lab("phi_chain")] + [_real(c.phi) for c in sp.chains]
         if s.solvents:
-            L += [_lab("phi_solvent")] + [_real(v.phi) for v in s.solvents]
+            L += [_lab("phi_solvent")] + [_real(v.phi) for v in sp.solvents]
     L += [_lab("stress"), "".join(_real(x) for x in r["stress"][:len(s.cell_param)])]
     if s.temperature is not None:                       # chi printed when it follows T
         L += [_lab("chi")] + lower(s.chi)

@@ -222,3 +222,23 @@ def test_sweep_reproduces_the_reference_sweep_files(tmp_path, monkeypatch):
         for k, (a, b) in enumerate(zip(got, want)):
             if k not in skip:
                 assert a == b, (j, k, a, b)
+
+
+def test_grand_canonical_summary_prints_the_solution_phi(tmp_path):
+    """Grand ensemble (ensemble = 1): COMPOSITION holds mu_chain, and THERMO
+    the chains' phi = Q exp(mu) (mu_phi_chain, src/scf_mod.fp.f90:768-785)
+    with f_homo of those phi (output_summary, src/pscf.fp.f90:1130-1150)."""
+    chains = [Chain([0, 1], [0.4, 0.6], mu=1.5), Chain([0], [0.5], mu=-0.25)]
+    s = System(dim=1, ngrid=[16], crystal_system="lamellar", cell_param=[1.7], kuhn=[1.0, 1.0],
+               chi=[[0, 12.0], [12.0, 0]], chains=chains, ds=0.01, ensemble=1)
+    q = [0.123, 1.9]
+    res = dict(f_helmholtz=2.0, pressure=3.0, stress=[1e-12], mu_chain=[1.5, -0.25], q=q)
+    it = dict(max_itr=10, error_max=1e-8, domain=True, itr_algo="AM", N_hist=20)
+    S.write_out(str(tmp_path / "g.out"), s, "-1", res, it, dict(n_star=9, final_error=1e-9, iterations=5))
+    d = S.read_out(str(tmp_path / "g.out"))
+    phi = [q[0] * np.exp(1.5), q[1] * np.exp(-0.25)]
+    np.testing.assert_allclose(d["phi_chain"], phi, rtol=1e-10)
+    np.testing.assert_allclose(d["mu_chain"], [1.5, -0.25])
+    sp = S.grand_phi(s, res)
+    assert [c.phi for c in sp.chains] == phi and s.chains[0].phi == 1.0       # the input is not modified
+    assert abs(d["f_homo"][0] - S.free_energy_fh(sp)) < 1e-9 * abs(S.free_energy_fh(sp))
