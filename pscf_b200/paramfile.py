@@ -303,9 +303,10 @@ def _response_sweep(system: System, omega, rp: Dict):
 
 def _decompose(system: System, group: str, omega, f_total: float) -> Dict:
     """f_component and overlap of a solution for the DECOMPOSE section
-    (sweep.divide_energy): one density of omega on the engine (fp64), the
-    chains' propagators at their first and last junctions, and the
-    reference-convention coefficients of omega and rho."""
+    (sweep.divide_energy), and the solvents' partition functions q_solvent
+    (for mu_solvent, or phi in the grand ensemble): one density of omega on
+    the engine (fp64), the chains' propagators at their first and last
+    junctions, and the reference-convention coefficients of omega and rho."""
     from . import field_io as F
     from .engine import FP64, Engine
     from .sweep import divide_energy, grand_phi
@@ -315,7 +316,8 @@ def _decompose(system: System, group: str, omega, f_total: float) -> Dict:
     e = Engine([system], FP64)
     try:
         rho, q = e.density(w.reshape(1, M, nr))
-        system = grand_phi(system, dict(q=q[0, :len(system.chains)], q_solvent=e.q_solvent[0, :len(system.solvents)]))
+        q_solvent = [float(x) for x in e.q_solvent[0, :len(system.solvents)]]
+        system = grand_phi(system, dict(q=q[0, :len(system.chains)], q_solvent=q_solvent))
         junctions = []
         for c, chain in enumerate(system.chains):
             qf, qr = e.propagators(0, c)
@@ -330,7 +332,7 @@ def _decompose(system: System, group: str, omega, f_total: float) -> Dict:
     omega_c = np.stack([fb.to_coeffs(x) for x in w])
     rho_c = np.stack([fb.to_coeffs(x) for x in rho[0]])
     fc, ov = divide_energy(system, omega_c, rho_c, q[0, :len(system.chains)], junctions, f_total)
-    return dict(f_component=fc, overlap=ov)
+    return dict(f_component=fc, overlap=ov, q_solvent=q_solvent)
 
 
 def _solver(it, group):

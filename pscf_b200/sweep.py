@@ -229,8 +229,9 @@ def write_out(path: str, system: System, group_name: str, result: Dict, iterate:
     system, FINISH, then THERMO, DECOMPOSE (when the result carries
     f_component and overlap, from divide_energy) and STATISTICS.  result:
     f_helmholtz, pressure, stress, mu_chain and, when present, mu_solvent
-    (canonical); the grand ensemble prints phi = Q exp(mu) from the
-    result's q (and q_solvent), and f_homo of those phi;
+    (canonical; without it, log(phi / q_solvent) when the result carries
+    the solvents' q_solvent); the grand ensemble prints phi = Q exp(mu)
+    from the result's q (and q_solvent), and f_homo of those phi;
     iterate: input_filename, output_prefix, max_itr, error_max, domain,
     itr_algo and N_cut or N_hist; stats: n_star, final_error, iterations,
     basis_time, scf_time."""
@@ -286,8 +287,12 @@ def write_out(path: str, system: System, group_name: str, result: Dict, iterate:
     if s.ensemble == 0:
         if s.chains:
             L += [_lab("mu_chain")] + [_real(m) for m in r["mu_chain"][:len(s.chains)]]
-        if s.solvents and "mu_solvent" in r:
-            L += [_lab("mu_solvent")] + [_real(m) for m in r["mu_solvent"][:len(s.solvents)]]
+        mus = r.get("mu_solvent")
+        if mus is None and "q_solvent" in r:
+            # mu = log(phi / Q) (mu_phi_solvent, src/scf_mod.fp.f90:803-820)
+            mus = [float(np.log(v.phi / q)) for v, q in zip(s.solvents, r["q_solvent"])]
+        if s.solvents and mus is not None:
+            L += [_lab("mu_solvent")] + [_real(m) for m in mus[:len(s.solvents)]]
     else:
         if s.chains:
             L += [_lab("phi_chain")] + [_real(c.phi) for c in sp.chains]

@@ -32,7 +32,7 @@ def _oracle_decompose(system, group, omega, f_total):
     fb = F.field_basis(group, system)
     fc, ov = divide_energy(system, np.stack([fb.to_coeffs(x) for x in w]), np.stack([fb.to_coeffs(x) for x in rho]),
                            q, junctions, f_total)
-    return dict(f_component=fc, overlap=ov)
+    return dict(f_component=fc, overlap=ov, q_solvent=[])
 
 
 @pytest.fixture(autouse=True)

@@ -242,3 +242,18 @@ def test_grand_canonical_summary_prints_the_solution_phi(tmp_path):
     sp = S.grand_phi(s, res)
     assert [c.phi for c in sp.chains] == phi and s.chains[0].phi == 1.0       # the input is not modified
     assert abs(d["f_homo"][0] - S.free_energy_fh(sp)) < 1e-9 * abs(S.free_energy_fh(sp))
+
+
+def test_canonical_solvent_mu_from_its_partition_function(tmp_path):
+    """Canonical ensemble with a solvent: THERMO prints mu_solvent =
+    log(phi / Q_solvent) (mu_phi_solvent, src/scf_mod.fp.f90:803-820) when
+    the result carries the solvent's Q."""
+    s = System(dim=1, ngrid=[16], crystal_system="lamellar", cell_param=[1.7], kuhn=[1.0, 1.0],
+               chi=[[0, 12.0], [12.0, 0]], chains=[Chain([0, 1], [0.4, 0.6], phi=0.9)],
+               solvents=[Solvent(1, 0.1, phi=0.1)], ds=0.01)
+    res = dict(f_helmholtz=2.0, pressure=3.0, stress=[1e-12], mu_chain=[1.5], q_solvent=[0.8])
+    it = dict(max_itr=10, error_max=1e-8, domain=True, itr_algo="AM", N_hist=20)
+    S.write_out(str(tmp_path / "s.out"), s, "-1", res, it, dict(n_star=9, final_error=1e-9, iterations=5))
+    d = S.read_out(str(tmp_path / "s.out"))
+    assert abs(d["mu_solvent"][0] - np.log(0.1 / 0.8)) < 1e-10
+    assert d["phi_solvent"] == [0.1] and d["solvent_size"] == [0.1]
