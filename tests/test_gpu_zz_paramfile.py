@@ -1,7 +1,10 @@
 """A reference-style parameter file run on the GPU engine: ITERATE from a
 basis-format omega file, then SWEEP in chi (src/pscf.fp.f90:520-700).  The
 files written are the reference's (<prefix>0.out, 1.out, ... with their
-omega and rho), and the last point equals a direct solve at its chi."""
+omega and rho), and the last point equals a direct solve at its chi.
+Collected after the other GPU files: it drives the whole host stack
+(parameter files, sweep, response, the summary's decomposition) over the
+kernels those files test."""
 import numpy as np
 import pytest
 
