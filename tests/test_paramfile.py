@@ -35,6 +35,9 @@ def _oracle_decompose(system, group, omega, f_total):
     return dict(f_component=fc, overlap=ov, q_solvent=[])
 
 
+_ENGINE_DECOMPOSE = P._decompose          # the product's, before the fixture below replaces it
+
+
 @pytest.fixture(autouse=True)
 def _decompose_on_the_oracle(monkeypatch):
     monkeypatch.setattr(P, "_decompose", _oracle_decompose)
@@ -595,3 +598,49 @@ def test_decompose_section_in_iterate_and_sweep_files(tmp_path, monkeypatch):
         assert abs(d["overlap_AB"][0] - want["overlap"][0, 1]) < 1e-9 * max(1.0, abs(want["overlap"][0, 1]))
         np.testing.assert_allclose([d[k][0] for k in ("f_enthalpy", "f_head", "f_tail", "f_excess")],
                                    want["f_component"], rtol=1e-9, atol=1e-10)
+
+
+class _OracleEngine:
+    """The engine's interface as _decompose uses it (density with q padded
+    to MAX_CHAIN, q_solvent, propagators, close), served by the oracle."""
+
+    def __init__(self, systems, precision):
+        from oracle import oracle as O
+        self.s = systems[0]
+        self.o = O.Oracle(self.s)
+
+    def density(self, omega):
+        from pscf_b200.system import MAX_CHAIN, MAX_SOLVENT
+        rho, q = self.o.density(np.asarray(omega)[0])
+        qq = np.zeros((1, MAX_CHAIN))
+        qq[0, :len(q)] = q
+        self.q_solvent = np.zeros((1, MAX_SOLVENT))
+        for i, v in enumerate(self.s.solvents):
+            w = np.asarray(omega)[0, v.monomer]
+            self.q_solvent[0, i] = np.mean(np.exp(-v.size * w))      # solvent_density's Q
+        return rho[None], qq
+
+    def propagators(self, inst=0, chain=0):
+        return self.o.propagators(chain)
+
+    def close(self):
+        pass
+
+
+def test_decompose_through_the_engine_interface(monkeypatch):
+    """The product's _decompose (not the stand-in used above), with the
+    engine class replaced by the oracle behind the same interface: its
+    slice bookkeeping, junction choice and solvent partition functions
+    give the stand-in's values, for a triblock with a solvent."""
+    import pscf_b200.engine as EN
+    from pscf_b200.system import Chain, Solvent, System
+    monkeypatch.setattr(EN, "Engine", _OracleEngine)
+    s = System(dim=1, ngrid=[16], crystal_system="lamellar", cell_param=[1.7], kuhn=[1.0, 1.1, 0.9],
+               chi=np.array([[0, 12.0, 20.0], [12.0, 0, 15.0], [20.0, 15.0, 0]]),
+               chains=[Chain([0, 1, 2], [0.3, 0.4, 0.3], phi=0.8)], solvents=[Solvent(1, 0.2, phi=0.2)], ds=0.01)
+    w = 1.5 * np.cos(2 * np.pi * np.arange(16) / 16)[None, :] * np.array([[1.0], [-0.5], [0.3]])
+    got = _ENGINE_DECOMPOSE(s, "-1", w, 2.5)
+    want = _oracle_decompose(s, "-1", w, 2.5)
+    np.testing.assert_allclose(got["f_component"], want["f_component"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(got["overlap"], want["overlap"], rtol=1e-12, atol=1e-14)
+    assert abs(got["q_solvent"][0] - np.mean(np.exp(-0.2 * w[1]))) < 1e-15
