@@ -31,6 +31,7 @@ FFT.
 """
 from __future__ import annotations
 
+import threading
 from collections import OrderedDict
 from typing import Dict, List, Sequence, Tuple
 
@@ -111,13 +112,24 @@ _STAR_BASES: "OrderedDict[Tuple, StarBasis]" = OrderedDict()
 _FIELD_BASES: "OrderedDict[Tuple, FieldBasis]" = OrderedDict()
 
 
+_CACHE_LOCK = threading.Lock()
+
+
 def _cached(cache: OrderedDict, key: Tuple, make, keep: int):
-    obj = cache.pop(key, None)
-    if obj is None:
-        obj = make()
-    cache[key] = obj
-    while len(cache) > keep:
-        cache.popitem(last=False)
+    """cache[key], made by make() when missing; the least recently used
+    entries beyond `keep` are dropped.  Safe across host threads (the
+    bases are read-only once made)."""
+    with _CACHE_LOCK:
+        obj = cache.pop(key, None)
+        if obj is not None:
+            cache[key] = obj
+            return obj
+    obj = make()
+    with _CACHE_LOCK:
+        obj = cache.pop(key, obj)          # another thread may have made it meanwhile
+        cache[key] = obj
+        while len(cache) > keep:
+            cache.popitem(last=False)
     return obj
 
 
